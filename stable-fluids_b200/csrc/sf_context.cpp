@@ -1,0 +1,648 @@
+// sf_context.cpp -- the C ABI of stable-fluids-3d.h / stable-fluids-b200.h:
+// context creation and validation, device memory, the step graph, views.
+//
+// Reference behaviour followed (Xayah-Graphics/stable-fluids backend-cuda.cu):
+//   create   :481-680  (validation 516-528/538-540, 1-based handles 544/551,
+//                       allocation 560-581, initial values 583-606,
+//                       one captured graph per step 608-675)
+//   destroy  :682-690  update_* :692-719  step :721-726  get_view :728-800
+// Differences, all additive: a null desc/context/out pointer, a non-positive
+// grid size or cell size, or a negative iteration count is rejected with
+// BACKEND_FAILURE instead of being dereferenced or used; destroy(nullptr) is a
+// no-op; update_* accept host pointers too (cudaMemcpyDefault).
+
+#include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string_view>
+#include <vector>
+
+#include "sf_launch.h"
+#include "sf_types.h"
+#include "stable-fluids-3d.h"
+#include "stable-fluids-b200.h"
+
+namespace sfb {
+namespace {
+
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
+
+struct ScalarField {
+    StableFluidsScalarFieldDesc desc{};
+    ScalarBC bc{};
+    float* data = nullptr;
+    float* temp = nullptr;
+    float* source = nullptr;
+};
+
+struct VectorField {
+    StableFluidsVectorFieldDesc desc{};
+    float* data[3] = {nullptr, nullptr, nullptr};
+};
+
+struct Context {
+    StableFluidsSimulationConfig config{};
+    StableFluidsB200Options options{};
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    Dims dims{};
+    size_t cells = 0;
+    size_t field_bytes = 0;
+    FlowBC flow{};
+
+    void* slab = nullptr;
+    size_t slab_bytes = 0;
+    float* vel[3] = {nullptr, nullptr, nullptr};
+    float* temp[3] = {nullptr, nullptr, nullptr};
+    void* packed = nullptr;  // float4 velocity
+    float* pressure = nullptr;
+    float* divergence = nullptr;
+    float* magnitude = nullptr;
+    float* scratch = nullptr;
+    DeviceStats* stats = nullptr;
+    DeviceStats* host_stats = nullptr;  // pinned
+    std::vector<ScalarField> scalars;
+    std::vector<VectorField> vectors;
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ready = nullptr;
+    bool residual_enabled = false;
+    int step_kernels = 0;  // kernel nodes in the step graph
+
+    ~Context() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ready) cudaEventDestroy(ready);
+        if (slab) cudaFree(slab);
+        if (host_stats) cudaFreeHost(host_stats);
+        if (owns_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+bool valid_flow_type(uint32_t t) { return t <= STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC; }
+bool valid_scalar_type(uint32_t t) { return t <= STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC; }
+
+// backend-cuda.cu:516-520 -- known kinds, periodic faces come in pairs.
+bool validate_flow(const StableFluidsFlowBoundaryConfig& b) {
+    const StableFluidsFlowBoundaryFaceDesc* f = &b.x_minus;
+    for (int a = 0; a < 3; ++a) {
+        const auto lo = f[2 * a].type, hi = f[2 * a + 1].type;
+        if (!valid_flow_type(lo) || !valid_flow_type(hi)) return false;
+        if ((lo == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC) != (hi == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC)) return false;
+    }
+    return true;
+}
+
+// backend-cuda.cu:521-525
+bool validate_scalar(const StableFluidsScalarBoundaryConfig& b) {
+    const StableFluidsScalarBoundaryFaceDesc* f = &b.x_minus;
+    for (int a = 0; a < 3; ++a) {
+        const auto lo = f[2 * a].type, hi = f[2 * a + 1].type;
+        if (!valid_scalar_type(lo) || !valid_scalar_type(hi)) return false;
+        if ((lo == STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC) != (hi == STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC)) return false;
+    }
+    return true;
+}
+
+FlowBC flatten(const StableFluidsFlowBoundaryConfig& b) {
+    FlowBC o{};
+    const StableFluidsFlowBoundaryFaceDesc* f = &b.x_minus;
+    for (int k = 0; k < 6; ++k) {
+        o.type[k] = static_cast<int32_t>(f[k].type);
+        o.vel[k][0] = f[k].velocity_x;
+        o.vel[k][1] = f[k].velocity_y;
+        o.vel[k][2] = f[k].velocity_z;
+        o.pressure[k] = f[k].pressure;
+        if (f[k].type == STABLE_FLUIDS_FLOW_BOUNDARY_OUTFLOW) o.any_outflow = 1;
+    }
+    for (int a = 0; a < 3; ++a) o.periodic[a] = f[2 * a].type == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC && f[2 * a + 1].type == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC;
+    return o;
+}
+
+ScalarBC flatten(const StableFluidsScalarBoundaryConfig& b) {
+    ScalarBC o{};
+    const StableFluidsScalarBoundaryFaceDesc* f = &b.x_minus;
+    for (int k = 0; k < 6; ++k) {
+        o.type[k] = static_cast<int32_t>(f[k].type);
+        o.value[k] = f[k].value;
+    }
+    for (int a = 0; a < 3; ++a) o.periodic[a] = f[2 * a].type == STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC && f[2 * a + 1].type == STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC;
+    return o;
+}
+
+bool env_flag(const char* name) {
+    const char* v = std::getenv(name);
+    return v != nullptr && *v != '\0' && std::string_view(v) != "0";
+}
+
+void apply_env_overrides(StableFluidsB200Options& o) {
+    if (const char* v = std::getenv("STABLE_FLUIDS_B200_SCHEME")) {
+        const std::string_view s(v);
+        if (s == "jacobi" || s == "JACOBI" || s == "1") o.scheme = STABLE_FLUIDS_B200_SCHEME_JACOBI;
+        else if (s == "rbgs" || s == "RBGS" || s == "0") o.scheme = STABLE_FLUIDS_B200_SCHEME_RBGS;
+    }
+    if (const char* v = std::getenv("STABLE_FLUIDS_B200_ITERATIONS_PER_PASS")) o.iterations_per_pass = std::atoi(v);
+    if (const char* v = std::getenv("STABLE_FLUIDS_B200_RESIDUAL_TOLERANCE")) o.residual_tolerance = static_cast<float>(std::atof(v));
+    if (const char* v = std::getenv("STABLE_FLUIDS_B200_MAX_PRESSURE_ITERATIONS")) o.max_pressure_iterations = std::atoi(v);
+    if (const char* v = std::getenv("STABLE_FLUIDS_B200_WARM_START")) {
+        const std::string_view s(v);
+        if (s == "previous" || s == "1") o.warm_start = STABLE_FLUIDS_B200_WARM_START_PREVIOUS;
+        else if (s == "zero" || s == "0") o.warm_start = STABLE_FLUIDS_B200_WARM_START_ZERO;
+    }
+    if (env_flag("STABLE_FLUIDS_B200_COMPUTE_RESIDUAL")) o.compute_residual = 1;
+}
+
+void default_options(StableFluidsB200Options& o) {
+    o = StableFluidsB200Options{};
+    o.scheme = STABLE_FLUIDS_B200_SCHEME_RBGS;
+    o.warm_start = STABLE_FLUIDS_B200_WARM_START_ZERO;
+    o.iterations_per_pass = 0;
+    o.residual_tolerance = 0.0f;
+    o.max_pressure_iterations = 0;
+    o.residual_check_interval = 8;
+    o.compute_residual = 0;
+}
+
+bool validate_options(const StableFluidsB200Options& o) {
+    if (o.scheme > STABLE_FLUIDS_B200_SCHEME_JACOBI) return false;
+    if (o.warm_start > STABLE_FLUIDS_B200_WARM_START_PREVIOUS) return false;  // learned: not in this build yet
+    if (o.iterations_per_pass < 0) return false;
+    if (!(o.residual_tolerance >= 0.0f) || !std::isfinite(o.residual_tolerance)) return false;
+    if (o.residual_tolerance > 0.0f && (o.max_pressure_iterations <= 0 || o.residual_check_interval <= 0)) return false;
+    return true;
+}
+
+// Carves every device array out of one allocation, each 256-byte aligned.
+struct SlabPlan {
+    struct Item {
+        void** where;
+        size_t bytes;
+    };
+    std::vector<Item> items;
+    void add(void** where, size_t bytes) { items.push_back({where, bytes}); }
+    size_t total() const {
+        size_t t = 0;
+        for (const auto& it : items) t += (it.bytes + 255) & ~static_cast<size_t>(255);
+        return t;
+    }
+    void assign(void* base) const {
+        auto* p = static_cast<char*>(base);
+        for (const auto& it : items) {
+            *it.where = p;
+            p += (it.bytes + 255) & ~static_cast<size_t>(255);
+        }
+    }
+};
+
+// ---- stages of the step, in the reference's order (backend-cuda.cu:612-671).
+// Each enqueues its work on the context stream (inside the step-graph capture
+// or, for profiling, directly) and adds its kernel count to `launches`.
+struct Stages {
+    Context& c;
+    int launches = 0;
+    cudaError_t e = cudaSuccess;
+
+    bool ok(cudaError_t r, int kernels = 1) {
+        if (r == cudaSuccess) launches += kernels;
+        else if (e == cudaSuccess) e = r;
+        return r == cudaSuccess;
+    }
+    float h() const { return c.config.cell_size; }
+    float alpha_v() const { return c.config.dt * c.config.viscosity / (h() * h()); }  // :622
+    float alpha_s(const ScalarField& f) const { return c.config.dt * f.desc.diffusion / (h() * h()); }  // :656
+    bool any_scalar_advects() const {
+        for (const auto& f : c.scalars)
+            if (alpha_s(f) > 0.0f) return true;
+        return false;
+    }
+
+    // 1. v += dt f field by field (:612-615), fused with packing the velocity
+    //    for the advection gathers.
+    void forces() {
+        std::vector<const VectorField*> list;
+        for (const auto& v : c.vectors)
+            if (v.desc.usage == STABLE_FLUIDS_VECTOR_FIELD_FORCE) list.push_back(&v);
+        const bool advect = alpha_v() > 0.0f;
+        size_t k = 0;
+        do {
+            ForceArgs fa{};
+            for (int comp = 0; comp < 3; ++comp) fa.vel[comp] = c.vel[comp];
+            fa.dt = c.config.dt;
+            fa.n = c.cells;
+            for (; k < list.size() && fa.force_count < kMaxForcesPerLaunch; ++k, ++fa.force_count)
+                for (int comp = 0; comp < 3; ++comp) fa.force[fa.force_count][comp] = list[k]->data[comp];
+            const bool last = k >= list.size();
+            // Only the last launch packs; the SoA velocity is written when more
+            // launches follow or when no advection reads the packed copy.
+            fa.write_soa = (!last || !advect) ? 1 : 0;
+            fa.packed = (last && advect) ? c.packed : nullptr;
+            if (fa.force_count > 0 || fa.packed) ok(launch_force_pack(fa, c.stream));
+        } while (k < list.size());
+    }
+
+    // 2. advection (:617-619); skipped when alpha <= 0 because the reference
+    //    then never copies the advected velocity back (:623).
+    void advect_velocity() {
+        if (alpha_v() > 0.0f) ok(launch_advect_velocity(c.packed, c.temp[0], c.temp[1], c.temp[2], c.config.dt, c.dims, h(), c.flow, c.stream));
+    }
+
+    StencilArgs stencil(int kind, int init, int iterations, float coef, float* x, const float* b) {
+        StencilArgs a{};
+        a.kind = kind;
+        a.scheme = static_cast<int>(c.options.scheme);
+        a.init = init;
+        a.iterations = iterations;
+        a.per_pass = c.options.iterations_per_pass;
+        a.coef = coef;
+        a.out_scale = 1.0f;
+        a.x = x;
+        a.b = b;
+        a.scratch = c.scratch;
+        a.dims = c.dims;
+        a.flow = c.flow;
+        a.launches = &launches;
+        return a;
+    }
+
+    // 3. implicit viscosity, x0 = advected velocity (:621-641).
+    void diffuse_velocity() {
+        if (!(alpha_v() > 0.0f)) return;
+        for (int comp = 0; comp < 3; ++comp) ok(launch_stencil(stencil(KIND_VEL_X + comp, INIT_FROM_B, c.config.diffuse_iterations, alpha_v(), c.vel[comp], c.temp[comp]), c.stream), 0);
+    }
+
+    // 4. divergence (:643).
+    void divergence() { ok(launch_divergence(c.divergence, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.stream)); }
+
+    // 5. pressure from zero (:644-649) or from the previous step's pressure.
+    void pressure() {
+        const int init = c.options.warm_start == STABLE_FLUIDS_B200_WARM_START_PREVIOUS ? INIT_FROM_X : INIT_ZERO;
+        ok(launch_stencil(stencil(KIND_PRESSURE, init, c.config.pressure_iterations, h() * h(), c.pressure, c.divergence), c.stream), 0);
+    }
+
+    // 6. projection (:650) + the FP64 residual of the pressure solve.
+    void project() {
+        if (c.residual_enabled) ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, c.residual_enabled ? c.stats : nullptr, c.stream));
+        if (c.residual_enabled) ok(launch_residual_finalize(c.stats, c.dims, c.flow.any_outflow ? 0 : 1, c.config.pressure_iterations, c.stream));
+    }
+
+    // 7. scalars: source, advection by the projected velocity, diffusion,
+    //    dissipation (:652-668).
+    void scalars() {
+        for (auto& f : c.scalars) {
+            const float a_s = alpha_s(f);
+            const float factor = f.desc.dissipation > 0.0f ? 1.0f / (1.0f + c.config.dt * f.desc.dissipation) : 1.0f;  // :665
+            if (a_s > 0.0f) {
+                ok(launch_scalar_source_advect(c.packed, f.data, f.source, f.temp, c.config.dt, c.dims, h(), c.flow, f.bc, c.stream));
+                auto a = stencil(KIND_SCALAR, INIT_FROM_B, c.config.diffuse_iterations, a_s, f.data, f.temp);
+                a.scalar = f.bc;
+                a.out_scale = factor;
+                ok(launch_stencil(a, c.stream), 0);
+            } else {
+                ok(launch_scalar_source(f.data, f.source, c.config.dt, c.cells, c.stream));
+                if (f.desc.dissipation > 0.0f) ok(launch_scale(f.data, factor, c.cells, c.stream));
+            }
+        }
+    }
+
+    // 8. post-projection divergence and |u| (:670-671).
+    void diagnostics() { ok(launch_post_diagnostics(c.divergence, c.magnitude, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.stream)); }
+
+    cudaError_t whole_step() {
+        forces();
+        advect_velocity();
+        diffuse_velocity();
+        divergence();
+        pressure();
+        project();
+        scalars();
+        diagnostics();
+        return e;
+    }
+};
+
+StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const StableFluidsB200Options* options_in, bool env, void** out_context, StableFluidsScalarFieldHandle* out_s, uint32_t cap_s, StableFluidsVectorFieldHandle* out_v, uint32_t cap_v) {
+    Range range("stable.create_context");
+    if (out_context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    *out_context = nullptr;
+    if (desc == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const auto& cfg = desc->config;
+    if (cfg.nx <= 0 || cfg.ny <= 0 || cfg.nz <= 0) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (!(cfg.cell_size > 0.0f) || !std::isfinite(cfg.cell_size) || !std::isfinite(cfg.dt) || !std::isfinite(cfg.viscosity)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cfg.diffuse_iterations < 0 || cfg.pressure_iterations < 0) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (desc->scalar_field_count > 0 && desc->scalar_fields == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (desc->vector_field_count > 0 && desc->vector_fields == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (!validate_flow(cfg.flow_boundary)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    for (uint32_t i = 0; i < desc->scalar_field_count; ++i)
+        if (!validate_scalar(desc->scalar_fields[i].boundary)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+
+    StableFluidsB200Options options{};
+    if (options_in) options = *options_in;
+    else default_options(options);
+    if (env) apply_env_overrides(options);
+    if (!validate_options(options)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+
+    std::unique_ptr<Context> c{new (std::nothrow) Context{}};
+    if (!c) return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
+    c->config = cfg;
+    c->options = options;
+    c->dims = Dims{cfg.nx, cfg.ny, cfg.nz, 0};
+    c->cells = static_cast<size_t>(cfg.nx) * static_cast<size_t>(cfg.ny) * static_cast<size_t>(cfg.nz);
+    c->field_bytes = c->cells * sizeof(float);
+    c->flow = flatten(cfg.flow_boundary);
+    c->residual_enabled = options.compute_residual != 0 || options.residual_tolerance > 0.0f;
+
+    // Handles are 1-based indices (:544, :551).
+    for (uint32_t i = 0; i < desc->scalar_field_count; ++i) {
+        ScalarField f;
+        f.desc = desc->scalar_fields[i];
+        f.bc = flatten(f.desc.boundary);
+        c->scalars.push_back(f);
+        if (out_s != nullptr && i < cap_s) out_s[i] = i + 1u;
+    }
+    for (uint32_t i = 0; i < desc->vector_field_count; ++i) {
+        VectorField f;
+        f.desc = desc->vector_fields[i];
+        c->vectors.push_back(f);
+        if (out_v != nullptr && i < cap_v) out_v[i] = i + 1u;
+    }
+
+    if (desc->stream != nullptr) c->stream = static_cast<cudaStream_t>(desc->stream);
+    else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        c->owns_stream = true;
+    }
+
+    {
+        Range alloc("stable.create_context.alloc");
+        SlabPlan plan;
+        const size_t fb = c->field_bytes;
+        for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->vel[k]), fb);
+        for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->temp[k]), fb);
+        plan.add(&c->packed, c->cells * 4 * sizeof(float));
+        plan.add(reinterpret_cast<void**>(&c->pressure), fb);
+        plan.add(reinterpret_cast<void**>(&c->divergence), fb);
+        plan.add(reinterpret_cast<void**>(&c->magnitude), fb);
+        if (options.scheme == STABLE_FLUIDS_B200_SCHEME_JACOBI) plan.add(reinterpret_cast<void**>(&c->scratch), fb);
+        plan.add(reinterpret_cast<void**>(&c->stats), sizeof(DeviceStats));
+        for (auto& f : c->scalars) {
+            plan.add(reinterpret_cast<void**>(&f.data), fb);
+            plan.add(reinterpret_cast<void**>(&f.temp), fb);
+            plan.add(reinterpret_cast<void**>(&f.source), fb);
+        }
+        for (auto& f : c->vectors)
+            for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&f.data[k]), fb);
+        // Host-side fault injection for the OUT_OF_MEMORY path (tests only).
+        if (env_flag("STABLE_FLUIDS_B200_INJECT_ALLOC_FAILURE")) return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
+        c->slab_bytes = plan.total();
+        if (cudaMalloc(&c->slab, c->slab_bytes) != cudaSuccess) {
+            c->slab = nullptr;
+            cudaGetLastError();
+            return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
+        }
+        plan.assign(c->slab);
+        if (cudaMallocHost(reinterpret_cast<void**>(&c->host_stats), sizeof(DeviceStats)) != cudaSuccess) {
+            c->host_stats = nullptr;
+            cudaGetLastError();
+            return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
+        }
+        std::memset(c->host_stats, 0, sizeof(DeviceStats));
+        if (cudaEventCreateWithFlags(&c->ready, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+
+    {
+        // Initial values (:583-606): everything zero, then the non-zero
+        // scalar and vector initial values.
+        Range init("stable.create_context.init");
+        if (cudaMemsetAsync(c->slab, 0, c->slab_bytes, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        for (auto& f : c->scalars) {
+            if (f.desc.initial_value == 0.0f) continue;
+            if (launch_fill(f.data, f.desc.initial_value, c->cells, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+            if (launch_fill(f.temp, f.desc.initial_value, c->cells, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        }
+        for (auto& f : c->vectors) {
+            const float init[3] = {f.desc.initial_value_x, f.desc.initial_value_y, f.desc.initial_value_z};
+            for (int k = 0; k < 3; ++k)
+                if (init[k] != 0.0f && launch_fill(f.data[k], init[k], c->cells, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        }
+    }
+
+    {
+        // The whole step as one graph (:608-675). Thread-local capture so
+        // other host threads' CUDA calls are unaffected.
+        Range graph("stable.create_context.graph");
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        Stages st{*c};
+        const cudaError_t rec = st.whole_step();
+        c->step_kernels = st.launches;
+        cudaGraph_t g = nullptr;
+        const cudaError_t end = cudaStreamEndCapture(c->stream, &g);
+        c->graph = g;
+        if (rec != cudaSuccess || end != cudaSuccess || g == nullptr) {
+            cudaGetLastError();
+            return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        }
+        if (cudaGraphInstantiate(&c->exec, c->graph, 0) != cudaSuccess) {
+            c->exec = nullptr;
+            cudaGetLastError();
+            return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        }
+    }
+    if (cudaGetLastError() != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    *out_context = c.release();
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+ScalarField* scalar_field(Context& c, StableFluidsScalarFieldHandle h) {
+    if (h == 0 || h > c.scalars.size()) return nullptr;
+    return &c.scalars[h - 1u];
+}
+
+cudaError_t copy_or_zero(float* dst, const float* src, size_t bytes, cudaStream_t s) {
+    return src == nullptr ? cudaMemsetAsync(dst, 0, bytes, s) : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
+}
+
+}  // namespace
+}  // namespace sfb
+
+using sfb::Context;
+
+extern "C" {
+
+StableFluidsResult stable_fluids_create_context_cuda(const StableFluidsContextCreateDesc* desc, void** out_context, StableFluidsScalarFieldHandle* out_scalar_field_handles, uint32_t out_scalar_field_handle_capacity, StableFluidsVectorFieldHandle* out_vector_field_handles, uint32_t out_vector_field_handle_capacity) {
+    return sfb::create(desc, nullptr, true, out_context, out_scalar_field_handles, out_scalar_field_handle_capacity, out_vector_field_handles, out_vector_field_handle_capacity);
+}
+
+StableFluidsResult stable_fluids_b200_create_context(const StableFluidsContextCreateDesc* desc, const StableFluidsB200Options* options, void** out_context, StableFluidsScalarFieldHandle* out_scalar_field_handles, uint32_t out_scalar_field_handle_capacity, StableFluidsVectorFieldHandle* out_vector_field_handles, uint32_t out_vector_field_handle_capacity) {
+    return sfb::create(desc, options, false, out_context, out_scalar_field_handles, out_scalar_field_handle_capacity, out_vector_field_handles, out_vector_field_handle_capacity);
+}
+
+StableFluidsResult stable_fluids_b200_default_options(StableFluidsB200Options* options) {
+    if (options == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    sfb::default_options(*options);
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_destroy_context_cuda(void* context) {
+    sfb::Range range("stable.destroy_context");
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_OK;
+    auto* c = static_cast<Context*>(context);
+    if (c->stream) cudaStreamSynchronize(c->stream);  // :685
+    delete c;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_update_scalar_field_cuda(void* context, StableFluidsScalarFieldHandle field, const float* values) {
+    sfb::Range range("stable.update_scalar_field");
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    auto* f = sfb::scalar_field(c, field);
+    if (f == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    return sfb::copy_or_zero(f->data, values, c.field_bytes, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
+StableFluidsResult stable_fluids_update_scalar_field_source_cuda(void* context, StableFluidsScalarFieldHandle field, const float* values) {
+    sfb::Range range("stable.update_scalar_field_source");
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    auto* f = sfb::scalar_field(c, field);
+    if (f == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    return sfb::copy_or_zero(f->source, values, c.field_bytes, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
+StableFluidsResult stable_fluids_update_vector_field_cuda(void* context, StableFluidsVectorFieldHandle field, const float* values_x, const float* values_y, const float* values_z) {
+    sfb::Range range("stable.update_vector_field");
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    if (field == 0 || field > c.vectors.size()) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& f = c.vectors[field - 1u];
+    const float* src[3] = {values_x, values_y, values_z};
+    for (int k = 0; k < 3; ++k)
+        if (sfb::copy_or_zero(f.data[k], src[k], c.field_bytes, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_step_cuda(void* context) {
+    sfb::Range range("stable.step");
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    return cudaGraphLaunch(c.exec, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
+StableFluidsResult stable_fluids_get_view_cuda(void* context, const StableFluidsViewRequest* request, StableFluidsView* out_view) {
+    sfb::Range range("stable.get_view");
+    if (context == nullptr || request == nullptr || out_view == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    StableFluidsView v{};
+    v.layout = STABLE_FLUIDS_VIEW_LAYOUT_F32_3D;
+    v.nx = c.config.nx;
+    v.ny = c.config.ny;
+    v.nz = c.config.nz;
+    v.row_stride_bytes = static_cast<uint64_t>(c.config.nx) * sizeof(float);
+    v.slice_stride_bytes = static_cast<uint64_t>(c.config.nx) * static_cast<uint64_t>(c.config.ny) * sizeof(float);
+    switch (request->kind) {
+    case STABLE_FLUIDS_VIEW_SCALAR_FIELD_DATA:
+    case STABLE_FLUIDS_VIEW_SCALAR_FIELD_SOURCE: {
+        auto* f = sfb::scalar_field(c, request->scalar_field);
+        if (f == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        v.data0 = request->kind == STABLE_FLUIDS_VIEW_SCALAR_FIELD_DATA ? f->data : f->source;
+        break;
+    }
+    case STABLE_FLUIDS_VIEW_VECTOR_FIELD: {
+        if (request->vector_field == 0 || request->vector_field > c.vectors.size()) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        const auto& f = c.vectors[request->vector_field - 1u];
+        v.layout = STABLE_FLUIDS_VIEW_LAYOUT_F32_3D_SOA3;
+        v.data0 = f.data[0];
+        v.data1 = f.data[1];
+        v.data2 = f.data[2];
+        break;
+    }
+    case STABLE_FLUIDS_VIEW_FLOW_VELOCITY:
+        v.layout = STABLE_FLUIDS_VIEW_LAYOUT_F32_3D_SOA3;
+        v.data0 = c.vel[0];
+        v.data1 = c.vel[1];
+        v.data2 = c.vel[2];
+        break;
+    case STABLE_FLUIDS_VIEW_FLOW_VELOCITY_MAGNITUDE: v.data0 = c.magnitude; break;
+    case STABLE_FLUIDS_VIEW_FLOW_PRESSURE: v.data0 = c.pressure; break;
+    case STABLE_FLUIDS_VIEW_FLOW_DIVERGENCE: v.data0 = c.divergence; break;
+    default: return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;  // :799
+    }
+    *out_view = v;
+    // Order the consumer stream after the work queued so far (:743-759).
+    if (request->consumer_stream != nullptr && static_cast<cudaStream_t>(request->consumer_stream) != c.stream) {
+        if (cudaEventRecord(c.ready, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaStreamWaitEvent(static_cast<cudaStream_t>(request->consumer_stream), c.ready, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_get_step_stats(void* context, StableFluidsB200StepStats* out_stats) {
+    if (context == nullptr || out_stats == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    if (cudaMemcpyAsync(c.host_stats, c.stats, sizeof(sfb::DeviceStats), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaStreamSynchronize(c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const auto& d = *c.host_stats;
+    StableFluidsB200StepStats o{};
+    o.rel_residual = c.residual_enabled ? d.rel_residual : -1.0;
+    o.rhs_norm = c.residual_enabled ? d.rhs_norm : 0.0;
+    o.pressure_iterations = c.residual_enabled ? d.iterations : c.config.pressure_iterations;
+    o.hit_cap = d.hit_cap;
+    o.used_fallback = d.used_fallback;
+    *out_stats = o;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+StableFluidsResult stable_fluids_b200_enqueue_stage(void* context, uint32_t stage, int32_t* out_kernel_launches) {
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    sfb::Stages st{c};
+    switch (stage) {
+    case STABLE_FLUIDS_B200_STAGE_FORCES: st.forces(); break;
+    case STABLE_FLUIDS_B200_STAGE_VELOCITY_ADVECTION: st.advect_velocity(); break;
+    case STABLE_FLUIDS_B200_STAGE_VELOCITY_DIFFUSION: st.diffuse_velocity(); break;
+    case STABLE_FLUIDS_B200_STAGE_DIVERGENCE: st.divergence(); break;
+    case STABLE_FLUIDS_B200_STAGE_PRESSURE: st.pressure(); break;
+    case STABLE_FLUIDS_B200_STAGE_PROJECTION: st.project(); break;
+    case STABLE_FLUIDS_B200_STAGE_SCALARS: st.scalars(); break;
+    case STABLE_FLUIDS_B200_STAGE_DIAGNOSTICS: st.diagnostics(); break;
+    case STABLE_FLUIDS_B200_STAGE_STEP:
+        if (cudaGraphLaunch(c.exec, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        st.launches = c.step_kernels;
+        break;
+    default: return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    if (st.e != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (out_kernel_launches) *out_kernel_launches = st.launches;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_get_step_info(void* context, StableFluidsB200StepInfo* out_info) {
+    if (context == nullptr || out_info == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const auto& c = *static_cast<const Context*>(context);
+    StableFluidsB200StepInfo o{};
+    o.kernels_per_step = c.step_kernels;
+    o.device_bytes = c.slab_bytes;
+    o.scheme = c.options.scheme;
+    o.iterations_per_pass = c.options.iterations_per_pass;
+    *out_info = o;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,322 @@
+// sf_kernels.cu -- per-cell kernels of the step: force injection + velocity
+// packing, fused RK2 advection, divergence, projection with the FP64
+// residual, scalar source/advection, diagnostics.
+//
+// Layout in HBM: every field is a dense x-fastest FP32 array (the layout the
+// ABI views expose); velocity additionally has a packed float4 copy
+// (x, y, z, 0) that the advection gathers read with one 16-byte load per
+// interpolation corner.
+
+#include <cuda_runtime.h>
+
+#include "sf_device.cuh"
+#include "sf_launch.h"
+
+namespace sfb {
+
+namespace {
+
+constexpr int kBX = 32, kBY = 4, kBZ = 2;
+
+dim3 cell_block() { return dim3(kBX, kBY, kBZ); }
+dim3 cell_grid(const Dims& d) {
+    return dim3(static_cast<unsigned>((d.nx + kBX - 1) / kBX), static_cast<unsigned>((d.ny + kBY - 1) / kBY), static_cast<unsigned>((d.nz + kBZ - 1) / kBZ));
+}
+unsigned linear_grid(size_t n, int threads) {
+    size_t g = (n + static_cast<size_t>(threads) - 1) / static_cast<size_t>(threads);
+    const size_t cap = 148u * 32u;
+    return static_cast<unsigned>(g < cap ? (g == 0 ? 1 : g) : cap);
+}
+
+__device__ __forceinline__ bool cell_coords(const Dims& d, int& x, int& y, int& z) {
+    x = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
+    z = static_cast<int>(blockIdx.z * blockDim.z + threadIdx.z);
+    return x < d.nx && y < d.ny && z < d.nz;
+}
+
+// ------------------------------------------------------------------ fill --
+__global__ void k_fill(float* __restrict__ f, float value, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) f[i] = value;
+}
+
+// ------------------------------------------------------- force + packing --
+// v += dt * f for each force field in order (backend-cuda.cu:310-319 applied
+// field after field), then writes the packed float4 copy.
+__global__ void k_force_pack(ForceArgs a) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < a.n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        float vx = a.vel[0][i], vy = a.vel[1][i], vz = a.vel[2][i];
+        for (int k = 0; k < a.force_count; ++k) {
+            vx += a.dt * a.force[k][0][i];
+            vy += a.dt * a.force[k][1][i];
+            vz += a.dt * a.force[k][2][i];
+        }
+        if (a.write_soa) {
+            a.vel[0][i] = vx;
+            a.vel[1][i] = vy;
+            a.vel[2][i] = vz;
+        }
+        if (a.packed) static_cast<float4*>(a.packed)[i] = make_float4(vx, vy, vz, 0.0f);
+    }
+}
+
+// ------------------------------------------------------------- advection --
+// One RK2 trace per cell for all three components (the reference re-traces
+// per component, backend-cuda.cu:330-340; the trace is deterministic so the
+// results are identical), then a trilinear sample of the packed velocity.
+__global__ void __launch_bounds__(256) k_advect_velocity(const float4* __restrict__ v, float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz, float dt, Dims d, float h, FlowBC b) {
+    int x, y, z;
+    if (!cell_coords(d, x, y, z)) return;
+    const float px = (static_cast<float>(x) + 0.5f) * h;
+    const float py = (static_cast<float>(y) + 0.5f) * h;
+    const float pz = (static_cast<float>(z) + 0.5f) * h;
+    const float3 t = trace_rk2(px, py, pz, v, dt, d, h, b);
+    const float3 s = sample_velocity3(v, t.x, t.y, t.z, d, h, b);
+    const size_t i = lin(x, y, z, d);
+    ox[i] = s.x;
+    oy[i] = s.y;
+    oz[i] = s.z;
+}
+
+// Scalar value after the source injection rho + dt * S at an interior cell,
+// or the fixed face value (the source never reaches a ghost).
+__device__ __forceinline__ float sourced_scalar(const float* __restrict__ q, const float* __restrict__ src, float dt, int x, int y, int z, const Dims& d, const ScalarBC& b) {
+    if (!inside(x, y, z, d)) {
+        float value;
+        if (!scalar_resolve(x, y, z, d, b, value)) return value;
+    }
+    const size_t i = lin(x, y, z, d);
+    return __ldg(&q[i]) + dt * __ldg(&src[i]);
+}
+
+// Source injection fused into the advection gather (backend-cuda.cu:321-328
+// followed by :342-352): each gathered corner is rho + dt * S, exactly the
+// value the reference stores before it advects.
+__global__ void __launch_bounds__(256) k_scalar_source_advect(const float4* __restrict__ v, const float* __restrict__ q, const float* __restrict__ src, float* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) {
+    int x, y, z;
+    if (!cell_coords(d, x, y, z)) return;
+    const float px = (static_cast<float>(x) + 0.5f) * h;
+    const float py = (static_cast<float>(y) + 0.5f) * h;
+    const float pz = (static_cast<float>(z) + 0.5f) * h;
+    float3 t = trace_rk2(px, py, pz, v, dt, d, h, fb);
+    if (sb.periodic[0]) t.x = wrap_world(t.x, static_cast<float>(d.nx) * h);
+    if (sb.periodic[1]) t.y = wrap_world(t.y, static_cast<float>(d.ny) * h);
+    if (sb.periodic[2]) t.z = wrap_world(t.z, static_cast<float>(d.nz) * h);
+    const Cell c = locate(t.x, t.y, t.z, h);
+    float s[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, sb);
+    out[lin(x, y, z, d)] = trilerp(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], c);
+}
+
+__global__ void k_scalar_source(float* __restrict__ q, const float* __restrict__ src, float dt, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] += dt * src[i];
+}
+
+// backend-cuda.cu:377-384
+__global__ void k_scale(float* __restrict__ q, float factor, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = q[i] * factor;
+}
+
+// ------------------------------------------------------------ divergence --
+__device__ __forceinline__ float divergence_at(const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, int x, int y, int z, const Dims& d, float h, const FlowBC& b) {
+    const float inv_2h = 0.5f / h;
+    const float ddx = (load_velocity(vx, 0, x + 1, y, z, d, b) - load_velocity(vx, 0, x - 1, y, z, d, b)) * inv_2h;
+    const float ddy = (load_velocity(vy, 1, x, y + 1, z, d, b) - load_velocity(vy, 1, x, y - 1, z, d, b)) * inv_2h;
+    const float ddz = (load_velocity(vz, 2, x, y, z + 1, d, b) - load_velocity(vz, 2, x, y, z - 1, d, b)) * inv_2h;
+    return ddx + ddy + ddz;
+}
+
+// backend-cuda.cu:386-396
+__global__ void __launch_bounds__(256) k_divergence(float* __restrict__ div, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, Dims d, float h, FlowBC b) {
+    int x, y, z;
+    if (!cell_coords(d, x, y, z)) return;
+    div[lin(x, y, z, d)] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
+}
+
+// --------------------------------------------------- residual reductions --
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of four doubles, then one atomicAdd per value per block.
+__device__ __forceinline__ void block_accumulate4(double a, double b, double c, double e, DeviceStats* stats) {
+    __shared__ double part[4][32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    e = warp_sum(e);
+    if (lane == 0) {
+        part[0][warp] = a;
+        part[1][warp] = b;
+        part[2][warp] = c;
+        part[3][warp] = e;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (nthreads + 31) >> 5;
+        a = lane < nw ? part[0][lane] : 0.0;
+        b = lane < nw ? part[1][lane] : 0.0;
+        c = lane < nw ? part[2][lane] : 0.0;
+        e = lane < nw ? part[3][lane] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        c = warp_sum(c);
+        e = warp_sum(e);
+        if (lane == 0) {
+            atomicAdd(&stats->sum_e, a);
+            atomicAdd(&stats->sum_e2, b);
+            atomicAdd(&stats->sum_b, c);
+            atomicAdd(&stats->sum_b2, e);
+        }
+    }
+}
+
+// ------------------------------------------------------------ projection --
+// u -= central gradient of p (backend-cuda.cu:409-422, in place), repacks the
+// float4 velocity for the scalar advection, and (stats != nullptr) adds the
+// FP64 residual terms of A p = b: e = h^2 div - (sum6(p) - 6 p).
+__global__ void __launch_bounds__(256) k_project(float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz, float4* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) {
+    int x, y, z;
+    const bool ok = cell_coords(d, x, y, z);
+    double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
+    if (ok) {
+        const float inv_2h = 0.5f / h;
+        const size_t i = lin(x, y, z, d);
+        const float pxp = load_pressure(p, x + 1, y, z, d, b), pxm = load_pressure(p, x - 1, y, z, d, b);
+        const float pyp = load_pressure(p, x, y + 1, z, d, b), pym = load_pressure(p, x, y - 1, z, d, b);
+        const float pzp = load_pressure(p, x, y, z + 1, d, b), pzm = load_pressure(p, x, y, z - 1, d, b);
+        const float grad_x = (pxp - pxm) * inv_2h;
+        const float grad_y = (pyp - pym) * inv_2h;
+        const float grad_z = (pzp - pzm) * inv_2h;
+        const float ux = vx[i] - grad_x;
+        const float uy = vy[i] - grad_y;
+        const float uz = vz[i] - grad_z;
+        vx[i] = ux;
+        vy[i] = uy;
+        vz[i] = uz;
+        if (packed) packed[i] = make_float4(ux, uy, uz, 0.0f);
+        if (stats) {
+            const double nb = static_cast<double>(pxm) + static_cast<double>(pxp) + static_cast<double>(pym) + static_cast<double>(pyp) + static_cast<double>(pzm) + static_cast<double>(pzp);
+            const double bb = static_cast<double>(h2) * static_cast<double>(div[i]);
+            const double e = bb - (nb - 6.0 * static_cast<double>(p[i]));
+            se = e;
+            se2 = e * e;
+            sb = bb;
+            sb2 = bb * bb;
+        }
+    }
+    if (stats) block_accumulate4(se, se2, sb, sb2, stats);
+}
+
+__global__ void __launch_bounds__(256) k_residual_sums(const float* __restrict__ p, const float* __restrict__ div, Dims d, float h2, FlowBC b, DeviceStats* stats) {
+    int x, y, z;
+    const bool ok = cell_coords(d, x, y, z);
+    double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
+    if (ok) {
+        const size_t i = lin(x, y, z, d);
+        const double nb = static_cast<double>(load_pressure(p, x - 1, y, z, d, b)) + static_cast<double>(load_pressure(p, x + 1, y, z, d, b)) + static_cast<double>(load_pressure(p, x, y - 1, z, d, b)) + static_cast<double>(load_pressure(p, x, y + 1, z, d, b))
+                        + static_cast<double>(load_pressure(p, x, y, z - 1, d, b)) + static_cast<double>(load_pressure(p, x, y, z + 1, d, b));
+        const double bb = static_cast<double>(h2) * static_cast<double>(div[i]);
+        const double e = bb - (nb - 6.0 * static_cast<double>(p[i]));
+        se = e;
+        se2 = e * e;
+        sb = bb;
+        sb2 = bb * bb;
+    }
+    block_accumulate4(se, se2, sb, sb2, stats);
+}
+
+// rel_res = ||b - A p|| / ||b||, with b's mean removed when the pressure
+// operator is singular (no OUTFLOW face: constants are in its null space).
+__global__ void k_residual_finalize(DeviceStats* s, double n, int singular, int iterations) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double r2 = s->sum_e2, b2 = s->sum_b2;
+    if (singular) {
+        const double mb = s->sum_b / n;
+        r2 = s->sum_e2 - 2.0 * mb * s->sum_e + n * mb * mb;
+        b2 = s->sum_b2 - n * mb * mb;
+    }
+    r2 = r2 < 0.0 ? 0.0 : r2;
+    b2 = b2 < 0.0 ? 0.0 : b2;
+    s->rhs_norm = sqrt(b2);
+    s->rel_residual = b2 > 0.0 ? sqrt(r2) / sqrt(b2) : 0.0;
+    if (iterations >= 0) s->iterations = iterations;
+}
+
+// ----------------------------------------------------------- diagnostics --
+// Post-projection divergence (backend-cuda.cu:670) and |u| (:424-434) in one pass.
+__global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, Dims d, float h, FlowBC b) {
+    int x, y, z;
+    if (!cell_coords(d, x, y, z)) return;
+    const size_t i = lin(x, y, z, d);
+    div[i] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
+    const float ux = vx[i], uy = vy[i], uz = vz[i];
+    mag[i] = sqrtf(ux * ux + uy * uy + uz * uz);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers --
+cudaError_t launch_fill(float* f, float value, size_t n, cudaStream_t s) {
+    k_fill<<<linear_grid(n, 256), 256, 0, s>>>(f, value, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_force_pack(const ForceArgs& a, cudaStream_t s) {
+    k_force_pack<<<linear_grid(a.n, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advect_velocity(const void* packed, float* ox, float* oy, float* oz, float dt, Dims d, float h, const FlowBC& b, cudaStream_t s) {
+    k_advect_velocity<<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const float4*>(packed), ox, oy, oz, dt, d, h, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scalar_source_advect(const void* packed, const float* data, const float* source, float* out, float dt, Dims d, float h, const FlowBC& fb, const ScalarBC& sb, cudaStream_t s) {
+    k_scalar_source_advect<<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const float4*>(packed), data, source, out, dt, d, h, fb, sb);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scalar_source(float* data, const float* source, float dt, size_t n, cudaStream_t s) {
+    k_scalar_source<<<linear_grid(n, 256), 256, 0, s>>>(data, source, dt, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale(float* data, float factor, size_t n, cudaStream_t s) {
+    k_scale<<<linear_grid(n, 256), 256, 0, s>>>(data, factor, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_divergence(float* div, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s) {
+    k_divergence<<<cell_grid(d), cell_block(), 0, s>>>(div, vx, vy, vz, d, h, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project(float* vx, float* vy, float* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
+    k_project<<<cell_grid(d), cell_block(), 0, s>>>(vx, vy, vz, static_cast<float4*>(packed), p, div, d, h, h2, b, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
+    k_residual_sums<<<cell_grid(d), cell_block(), 0, s>>>(p, div, d, h2, b, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_finalize(DeviceStats* stats, Dims d, int singular, int iterations, cudaStream_t s) {
+    const double n = static_cast<double>(d.nx) * static_cast<double>(d.ny) * static_cast<double>(d.nz);
+    k_residual_finalize<<<1, 32, 0, s>>>(stats, n, singular, iterations);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post_diagnostics(float* div, float* mag, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s) {
+    k_post_diagnostics<<<cell_grid(d), cell_block(), 0, s>>>(div, mag, vx, vy, vz, d, h, b);
+    return cudaGetLastError();
+}
+
+}  // namespace sfb

@@ -1,0 +1,189 @@
+"""`Simulation`: one stable-fluids context driven through the C ABI.
+
+Field arrays are shaped (nz, ny, nx) -- x fastest, the ABI's dense layout.
+Inputs may be numpy arrays (copied to the device on the simulation's stream
+first, since the upstream ABI takes device pointers), CUDA torch tensors, or
+None (zero-fill, as the ABI defines for a null pointer).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_uint32, c_void_p
+
+import numpy as np
+
+from . import (
+    RESULT_OK,
+    VIEW_FLOW_VELOCITY,
+    VIEW_VECTOR_FIELD,
+    B200Options,
+    B200StepInfo,
+    B200StepStats,
+    ContextCreateDesc,
+    ScalarFieldDesc,
+    SimulationConfig,
+    VectorFieldDesc,
+    View,
+    ViewRequest,
+    load_library,
+)
+
+
+class StableFluidsError(RuntimeError):
+    def __init__(self, what: str, code: int):
+        super().__init__(f"{what} failed with StableFluidsResult {code}")
+        self.code = code
+
+
+class _DeviceArray:
+    """Zero-copy handle on library-owned device memory for torch.as_tensor."""
+
+    def __init__(self, ptr: int, shape: tuple[int, ...]):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (int(ptr), True), "version": 3, "strides": None, "stream": None}
+
+
+class Simulation:
+    def __init__(self, config: SimulationConfig, scalar_fields=(), vector_fields=(), *, lib=None, options: B200Options | None = None, device: int = 0):
+        import torch
+
+        self._torch = torch
+        self.lib = lib if lib is not None else load_library()
+        self.config = config
+        self.shape = (config.nz, config.ny, config.nx)
+        self.cells = config.nx * config.ny * config.nz
+        self.device = torch.device("cuda", device)
+        self.stream = torch.cuda.Stream(device=self.device)
+        self._keep: list = []
+        self._scalars = (ScalarFieldDesc * max(1, len(scalar_fields)))(*scalar_fields)
+        self._vectors = (VectorFieldDesc * max(1, len(vector_fields)))(*vector_fields)
+        desc = ContextCreateDesc(
+            config=config,
+            stream=c_void_p(self.stream.cuda_stream),
+            scalar_fields=ctypes.cast(self._scalars, ctypes.POINTER(ScalarFieldDesc)),
+            scalar_field_count=len(scalar_fields),
+            vector_fields=ctypes.cast(self._vectors, ctypes.POINTER(VectorFieldDesc)),
+            vector_field_count=len(vector_fields),
+        )
+        self._desc = desc
+        hs = (c_uint32 * max(1, len(scalar_fields)))()
+        hv = (c_uint32 * max(1, len(vector_fields)))()
+        ctx = c_void_p()
+        with torch.cuda.device(self.device):
+            if options is not None:
+                if not getattr(self.lib, "_sf_extended", False):
+                    raise ValueError("this library has no stable_fluids_b200_create_context")
+                rc = self.lib.stable_fluids_b200_create_context(byref(desc), byref(options), byref(ctx), hs, len(scalar_fields), hv, len(vector_fields))
+            else:
+                rc = self.lib.stable_fluids_create_context_cuda(byref(desc), byref(ctx), hs, len(scalar_fields), hv, len(vector_fields))
+        if rc != RESULT_OK:
+            raise StableFluidsError("stable_fluids_create_context", rc)
+        self.ctx = ctx
+        self.scalar_handles = [hs[i] for i in range(len(scalar_fields))]
+        self.vector_handles = [hv[i] for i in range(len(vector_fields))]
+
+    # ----------------------------------------------------------- inputs --
+    def _device_ptr(self, values):
+        if values is None:
+            return None
+        torch = self._torch
+        if isinstance(values, torch.Tensor):
+            t = values
+            if t.device != self.device or t.dtype != torch.float32 or not t.is_contiguous():
+                with torch.cuda.stream(self.stream):
+                    t = t.to(self.device, torch.float32).contiguous()
+        else:
+            a = np.ascontiguousarray(values, dtype=np.float32)
+            with torch.cuda.stream(self.stream):
+                t = torch.from_numpy(a).to(self.device, non_blocking=False)
+        if t.numel() != self.cells:
+            raise ValueError(f"field has {t.numel()} values, grid has {self.cells}")
+        self._keep.append(t)
+        return t.data_ptr()
+
+    def _check(self, rc: int, what: str):
+        if rc != RESULT_OK:
+            raise StableFluidsError(what, rc)
+
+    def set_scalar(self, handle: int, values):
+        self._check(self.lib.stable_fluids_update_scalar_field_cuda(self.ctx, handle, self._device_ptr(values)), "update_scalar_field")
+
+    def set_scalar_source(self, handle: int, values):
+        self._check(self.lib.stable_fluids_update_scalar_field_source_cuda(self.ctx, handle, self._device_ptr(values)), "update_scalar_field_source")
+
+    def set_vector(self, handle: int, x, y, z):
+        px, py, pz = self._device_ptr(x), self._device_ptr(y), self._device_ptr(z)
+        self._check(self.lib.stable_fluids_update_vector_field_cuda(self.ctx, handle, px, py, pz), "update_vector_field")
+
+    # ------------------------------------------------------------- step --
+    def step(self, n: int = 1):
+        for _ in range(n):
+            self._check(self.lib.stable_fluids_step_cuda(self.ctx), "step")
+
+    def synchronize(self):
+        self.stream.synchronize()
+        self._keep.clear()
+
+    # ---------------------------------------------------------- outputs --
+    def raw_view(self, kind: int, handle: int = 0) -> View:
+        req = ViewRequest(kind=kind, scalar_field=handle if kind in (0, 1) else 0, vector_field=handle if kind == VIEW_VECTOR_FIELD else 0, consumer_stream=c_void_p(self.stream.cuda_stream))
+        v = View()
+        self._check(self.lib.stable_fluids_get_view_cuda(self.ctx, byref(req), byref(v)), "get_view")
+        return v
+
+    def view(self, kind: int, handle: int = 0):
+        """Zero-copy torch tensors on the library's memory (valid until the
+        next step); a tuple of three for the vector layouts."""
+        torch = self._torch
+        v = self.raw_view(kind, handle)
+        shape = (v.nz, v.ny, v.nx)
+        ts = [torch.as_tensor(_DeviceArray(p, shape), device=self.device) for p in (v.data0, v.data1, v.data2) if p]
+        return tuple(ts) if kind in (VIEW_FLOW_VELOCITY, VIEW_VECTOR_FIELD) else ts[0]
+
+    def fetch(self, kind: int, handle: int = 0):
+        """Host copies (numpy float32, shape (nz, ny, nx)) of a view."""
+        torch = self._torch
+        v = self.view(kind, handle)
+        with torch.cuda.stream(self.stream):
+            if isinstance(v, tuple):
+                out = tuple(t.clone() for t in v)
+            else:
+                out = v.clone()
+        self.stream.synchronize()
+        if isinstance(out, tuple):
+            return tuple(t.cpu().numpy() for t in out)
+        return out.cpu().numpy()
+
+    def stats(self) -> B200StepStats:
+        s = B200StepStats()
+        self._check(self.lib.stable_fluids_b200_get_step_stats(self.ctx, byref(s)), "get_step_stats")
+        return s
+
+    def info(self) -> B200StepInfo:
+        i = B200StepInfo()
+        self._check(self.lib.stable_fluids_b200_get_step_info(self.ctx, byref(i)), "get_step_info")
+        return i
+
+    def enqueue_stage(self, stage: int) -> int:
+        """Enqueues one stage outside the step graph; returns its kernel count."""
+        n = ctypes.c_int32(0)
+        self._check(self.lib.stable_fluids_b200_enqueue_stage(self.ctx, stage, byref(n)), "enqueue_stage")
+        return n.value
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.stable_fluids_destroy_context_cuda(self.ctx)
+            self.ctx = None
+        self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

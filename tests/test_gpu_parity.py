@@ -1,0 +1,207 @@
+"""Parity of libstable-fluids.so (through the C ABI) against the CPU oracle and
+against the reference library itself, on the GPU.
+
+Error measure: max |a - b| / max(|b|, FLOOR * max|b|) over every cell of
+every output field (velocity x/y/z, pressure, divergence, |u|, each scalar).
+"""
+
+import numpy as np
+import pytest
+
+from tests.golden import cases as C
+
+# Against the reference library (same CUDA compiler, same expression shapes,
+# same FP32 arithmetic): within 1e-5 relative, floor 1e-3 of the field scale.
+REF_TOL, REF_FLOOR = 1e-5, 1e-3
+# Against the FP32 CPU oracle (fused multiply-adds placed by hand, so a few
+# roundings may differ and grow over the steps): 1e-4 relative, same floor.
+ORACLE_TOL, ORACLE_FLOOR = 1e-4, 1e-3
+
+CASES = {c.name: c for c in C.build_cases()}
+
+
+def run_lib(sf, lib, case, steps=None, options=None):
+    sim = sf.Simulation(case.config, case.scalars, case.vectors, lib=lib, options=options)
+    case.drive(sim, steps)
+    out = C.collect_outputs(sim, sf, case)
+    sim.close()
+    return out
+
+
+def run_oracle(orc, case, steps=None, scheme=0, precision=32, **solver):
+    o = orc.Oracle(case.config, case.scalars, case.vectors, precision=precision, scheme=scheme)
+    if solver:
+        o.set_solver(**solver)
+    case.drive(o, steps)
+    out = C.collect_oracle(o, orc, case)
+    return out, o
+
+
+def errors(a, b, floor):
+    return {k: C.max_rel_err(a[k], b[k], floor) for k in b}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_rbgs_matches_reference_library(name, sf, lib, ref_lib, cuda):
+    case = CASES[name]
+    ours = run_lib(sf, lib, case)
+    ref = run_lib(sf, ref_lib, case)
+    err = errors(ours, ref, REF_FLOOR)
+    assert max(err.values()) <= REF_TOL, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_rbgs_matches_oracle(name, sf, lib, orc, cuda):
+    case = CASES[name]
+    ours = run_lib(sf, lib, case)
+    ref, _ = run_oracle(orc, case)
+    err = errors(ours, ref, ORACLE_FLOOR)
+    assert max(err.values()) <= ORACLE_TOL, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_jacobi_matches_oracle(name, sf, lib, orc, cuda):
+    case = CASES[name]
+    opts = sf.default_options(lib)
+    opts.scheme = sf.SCHEME_JACOBI
+    ours = run_lib(sf, lib, case, options=opts)
+    ref, _ = run_oracle(orc, case, scheme=orc.JACOBI)
+    err = errors(ours, ref, ORACLE_FLOOR)
+    assert max(err.values()) <= ORACLE_TOL, err
+
+
+@pytest.mark.gpu
+def test_config0_100_steps_matches_reference(sf, lib, ref_lib, cuda):
+    """The 64^3 Stam-walls plume, 100 steps, against the reference library."""
+    scene = sf.scenes.config0()
+    outs = []
+    for L in (lib, ref_lib):
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=L)
+        sf.scenes.run(sim, scene)
+        case = C.Case("config0", scene.config, scene.scalars, scene.vectors, scene.steps)
+        outs.append(C.collect_outputs(sim, sf, case))
+        sim.close()
+    err = errors(outs[0], outs[1], REF_FLOOR)
+    assert max(err.values()) <= REF_TOL, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("warm", [False, True])
+def test_residual_matches_oracle(warm, sf, lib, orc, cuda):
+    case = CASES["walls_16x12x10"]
+    opts = sf.default_options(lib)
+    opts.compute_residual = 1
+    opts.warm_start = sf.WARM_START_PREVIOUS if warm else sf.WARM_START_ZERO
+    sim = sf.Simulation(case.config, case.scalars, case.vectors, lib=lib, options=opts)
+    case.drive(sim)
+    st = sim.stats()
+    p = sim.fetch(sf.VIEW_FLOW_PRESSURE)
+    sim.close()
+    ref, o = run_oracle(orc, case, warm_previous=warm, compute_residual=True)
+    ost = o.stats()
+    assert st.pressure_iterations == case.config.pressure_iterations
+    assert abs(st.rel_residual - ost["rel_residual"]) <= 1e-4 * ost["rel_residual"] + 1e-7, (st.rel_residual, ost)
+    assert abs(st.rhs_norm - ost["rhs_norm"]) <= 1e-4 * ost["rhs_norm"]
+    assert C.max_rel_err(p, ref["pressure"], ORACLE_FLOOR) <= ORACLE_TOL
+
+
+@pytest.mark.gpu
+def test_abi_error_paths(sf, lib, cuda):
+    import ctypes
+
+    case = CASES["walls_16x12x10"]
+    sim = sf.Simulation(case.config, case.scalars, case.vectors, lib=lib)
+    ctx = sim.ctx
+    # bad handles (upstream :695, :704, :713, :762)
+    assert lib.stable_fluids_update_scalar_field_cuda(ctx, 0, None) == sf.RESULT_BACKEND_FAILURE
+    assert lib.stable_fluids_update_scalar_field_cuda(ctx, 2, None) == sf.RESULT_BACKEND_FAILURE
+    assert lib.stable_fluids_update_scalar_field_source_cuda(ctx, 7, None) == sf.RESULT_BACKEND_FAILURE
+    assert lib.stable_fluids_update_vector_field_cuda(ctx, 0, None, None, None) == sf.RESULT_BACKEND_FAILURE
+    req = sf.ViewRequest(kind=99)
+    v = sf.View()
+    assert lib.stable_fluids_get_view_cuda(ctx, ctypes.byref(req), ctypes.byref(v)) == sf.RESULT_BACKEND_FAILURE
+    req = sf.ViewRequest(kind=sf.VIEW_SCALAR_FIELD_DATA, scalar_field=5)
+    assert lib.stable_fluids_get_view_cuda(ctx, ctypes.byref(req), ctypes.byref(v)) == sf.RESULT_BACKEND_FAILURE
+    assert lib.stable_fluids_step_cuda(None) == sf.RESULT_BACKEND_FAILURE
+    assert lib.stable_fluids_get_view_cuda(None, ctypes.byref(req), ctypes.byref(v)) == sf.RESULT_BACKEND_FAILURE
+    # null pointer = zero fill (upstream :697)
+    assert lib.stable_fluids_update_scalar_field_cuda(ctx, 1, None) == sf.RESULT_OK
+    assert not sim.fetch(sf.VIEW_SCALAR_FIELD_DATA, 1).any()
+    # views are dense, x-fastest (upstream :732-742)
+    v = sim.raw_view(sf.VIEW_FLOW_VELOCITY)
+    assert v.layout == sf.VIEW_LAYOUT_F32_3D_SOA3 and v.row_stride_bytes == 4 * v.nx and v.slice_stride_bytes == 4 * v.nx * v.ny
+    assert sim.raw_view(sf.VIEW_FLOW_PRESSURE).layout == sf.VIEW_LAYOUT_F32_3D
+    sim.close()
+    assert lib.stable_fluids_destroy_context_cuda(None) == sf.RESULT_OK
+
+
+def _create_rc(sf, lib, cfg, scalars=(), vectors=()):
+    import ctypes
+
+    sa = (sf.ScalarFieldDesc * max(1, len(scalars)))(*scalars)
+    va = (sf.VectorFieldDesc * max(1, len(vectors)))(*vectors)
+    desc = sf.ContextCreateDesc(config=cfg, stream=None, scalar_fields=ctypes.cast(sa, ctypes.POINTER(sf.ScalarFieldDesc)), scalar_field_count=len(scalars), vector_fields=ctypes.cast(va, ctypes.POINTER(sf.VectorFieldDesc)), vector_field_count=len(vectors))
+    ctx = ctypes.c_void_p()
+    rc = lib.stable_fluids_create_context_cuda(ctypes.byref(desc), ctypes.byref(ctx), None, 0, None, 0)
+    if rc == sf.RESULT_OK:
+        lib.stable_fluids_destroy_context_cuda(ctx)
+    return rc
+
+
+@pytest.mark.gpu
+def test_create_validation(sf, lib, cuda):
+    sc = sf.scenes
+    good = sc.make_config((8, 8, 8), 0.125, 0.1, 1e-4, 2, 2, sc.stam_walls()[0])
+    assert _create_rc(sf, lib, good) == sf.RESULT_OK
+    # unpaired periodic face (upstream :519)
+    bad = sc.make_config((8, 8, 8), 0.125, 0.1, 1e-4, 2, 2, sc.flow_boundary([sf.FLOW_PERIODIC, sf.FLOW_FREE_SLIP_WALL] + [sf.FLOW_FREE_SLIP_WALL] * 4))
+    assert _create_rc(sf, lib, bad) == sf.RESULT_BACKEND_FAILURE
+    # unknown kind (upstream :517)
+    bad = sc.make_config((8, 8, 8), 0.125, 0.1, 1e-4, 2, 2, sc.flow_boundary([7] + [sf.FLOW_FREE_SLIP_WALL] * 5))
+    assert _create_rc(sf, lib, bad) == sf.RESULT_BACKEND_FAILURE
+    # scalar periodic unpaired (upstream :524)
+    s = sf.ScalarFieldDesc(0, 0, 0, sc.scalar_boundary([sf.SCALAR_PERIODIC] + [sf.SCALAR_ZERO_FLUX] * 5))
+    assert _create_rc(sf, lib, good, [s]) == sf.RESULT_BACKEND_FAILURE
+    # stricter than upstream: empty grid, non-positive cell size, negative iterations
+    assert _create_rc(sf, lib, sc.make_config((0, 8, 8), 0.125, 0.1, 1e-4, 2, 2, sc.stam_walls()[0])) == sf.RESULT_BACKEND_FAILURE
+    assert _create_rc(sf, lib, sc.make_config((8, 8, 8), 0.0, 0.1, 1e-4, 2, 2, sc.stam_walls()[0])) == sf.RESULT_BACKEND_FAILURE
+    assert _create_rc(sf, lib, sc.make_config((8, 8, 8), 0.125, 0.1, 1e-4, -1, 2, sc.stam_walls()[0])) == sf.RESULT_BACKEND_FAILURE
+
+
+@pytest.mark.gpu
+def test_out_of_memory_paths(sf, lib, cuda, monkeypatch):
+    sc = sf.scenes
+    # host-side fault injection: the allocation reports failure
+    monkeypatch.setenv("STABLE_FLUIDS_B200_INJECT_ALLOC_FAILURE", "1")
+    good = sc.make_config((8, 8, 8), 0.125, 0.1, 1e-4, 2, 2, sc.stam_walls()[0])
+    assert _create_rc(sf, lib, good) == sf.RESULT_OUT_OF_MEMORY
+    monkeypatch.delenv("STABLE_FLUIDS_B200_INJECT_ALLOC_FAILURE")
+    # a real allocation larger than the device: 4096^3 cells x 15 fields
+    huge = sc.make_config((4096, 4096, 4096), 1.0 / 4096, 0.1, 1e-4, 2, 2, sc.stam_walls()[0])
+    assert _create_rc(sf, lib, huge) == sf.RESULT_OUT_OF_MEMORY
+    assert _create_rc(sf, lib, good) == sf.RESULT_OK  # the device is still usable
+
+
+@pytest.mark.gpu
+def test_views_and_consumer_stream(sf, lib, cuda):
+    torch = cuda
+    case = CASES["benchmark_walls_16x12x16"]
+    sim = sf.Simulation(case.config, case.scalars, case.vectors, lib=lib)
+    case.drive(sim)
+    consumer = torch.cuda.Stream()
+    import ctypes
+
+    req = sf.ViewRequest(kind=sf.VIEW_SCALAR_FIELD_SOURCE, scalar_field=2, consumer_stream=ctypes.c_void_p(consumer.cuda_stream))
+    v = sf.View()
+    assert lib.stable_fluids_get_view_cuda(sim.ctx, ctypes.byref(req), ctypes.byref(v)) == sf.RESULT_OK
+    t = torch.as_tensor(sf.simulation._DeviceArray(v.data0, case.shape), device="cuda")
+    with torch.cuda.stream(consumer):
+        got = t.clone()
+    consumer.synchronize()
+    np.testing.assert_array_equal(got.cpu().numpy(), case.sources[2])
+    fx, fy, fz = sim.fetch(sf.VIEW_VECTOR_FIELD, 2)
+    np.testing.assert_array_equal(fx, case.forces[2][0])
+    sim.close()
