@@ -80,6 +80,7 @@ struct Context {
     cudaEvent_t ready = nullptr;
     bool residual_enabled = false;
     int step_kernels = 0;  // kernel nodes in the step graph
+    bool blocked = true;   // temporally blocked stencil passes
 
     ~Context() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -273,6 +274,8 @@ struct Stages {
         a.dims = c.dims;
         a.flow = c.flow;
         a.launches = &launches;
+        a.blocked = c.blocked ? 1 : 0;
+        a.error_flag = &c.stats->error;
         return a;
     }
 
@@ -363,6 +366,7 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
     c->field_bytes = c->cells * sizeof(float);
     c->flow = flatten(cfg.flow_boundary);
     c->residual_enabled = options.compute_residual != 0 || options.residual_tolerance > 0.0f;
+    c->blocked = !env_flag("STABLE_FLUIDS_B200_UNBLOCKED_STENCIL");
 
     // Handles are 1-based indices (:544, :551).
     for (uint32_t i = 0; i < desc->scalar_field_count; ++i) {
@@ -395,7 +399,7 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         plan.add(reinterpret_cast<void**>(&c->pressure), fb);
         plan.add(reinterpret_cast<void**>(&c->divergence), fb);
         plan.add(reinterpret_cast<void**>(&c->magnitude), fb);
-        if (options.scheme == STABLE_FLUIDS_B200_SCHEME_JACOBI) plan.add(reinterpret_cast<void**>(&c->scratch), fb);
+        plan.add(reinterpret_cast<void**>(&c->scratch), fb);
         plan.add(reinterpret_cast<void**>(&c->stats), sizeof(DeviceStats));
         for (auto& f : c->scalars) {
             plan.add(reinterpret_cast<void**>(&f.data), fb);

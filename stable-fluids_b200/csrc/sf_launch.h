@@ -41,6 +41,8 @@ struct StencilArgs {
     FlowBC flow;
     ScalarBC scalar;
     int* launches;       // incremented by the number of kernels enqueued (may be null)
+    int blocked;         // 1: temporally blocked passes where supported; 0: one launch per sweep
+    unsigned* error_flag;  // device word a kernel sets when a bounded wait gives up
 };
 
 cudaError_t launch_fill(float* f, float value, size_t n, cudaStream_t s);

@@ -9,10 +9,15 @@
 // RBGS updates (x+y+z) even cells, then odd ones, in place; JACOBI updates
 // every cell from the previous iterate.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <climits>
 
 #include "sf_device.cuh"
 #include "sf_launch.h"
+#include "sf_stencil_tb.cuh"
 
 namespace sfb {
 
@@ -123,9 +128,168 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
     return e;
 }
 
+
+// ------------------------------------------------ temporally blocked path --
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// 3D map over a dense x-fastest FP32 field with a W x HH x 1 box.
+bool plane_map(CUtensorMap* m, const float* base, const Dims& d, int w, int hh) {
+    auto encode = tensor_map_encoder();
+    if (encode == nullptr || base == nullptr) return false;
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(d.nx), static_cast<cuuint64_t>(d.ny), static_cast<cuuint64_t>(d.nz)};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(d.nx) * 4u, static_cast<cuuint64_t>(d.nx) * static_cast<cuuint64_t>(d.ny) * 4u};
+    const cuuint32_t box[3] = {static_cast<cuuint32_t>(w), static_cast<cuuint32_t>(hh), 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Face ghost rules of a field kind, from the flattened boundary (the same
+// rules as load_pressure / load_scalar / load_velocity for a face neighbour).
+GhostRule ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb) {
+    GhostRule g{};
+    for (int f = 0; f < 6; ++f) {
+        const int axis = f / 2;
+        if (kind == KIND_PRESSURE) {
+            g.mode[f] = fb.type[f] == STABLE_FLUIDS_FLOW_BOUNDARY_OUTFLOW ? GHOST_CONST : GHOST_COPY;
+            g.k[f] = fb.pressure[f];
+        } else if (kind == KIND_SCALAR) {
+            g.mode[f] = sb.type[f] == STABLE_FLUIDS_SCALAR_BOUNDARY_FIXED_VALUE ? GHOST_CONST : GHOST_COPY;
+            g.k[f] = sb.value[f];
+        } else {
+            const int comp = kind;
+            const bool copy = fb.type[f] == STABLE_FLUIDS_FLOW_BOUNDARY_OUTFLOW || (fb.type[f] == STABLE_FLUIDS_FLOW_BOUNDARY_FREE_SLIP_WALL && comp != axis);
+            g.mode[f] = copy ? GHOST_COPY : GHOST_REFLECT;
+            g.k[f] = 2.0f * fb.vel[f][comp];
+        }
+    }
+    for (int a = 0; a < 3; ++a) g.periodic[a] = kind == KIND_SCALAR ? sb.periodic[a] : fb.periodic[a];
+    return g;
+}
+
+struct TbShape {
+    int k, w, hh, nt, ctas_per_sm;
+};
+
+template <int KIND, int K, int W, int HH, int NT>
+cudaError_t launch_tb_pass(const TbArgs& args, const CUtensorMap& mx, const CUtensorMap& mb, int z_chunk, cudaStream_t s) {
+    constexpr int D = tb::kPrefetch;
+    constexpr size_t smem = static_cast<size_t>((K + D + 2) + (K + D + 1)) * W * HH * 4 + (D + 1) * 8;
+    auto kern = k_rbgs_tb<KIND, K, W, HH, NT>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (attr != cudaSuccess) return attr;
+    constexpr int HX = ((K + 3) / 4) * 4;
+    const dim3 grid(static_cast<unsigned>((args.d.nx + W - 2 * HX - 1) / (W - 2 * HX)), static_cast<unsigned>((args.d.ny + HH - 2 * K - 1) / (HH - 2 * K)), static_cast<unsigned>((args.d.nz + z_chunk - 1) / z_chunk));
+    kern<<<grid, NT, smem, s>>>(mx, mb, args);
+    return cudaGetLastError();
+}
+
+// Planes per CTA: minimise (waves x streamed planes per CTA).
+int choose_z_chunk(const Dims& d, int tiles_xy, int k, int ctas_per_sm) {
+    const int slots = 148 * ctas_per_sm;
+    int best = d.nz;
+    long long best_cost = LLONG_MAX;
+    for (int c = 1; c <= d.nz; ++c) {
+        const int z = (d.nz + c - 1) / c;
+        if ((c - 1) * z >= d.nz) continue;
+        const long long waves = (static_cast<long long>(tiles_xy) * c + slots - 1) / slots;
+        const long long cost = waves * (z + 2 * k);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = z;
+        }
+    }
+    return best;
+}
+
+constexpr TbShape kTbShape{4, 96, 32, 384, 1};
+
+template <int KIND>
+cudaError_t run_tb(const StencilArgs& a, cudaStream_t s, unsigned* error_flag) {
+    constexpr int K = 4, W = 96, HH = 32, NT = 384;
+    const Dims& d = a.dims;
+    const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
+    const size_t bytes = n * sizeof(float);
+    const int per_pass = a.per_pass > 0 ? (a.per_pass < K / 2 ? a.per_pass : K / 2) : K / 2;
+    cudaError_t e = cudaSuccess;
+    if (a.iterations == 0) {
+        if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
+        else if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(a.x, a.b, bytes, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+        if (a.out_scale != 1.0f) {
+            k_scale_field<<<148u * 32u, 256, 0, s>>>(a.x, a.out_scale, n);
+            if (a.launches) *a.launches += 1;
+            return cudaGetLastError();
+        }
+        return cudaSuccess;
+    }
+    TbArgs t{};
+    t.b = a.b;
+    t.coef = a.coef;
+    t.d = d;
+    t.g = ghost_rule(a.kind, a.flow, a.scalar);
+    t.error = error_flag;
+    const bool aligned = d.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(a.x) & 15) == 0 && (reinterpret_cast<uintptr_t>(a.scratch) & 15) == 0 && (reinterpret_cast<uintptr_t>(a.b) & 15) == 0;
+    CUtensorMap map_b{}, map_x{}, map_s{};
+    t.tma_ok = aligned && plane_map(&map_b, a.b, d, W, HH) && plane_map(&map_x, a.x, d, W, HH) && plane_map(&map_s, a.scratch, d, W, HH);
+    constexpr int HX = ((K + 3) / 4) * 4;
+    const int tiles_xy = ((d.nx + W - 2 * HX - 1) / (W - 2 * HX)) * ((d.ny + HH - 2 * K - 1) / (HH - 2 * K));
+    const int passes = (a.iterations + per_pass - 1) / per_pass;
+    const float* src = a.init == INIT_ZERO ? nullptr : (a.init == INIT_FROM_B ? a.b : a.x);
+    const CUtensorMap* src_map = a.init == INIT_FROM_B ? &map_b : &map_x;
+    for (int i = 0; i < passes; ++i) {
+        float* dst = ((passes - 1 - i) % 2 == 0) ? a.x : a.scratch;
+        const CUtensorMap* dst_map = dst == a.x ? &map_x : &map_s;
+        if (src == dst) {  // warm start from x with an odd pass count: move it aside
+            if ((e = cudaMemcpyAsync(a.scratch, a.x, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+            src = a.scratch;
+            src_map = &map_s;
+        }
+        const int iters = (i == passes - 1) ? a.iterations - per_pass * (passes - 1) : per_pass;
+        t.src = src;
+        t.dst = dst;
+        t.k_run = 2 * iters;
+        t.out_scale = (i == passes - 1) ? a.out_scale : 1.0f;
+        t.z_chunk = choose_z_chunk(d, tiles_xy, t.k_run, kTbShape.ctas_per_sm);
+        if ((e = launch_tb_pass<KIND, K, W, HH, NT>(t, *src_map, map_b, t.z_chunk, s)) != cudaSuccess) return e;
+        if (a.launches) *a.launches += 1;
+        src = dst;
+        src_map = dst_map;
+    }
+    return cudaSuccess;
+}
+
+bool tb_supported(const StencilArgs& a) {
+    if (a.scheme != SCHEME_RBGS || a.scratch == nullptr) return false;
+    const int kind = a.kind;
+    const int per[3] = {kind == KIND_SCALAR ? a.scalar.periodic[0] : a.flow.periodic[0], kind == KIND_SCALAR ? a.scalar.periodic[1] : a.flow.periodic[1], kind == KIND_SCALAR ? a.scalar.periodic[2] : a.flow.periodic[2]};
+    const int n[3] = {a.dims.nx, a.dims.ny, a.dims.nz};
+    // An odd periodic size breaks the red-black colouring across the wrap.
+    for (int k = 0; k < 3; ++k)
+        if (per[k] && (n[k] & 1)) return false;
+    return true;
+}
+
 }  // namespace
 
 cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
+    if (a.blocked && tb_supported(a)) {
+        switch (a.kind) {
+        case KIND_VEL_X: return run_tb<KIND_VEL_X>(a, s, a.error_flag);
+        case KIND_VEL_Y: return run_tb<KIND_VEL_Y>(a, s, a.error_flag);
+        case KIND_VEL_Z: return run_tb<KIND_VEL_Z>(a, s, a.error_flag);
+        case KIND_SCALAR: return run_tb<KIND_SCALAR>(a, s, a.error_flag);
+        case KIND_PRESSURE: return run_tb<KIND_PRESSURE>(a, s, a.error_flag);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     switch (a.kind) {
     case KIND_VEL_X: return run_simple<KIND_VEL_X>(a, s);
     case KIND_VEL_Y: return run_simple<KIND_VEL_Y>(a, s);

@@ -55,6 +55,8 @@ struct DeviceStats {
     int32_t hit_cap;
     int32_t used_fallback;
     int32_t keep_going;  // residual-driven loop: 1 while another block of sweeps is needed
+    uint32_t error;      // set by a kernel whose bounded wait gave up
+    uint32_t pad;
 };
 
 }  // namespace sfb

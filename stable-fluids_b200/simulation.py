@@ -40,7 +40,7 @@ class _DeviceArray:
     """Zero-copy handle on library-owned device memory for torch.as_tensor."""
 
     def __init__(self, ptr: int, shape: tuple[int, ...]):
-        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (int(ptr), True), "version": 3, "strides": None, "stream": None}
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (int(ptr), False), "version": 3, "strides": None, "stream": None}
 
 
 class Simulation:

@@ -10,12 +10,19 @@ import pytest
 
 from tests.golden import cases as C
 
-# Against the reference library (same CUDA compiler, same expression shapes,
-# same FP32 arithmetic): within 1e-5 relative, floor 1e-3 of the field scale.
+# The required bound against the reference library is 1e-5 max relative
+# error (floor 1e-3 of the field scale). The RBGS scheme computes the
+# reference's arithmetic in the same order, so it is held to bit equality.
 REF_TOL, REF_FLOOR = 1e-5, 1e-3
-# Against the FP32 CPU oracle (fused multiply-adds placed by hand, so a few
-# roundings may differ and grow over the steps): 1e-4 relative, same floor.
-ORACLE_TOL, ORACLE_FLOOR = 1e-4, 1e-3
+# Against the FP32 CPU oracle (which is itself bit-equal to the reference):
+# bit equality for RBGS; Jacobi has no reference counterpart and is held to
+# 1e-5 against the oracle's Jacobi scheme.
+ORACLE_TOL, ORACLE_FLOOR = 1e-5, 1e-3
+
+
+def assert_bit_equal(a, b):
+    diff = {k: int(np.sum(np.asarray(a[k], np.float32) != np.asarray(b[k], np.float32))) for k in b}
+    assert not any(diff.values()), diff
 
 CASES = {c.name: c for c in C.build_cases()}
 
@@ -49,6 +56,7 @@ def test_rbgs_matches_reference_library(name, sf, lib, ref_lib, cuda):
     ref = run_lib(sf, ref_lib, case)
     err = errors(ours, ref, REF_FLOOR)
     assert max(err.values()) <= REF_TOL, err
+    assert_bit_equal(ours, ref)
 
 
 @pytest.mark.gpu
@@ -57,8 +65,7 @@ def test_rbgs_matches_oracle(name, sf, lib, orc, cuda):
     case = CASES[name]
     ours = run_lib(sf, lib, case)
     ref, _ = run_oracle(orc, case)
-    err = errors(ours, ref, ORACLE_FLOOR)
-    assert max(err.values()) <= ORACLE_TOL, err
+    assert_bit_equal(ours, ref)
 
 
 @pytest.mark.gpu
@@ -86,6 +93,7 @@ def test_config0_100_steps_matches_reference(sf, lib, ref_lib, cuda):
         sim.close()
     err = errors(outs[0], outs[1], REF_FLOOR)
     assert max(err.values()) <= REF_TOL, err
+    assert_bit_equal(outs[0], outs[1])
 
 
 @pytest.mark.gpu

@@ -1,0 +1,116 @@
+"""CPU tests of the oracle (the checker): pinned against fixtures produced by
+the reference library itself, plus properties of the restated algorithm."""
+
+import pathlib
+
+import numpy as np
+import pytest
+
+from tests.golden import cases as C
+
+GOLDEN = sorted((pathlib.Path(__file__).resolve().parent / "golden").glob("ref_*.npz"))
+
+# The FP32 oracle places the fused multiply-adds where the CUDA compiler
+# forms them for the reference's expressions; with that placement it
+# reproduces the reference library bit for bit, which is what is asserted.
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_oracle_matches_reference_fixture(path, sf, orc):
+    from tests.golden.load import load_fixture
+
+    case, ref = load_fixture(path, sf)
+    o = orc.Oracle(case.config, case.scalars, case.vectors, precision=32)
+    case.drive(o)
+    got = C.collect_oracle(o, orc, case)
+    mismatched = {k: int(np.sum(got[k].astype(np.float32) != ref[k])) for k in ref}
+    assert not any(mismatched.values()), mismatched
+
+
+def test_golden_fixtures_present():
+    assert len(GOLDEN) >= 5, "tests/golden/ref_*.npz missing: run tests/golden/make_golden.py on a GPU machine"
+
+
+def _small_case(sf, **kw):
+    return sf.scenes.plume("t", (16, 14, 12), sources=[(8, 5, 6, 3.0, 10.0, 5.0)], velocity_seed=0, diffuse_iterations=4, pressure_iterations=8, **kw)
+
+
+def test_still_fluid_stays_still(sf, orc):
+    sc = sf.scenes.plume("still", (10, 9, 8), diffuse_iterations=3, pressure_iterations=5)
+    o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64)
+    o.step(3)
+    for k in range(3):
+        assert not o.get(orc.VELOCITY, 0, k).any()
+    assert not o.get(orc.PRESSURE).any() and not o.get(orc.SCALAR, 1).any()
+
+
+def test_fp32_instance_tracks_fp64(sf, orc):
+    sc = _small_case(sf)
+    res = []
+    for prec in (32, 64):
+        o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=prec)
+        sf.scenes.run(o, sc, steps=4)
+        res.append((o.get(orc.SCALAR, 1), o.get(orc.PRESSURE), o.get(orc.VELOCITY, 0, 1)))
+    for a, b in zip(*res):
+        assert C.max_rel_err(a, b, 1e-2) < 1e-3
+
+
+def test_mirror_symmetry(sf, orc):
+    """A source centred in x under symmetric walls keeps the density mirror
+    symmetric in x and u_x antisymmetric (FP64)."""
+    sc = sf.scenes.plume("sym", (16, 12, 10), sources=[(8.0, 4.0, 5.0, 3.0, 10.0, 5.0)], diffuse_iterations=4, pressure_iterations=8)
+    o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64)
+    sf.scenes.run(o, sc, steps=3)
+    rho = o.get(orc.SCALAR, 1)
+    ux = o.get(orc.VELOCITY, 0, 0)
+    np.testing.assert_allclose(rho, rho[:, :, ::-1], atol=1e-10 * np.abs(rho).max())
+    np.testing.assert_allclose(ux, -ux[:, :, ::-1], atol=1e-10 * np.abs(ux).max() + 1e-14)
+
+
+def test_rbgs_and_jacobi_reach_the_same_pressure(sf, orc):
+    """Both iteration schemes solve the same system: after many iterations the
+    pressures agree (up to the constant null-space mode of the all-wall
+    Poisson operator) and the residual is tiny."""
+    sc = sf.scenes.plume("p", (10, 9, 8), sources=[(5, 3, 4, 2.5, 10.0, 5.0)], velocity_seed=0, diffuse_iterations=2, pressure_iterations=1500)
+    ps = []
+    for scheme in (orc.RBGS, orc.JACOBI):
+        o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64, scheme=scheme)
+        o.set_solver(compute_residual=True)
+        sf.scenes.run(o, sc, steps=1)
+        assert o.stats()["rel_residual"] < 1e-6
+        p = o.get(orc.PRESSURE)
+        ps.append(p - p.mean())
+    np.testing.assert_allclose(ps[0], ps[1], atol=1e-8 * np.abs(ps[0]).max())
+
+
+def test_residual_definition(sf, orc):
+    """rel_res = ||b - A p|| / ||b||, b = h^2 div with its mean removed (all
+    walls: singular operator), A p = sum6(p) - 6 p with clamped ghosts."""
+    sc = _small_case(sf)
+    o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64)
+    o.set_solver(compute_residual=True)
+    sf.scenes.run(o, sc, steps=2)
+    # the last step ends with the post-projection divergence; rebuild the
+    # pressure system of a fresh solve instead
+    p = o.get(orc.PRESSURE)
+    div = o.get(orc.DIVERGENCE)
+    h2 = float(np.float32(sc.config.cell_size) * np.float32(sc.config.cell_size))
+    b = h2 * div
+    q = np.pad(p, 1, mode="edge")
+    ap = q[:-2, 1:-1, 1:-1] + q[2:, 1:-1, 1:-1] + q[1:-1, :-2, 1:-1] + q[1:-1, 2:, 1:-1] + q[1:-1, 1:-1, :-2] + q[1:-1, 1:-1, 2:] - 6 * p
+    bm = b - b.mean()
+    expect = np.linalg.norm(bm - ap) / np.linalg.norm(bm)
+    assert abs(o.rel_residual() - expect) <= 1e-10 * max(1.0, expect)
+
+
+def test_residual_driven_solve_stops_at_tolerance(sf, orc):
+    sc = _small_case(sf)
+    o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64)
+    o.set_solver(tolerance=1e-3, max_iterations=5000, check_interval=4)
+    sf.scenes.run(o, sc, steps=1)
+    st = o.stats()
+    assert st["rel_residual"] <= 1e-3 and st["hit_cap"] == 0 and st["iterations"] % 4 == 0 and st["iterations"] > 0
+    o2 = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64)
+    o2.set_solver(tolerance=1e-3, max_iterations=8, check_interval=4)
+    sf.scenes.run(o2, sc, steps=1)
+    assert o2.stats()["hit_cap"] == 1 and o2.stats()["iterations"] == 8
