@@ -285,9 +285,9 @@ def main():
     t_stage, launches = time_stage(sim, sf.STAGE_PRESSURE, 3)
     per_launch = t_stage / max(launches, 1)
     cells = n ** 3
-    if args.scheme == "rbgs" and info.iterations_per_pass <= 0 and "simple" in os.environ.get("SFB200_STENCIL", "simple"):
-        bytes_per_launch = 6 * cells  # one colour: read n/2 other-colour + n/2 rhs, write n/2
-        unit_note = "one red-black colour sweep: 6 B/cell"
+    if args.scheme == "jacobi" or not info.blocked:
+        bytes_per_launch = (12 if args.scheme == "jacobi" else 6) * cells
+        unit_note = "one Jacobi sweep: read x + rhs, write x = 12 B/cell" if args.scheme == "jacobi" else "one red-black colour sweep: read n/2 other colour + n/2 rhs, write n/2 = 6 B/cell"
     else:
         bytes_per_launch = 12 * cells
         unit_note = "one temporally blocked pass: read p + rhs, write p = 12 B/cell"

@@ -90,7 +90,7 @@ typedef struct StableFluidsB200StepInfo {
     int32_t kernels_per_step;         /* kernel launches in one step */
     uint32_t scheme;
     int32_t iterations_per_pass;
-    int32_t reserved;
+    int32_t blocked;                  /* 1: temporally blocked stencil passes */
     uint64_t device_bytes;            /* device memory the context holds */
 } StableFluidsB200StepInfo;
 

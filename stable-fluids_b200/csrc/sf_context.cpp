@@ -366,7 +366,9 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
     c->field_bytes = c->cells * sizeof(float);
     c->flow = flatten(cfg.flow_boundary);
     c->residual_enabled = options.compute_residual != 0 || options.residual_tolerance > 0.0f;
-    c->blocked = !env_flag("STABLE_FLUIDS_B200_UNBLOCKED_STENCIL");
+    // Temporally blocked passes when asked for (iterations_per_pass >= 1);
+    // the default one-launch-per-colour kernels are faster on B200 today.
+    c->blocked = options.iterations_per_pass > 0 || env_flag("STABLE_FLUIDS_B200_BLOCKED_STENCIL");
 
     // Handles are 1-based indices (:544, :551).
     for (uint32_t i = 0; i < desc->scalar_field_count; ++i) {
@@ -645,6 +647,7 @@ StableFluidsResult stable_fluids_b200_get_step_info(void* context, StableFluidsB
     o.device_bytes = c.slab_bytes;
     o.scheme = c.options.scheme;
     o.iterations_per_pass = c.options.iterations_per_pass;
+    o.blocked = c.blocked ? 1 : 0;
     *out_info = o;
     return STABLE_FLUIDS_RESULT_OK;
 }

@@ -42,19 +42,52 @@ __device__ __forceinline__ float neighbour_sum(const float* __restrict__ f, int 
          + neighbour<KIND>(f, x, y, z + 1, d, fb, sb);
 }
 
-// One colour of an RBGS iteration; thread (hx, y, z) owns cell
-// x = 2 hx + ((y + z + parity) & 1), so every thread is active.
+// One colour of an RBGS iteration. Thread (hx, y) owns, in each of ZC
+// consecutive planes, the cell x = 2 hx + ((y + z + parity) & 1) of the
+// colour, so every thread is active. Cells of one colour never read each
+// other, so the thread loads the neighbours of all its cells first, then
+// updates, then stores (independent memory requests in flight). Interior
+// cells read their six neighbours directly; cells on the boundary use the
+// reference's ghost rules.
+constexpr int kColourPlanes = 4;
+
 template <int KIND>
 __global__ void __launch_bounds__(256) k_rbgs_colour(float* x, const float* __restrict__ rhs, float coef, int parity, Dims d, FlowBC fb, ScalarBC sb) {
     const int hx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
-    const int z = static_cast<int>(blockIdx.z * blockDim.z + threadIdx.z);
-    if (y >= d.ny || z >= d.nz) return;
-    const int cx = 2 * hx + ((y + z + parity) & 1);
-    if (cx >= d.nx) return;
-    const float nb = neighbour_sum<KIND>(x, cx, y, z, d, fb, sb);
-    const size_t i = lin(cx, y, z, d);
-    x[i] = update<KIND>(nb, rhs[i], coef);
+    const int z0 = static_cast<int>(blockIdx.z) * kColourPlanes;
+    if (y >= d.ny) return;
+    const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    float num[kColourPlanes];
+    size_t idx[kColourPlanes];
+    bool ok[kColourPlanes];
+#pragma unroll
+    for (int k = 0; k < kColourPlanes; ++k) {
+        const int z = z0 + k;
+        const int cx = 2 * hx + ((y + z + parity) & 1);
+        ok[k] = z < d.nz && cx < d.nx;
+        idx[k] = ok[k] ? lin(cx, y, z, d) : 0;
+        float nb = 0.0f;
+        if (ok[k]) {
+            const bool interior = cx >= 1 && cx <= d.nx - 2 && y >= 1 && y <= d.ny - 2 && z >= 1 && z <= d.nz - 2;
+            if (interior) {
+                const float* c = x + idx[k];
+                nb = c[-1] + c[1] + c[-static_cast<ptrdiff_t>(sy)] + c[sy] + c[-static_cast<ptrdiff_t>(sz)] + c[sz];
+            } else {
+                nb = neighbour_sum<KIND>(x, cx, y, z, d, fb, sb);
+            }
+        }
+        num[k] = tb::numerator<KIND>(nb, ok[k] ? rhs[idx[k]] : 0.0f, coef);
+    }
+#pragma unroll
+    for (int k = 0; k < kColourPlanes; ++k) {
+        if (!ok[k]) continue;
+        float q = tb::markstein_div(num[k], divisor, recip);
+        if (tb::needs_ieee_div(num[k])) q = num[k] / divisor;
+        x[idx[k]] = q;
+    }
 }
 
 template <int KIND>
@@ -83,10 +116,11 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(a.x, a.b, bytes, cudaMemcpyDeviceToDevice, s);
         else if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
         if (e != cudaSuccess) return e;
-        const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 3) / 4), static_cast<unsigned>((d.nz + 1) / 2));
+        const dim3 cblock(32, 8, 1);
+        const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
         for (int it = 0; it < a.iterations; ++it) {
-            k_rbgs_colour<KIND><<<grid, block, 0, s>>>(a.x, a.b, a.coef, 0, d, a.flow, a.scalar);
-            k_rbgs_colour<KIND><<<grid, block, 0, s>>>(a.x, a.b, a.coef, 1, d, a.flow, a.scalar);
+            k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, 0, d, a.flow, a.scalar);
+            k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, 1, d, a.flow, a.scalar);
         }
         if (a.launches) *a.launches += 2 * a.iterations;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -178,11 +212,11 @@ struct TbShape {
     int k, w, hh, nt, ctas_per_sm;
 };
 
-template <int KIND, int K, int W, int HH, int NT>
+template <int KIND, int K, int W, int HH, int ZP, int NT>
 cudaError_t launch_tb_pass(const TbArgs& args, const CUtensorMap& mx, const CUtensorMap& mb, int z_chunk, cudaStream_t s) {
-    constexpr int D = tb::kPrefetch;
-    constexpr size_t smem = static_cast<size_t>((K + D + 2) + (K + D + 1)) * W * HH * 4 + (D + 1) * 8;
-    auto kern = k_rbgs_tb<KIND, K, W, HH, NT>;
+    constexpr size_t smem = TbLayout<K, W, HH, ZP>::bytes;
+    static_assert(smem <= 232448, "shared memory per CTA");
+    auto kern = k_rbgs_tb<KIND, K, W, HH, ZP, NT>;
     static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (attr != cudaSuccess) return attr;
     constexpr int HX = ((K + 3) / 4) * 4;
@@ -209,11 +243,11 @@ int choose_z_chunk(const Dims& d, int tiles_xy, int k, int ctas_per_sm) {
     return best;
 }
 
-constexpr TbShape kTbShape{4, 96, 32, 384, 1};
+constexpr TbShape kTbShape{4, 96, 24, 384, 1};
 
 template <int KIND>
 cudaError_t run_tb(const StencilArgs& a, cudaStream_t s, unsigned* error_flag) {
-    constexpr int K = 4, W = 96, HH = 32, NT = 384;
+    constexpr int K = 4, W = 96, HH = 24, ZP = 2, NT = 384;
     const Dims& d = a.dims;
     const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
     const size_t bytes = n * sizeof(float);
@@ -258,7 +292,7 @@ cudaError_t run_tb(const StencilArgs& a, cudaStream_t s, unsigned* error_flag) {
         t.k_run = 2 * iters;
         t.out_scale = (i == passes - 1) ? a.out_scale : 1.0f;
         t.z_chunk = choose_z_chunk(d, tiles_xy, t.k_run, kTbShape.ctas_per_sm);
-        if ((e = launch_tb_pass<KIND, K, W, HH, NT>(t, *src_map, map_b, t.z_chunk, s)) != cudaSuccess) return e;
+        if ((e = launch_tb_pass<KIND, K, W, HH, ZP, NT>(t, *src_map, map_b, t.z_chunk, s)) != cudaSuccess) return e;
         if (a.launches) *a.launches += 1;
         src = dst;
         src_map = dst_map;

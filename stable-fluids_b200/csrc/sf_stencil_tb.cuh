@@ -1,35 +1,45 @@
 // sf_stencil_tb.cuh -- temporally blocked red-black Gauss-Seidel pass.
 //
-// One launch runs K_run colour half-sweeps (K_run/2 full RBGS iterations)
+// One launch runs k_run colour half-sweeps (k_run/2 full RBGS iterations)
 // over the whole field while reading x and b from HBM once and writing x
-// once (12 B per cell per pass instead of ~12 B per cell per half-sweep).
+// once: 12 B per cell per pass instead of ~12 B per cell per half-sweep.
 //
-// Tiling (2.5D): each CTA owns an xy tile of TX x TY output cells and a
-// chunk of Z planes. It loads the tile plus a halo of HX (x, rounded up to 4
-// cells for 16-byte TMA alignment) and K (y) cells, and streams the planes of
-// its chunk (plus K halo planes at each chunk end) through a ring of shared
-// memory planes. At stream time j plane j is loaded and colour stage s
-// (s = 1..K_run) updates plane j - s in place:
-//   - stage s - 1 finished plane j - s + 1 earlier in the same time step,
-//   - stage s + 1 has not yet touched plane j - s - 1,
+// Tiling (2.5D): each CTA owns an xy tile of TX x TY output cells and a chunk
+// of planes. It loads the tile plus a halo of HX (x, a multiple of 4 cells for
+// 16-byte TMA alignment) and K (y) cells, and streams its planes (plus k_run
+// halo planes at each chunk end) through a ring of shared-memory planes, ZP
+// planes per time step. At time step j colour stage s (s = 1..k_run) updates
+// planes ZP*j - s - k (k = 0..ZP-1) in place:
+//   - stage s-1 finished plane ZP*j - s + 1 earlier in the same time step,
+//   - stage s+1 has not yet touched the planes below,
 // so every stage reads exactly the values the global half-sweep would see.
-// Each stage shrinks the region of correct values by one cell in x and y
-// (and one plane at each chunk end), which the halo absorbs. The updates use
-// the reference's arithmetic (backend-cuda.cu:354-375, 398-407), so the
-// result equals K_run/2 reference iterations bit for bit.
+// Each stage shrinks the region of correct values by one cell in x and y (and
+// one plane at each chunk end), which the halo absorbs. The updates use the
+// reference's arithmetic (backend-cuda.cu:354-375, 398-407), so the result
+// equals k_run/2 reference iterations bit for bit.
 //
-// Shared-memory mapping: a warp updates 16 cells of one colour in each of two
-// adjacent rows. Because the row pitch W is even and adjacent rows hold
-// opposite colours, the 32 lanes address 32 distinct banks for the cell, its
-// x, y and z neighbours and b: no bank conflicts with a plain row-major plane,
-// which is what a TMA box writes.
+// Work split: warp w owns x segment w % 3 (32 columns) and every PG-th row
+// pair from w / 3; lanes 0-15 take the lower row of a pair, lanes 16-31 the
+// upper one, each lane the cell of the stage's colour in its column pair.
+// Because the row pitch W is even and adjacent rows hold opposite colours,
+// the 32 lanes hit 32 distinct banks for the cell, its x, y, z neighbours and
+// b: no bank conflicts on a plain row-major plane, which is what a TMA box
+// writes. Within a stage every load reads the other colour and every store
+// writes this colour, so a lane issues all loads of the stage first, then
+// computes, then stores; all addresses are immediate offsets from one base
+// per plane.
+//
+// Boundaries: x/y ghost values are written into the halo cells just outside
+// the domain before each stage (fill_ghosts); z ghosts are applied on the
+// first and last plane of a non-periodic z axis. Periodic axes need no
+// ghosts: the halo holds the wrapped cells.
 //
 // Loads: one elected thread issues a 3D TMA box per plane for x and for b
-// (cp.async.bulk.tensor, mbarrier completion, prefetch distance D planes).
-// CTAs whose halo wraps around a periodic x or y boundary (TMA fills outside
-// the tensor instead of wrapping) and grids whose rows are not 16-byte
-// aligned load with cp.async instead. Every mbarrier wait is bounded: on
-// timeout the kernel records an error flag and returns.
+// (cp.async.bulk.tensor, mbarrier completion, D time steps ahead). CTAs whose
+// halo wraps around a periodic x or y boundary (a TMA box fills outside the
+// tensor instead of wrapping) and grids whose rows are not 16-byte aligned
+// load with cp.async instead. The mbarrier wait is bounded: on timeout the
+// kernel sets an error flag and returns.
 #pragma once
 
 #include <cuda.h>
@@ -65,9 +75,22 @@ struct TbArgs {
     unsigned* error;   // set to 1 if a bounded wait gives up
 };
 
+#ifdef SFB_TB_PROFILE
+// Per-CTA cycle counters of a profiling build: [0] waits, [1] stages,
+// [2] output, [3] TMA path used, [4] time steps.
+__device__ unsigned long long g_tb_profile[4096][5];
+#define SFB_TB_MARK(var) const long long var = clock64()
+#define SFB_TB_ADD(slot, from) \
+    if (threadIdx.x == 0) g_tb_profile[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)][slot] += clock64() - (from)
+#else
+#define SFB_TB_MARK(var)
+#define SFB_TB_ADD(slot, from)
+#endif
+
 namespace tb {
 
-constexpr int kPrefetch = 2;  // planes in flight ahead of the one being consumed
+constexpr int kPrefetch = 2;  // time steps of loads in flight ahead of the one consumed
+constexpr int kSlackFloats = 1536;  // read-only slack after the rings for masked lanes
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
 
@@ -111,7 +134,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <int KIND>
 __device__ __forceinline__ float ghost(const GhostRule& g, int face, float self) {
     const int m = g.mode[face];
     if (m == GHOST_COPY) return self;
@@ -119,34 +141,178 @@ __device__ __forceinline__ float ghost(const GhostRule& g, int face, float self)
     return g.k[face] - self;
 }
 
+// Correctly rounded n / d from y = RN(1 / d) by Markstein's correction
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990): q = RN(n y), r = n - q d
+// (exact with an FMA), q' = RN(q + r y). It equals IEEE division for every
+// numerator checked with |n| >= 1e-30 (all 2^32 numerators for d = 6,
+// sampled ones for the diffusion divisors 1 + 6 alpha). Zeros keep their
+// sign here; the caller sends the few numerators with 0 < |n| < 2^-99 to the
+// IEEE division (needs_ieee_div).
+__device__ __forceinline__ float markstein_div(float n, float d, float y) {
+    const float q = __fmul_rn(n, y);
+    const float r = __fmaf_rn(-q, d, n);
+    const float out = __fmaf_rn(r, y, q);
+    return n == 0.0f ? n : out;
+}
+__device__ __forceinline__ bool needs_ieee_div(float n) { return !(fabsf(n) >= 0x1p-99f) && n != 0.0f; }
+
+// Numerator of the update in the reference's expression shape
+// (backend-cuda.cu:363, :406), so the compiler fuses it the same way.
 template <int KIND>
-__device__ __forceinline__ float update(float nb, float rhs, float coef) {
-    if constexpr (KIND == KIND_PRESSURE) return (nb - coef * rhs) / 6.0f;
-    else return (rhs + coef * nb) / (1.0f + 6.0f * coef);
+__device__ __forceinline__ float numerator(float nb, float rhs, float coef) {
+    if constexpr (KIND == KIND_PRESSURE) return nb - coef * rhs;
+    else return rhs + coef * nb;
 }
 
 }  // namespace tb
 
+// CTA-uniform values of one (stage, plane) of a time step.
+struct Combo {
+    int x, xm, xp, b;  // ring offsets (floats) of the plane, its z neighbours and its b plane; x < 0: no plane
+    int parity;        // x parity of the stage's colour in the tile's even rows
+    int zflags;        // 1: first plane of a non-periodic z axis, 2: last plane
+    int pad0, pad1;
+};
+
+// One colour stage for one warp: NPL planes x MP row pairs, loads first,
+// then the updates, then predicated stores.
+template <int KIND, int W, int MP, int PG, int NPL>
+__device__ __forceinline__ void stage_all(const Combo* combo, float* xs, const float* bs, int s, int npairs, int pg, int hi, int lane_off, int lx_lane, int lo_x, bool mask_x, int gx_base, int nx, bool mask_y, int gy_base, int ny, const TbArgs& a,
+                                          float divisor, float recip) {
+    constexpr int STEP = 2 * PG * W;  // floats between this lane's row pairs
+    float num[NPL][MP];
+    float* cell[NPL];
+    bool lane_ok[NPL];
+#pragma unroll
+    for (int k = 0; k < NPL; ++k) {
+        const Combo e = combo[k];
+        const bool plane_ok = e.x >= 0;
+        const int par = e.parity ^ hi;
+        const int c0 = lane_off + s * W + par;  // this lane's first cell
+        const int lx = lx_lane + par;
+        bool ok = plane_ok && lx >= lo_x + s && lx < W - lo_x - s;
+        if (mask_x) ok = ok && static_cast<unsigned>(gx_base + par) < static_cast<unsigned>(nx);
+        lane_ok[k] = ok;
+        const float* P = xs + (plane_ok ? e.x : 0) + c0;
+        const float* Pm = xs + (plane_ok ? e.xm : 0) + c0;
+        const float* Pp = xs + (plane_ok ? e.xp : 0) + c0;
+        const float* B = bs + (plane_ok ? e.b : 0) + c0;
+        cell[k] = xs + (plane_ok ? e.x : 0) + c0;
+        if (e.zflags == 0) {  // CTA-uniform
+#pragma unroll
+            for (int m = 0; m < MP; ++m) {
+                const int o = m * STEP;
+                const float nb = P[o - 1] + P[o + 1] + P[o - W] + P[o + W] + Pm[o] + Pp[o];
+                num[k][m] = tb::numerator<KIND>(nb, B[o], a.coef);
+            }
+        } else {
+            const bool zlo = (e.zflags & 1) != 0, zhi = (e.zflags & 2) != 0;
+#pragma unroll
+            for (int m = 0; m < MP; ++m) {
+                const int o = m * STEP;
+                const float self = P[o];
+                const float zm = zlo ? tb::ghost(a.g, ZM, self) : Pm[o];
+                const float zp = zhi ? tb::ghost(a.g, ZP, self) : Pp[o];
+                const float nb = P[o - 1] + P[o + 1] + P[o - W] + P[o + W] + zm + zp;
+                num[k][m] = tb::numerator<KIND>(nb, B[o], a.coef);
+            }
+        }
+    }
+    bool rare = false;
+#pragma unroll
+    for (int k = 0; k < NPL; ++k)
+#pragma unroll
+        for (int m = 0; m < MP; ++m) rare = rare || tb::needs_ieee_div(num[k][m]);
+    const bool any_rare = __any_sync(0xffffffffu, rare);
+#pragma unroll
+    for (int k = 0; k < NPL; ++k)
+#pragma unroll
+        for (int m = 0; m < MP; ++m) {
+            const int pair = pg + PG * m;
+            bool ok = lane_ok[k] && pair < npairs;
+            if (mask_y) ok = ok && static_cast<unsigned>(gy_base + s + 2 * PG * m) < static_cast<unsigned>(ny);
+            float q = tb::markstein_div(num[k][m], divisor, recip);
+            if (any_rare && tb::needs_ieee_div(num[k][m])) q = num[k][m] / divisor;
+            if (ok) cell[k][m * STEP] = q;
+        }
+}
+
+// Writes the x/y ghost values of the boundary cells of one colour into the
+// halo cells just outside the domain (non-periodic faces only). A ghost cell
+// is the face neighbour of exactly one domain cell, so it can hold that
+// cell's ghost value (a function of the cell itself: copy, constant or
+// reflection, backend-cuda.cu:62-189 for a face neighbour) for as long as the
+// cell keeps its value, i.e. until the stage that updates it.
+template <int W, int HH>
+__device__ __forceinline__ void fill_ghosts(float* P, int gz, int colour, int xo, int yo, const TbArgs& a, int tid, int nt) {
+    const Dims& d = a.d;
+    const bool px = a.g.periodic[0] != 0, py = a.g.periodic[1] != 0;
+    if (!px) {
+        const int lb0 = -xo, lb1 = d.nx - 1 - xo;  // local columns of x = 0 and x = nx - 1
+        const bool lo = lb0 >= 1 && lb0 < W, hi = lb1 >= 0 && lb1 + 1 < W;
+        if (lo || hi)
+            for (int row = tid; row < HH; row += nt) {
+                const int gy = yo + row;
+                if (!py && static_cast<unsigned>(gy) >= static_cast<unsigned>(d.ny)) continue;
+                if (lo && ((gy + gz) & 1) == colour) P[row * W + lb0 - 1] = tb::ghost(a.g, XM, P[row * W + lb0]);
+                if (hi && ((d.nx - 1 + gy + gz) & 1) == colour) P[row * W + lb1 + 1] = tb::ghost(a.g, XP, P[row * W + lb1]);
+            }
+    }
+    if (!py) {
+        const int rb0 = -yo, rb1 = d.ny - 1 - yo;  // local rows of y = 0 and y = ny - 1
+        const bool lo = rb0 >= 1 && rb0 < HH, hi = rb1 >= 0 && rb1 + 1 < HH;
+        if (lo || hi)
+            for (int lx = tid; lx < W; lx += nt) {
+                const int gx = xo + lx;
+                if (!px && static_cast<unsigned>(gx) >= static_cast<unsigned>(d.nx)) continue;
+                if (lo && ((gx + gz) & 1) == colour) P[(rb0 - 1) * W + lx] = tb::ghost(a.g, YM, P[rb0 * W + lx]);
+                if (hi && ((gx + d.ny - 1 + gz) & 1) == colour) P[(rb1 + 1) * W + lx] = tb::ghost(a.g, YP, P[rb1 * W + lx]);
+            }
+    }
+}
+
+// Shared memory of one CTA: x ring, b ring, read-only slack (masked lanes
+// may read past the last plane), barriers, combo table, abort flag.
+template <int K, int W, int HH, int ZP>
+struct TbLayout {
+    static constexpr int D = tb::kPrefetch;
+    static constexpr int R = ZP * D + 2 * ZP + K;  // x planes resident or in flight
+    static constexpr int RB = R - 1;               // b planes
+    static constexpr int NB = D + 1;               // one barrier per time step in flight
+    static constexpr int PLANE = W * HH;
+    static constexpr size_t slack_off = static_cast<size_t>(R + RB) * PLANE * 4;
+    static constexpr size_t bars_off = slack_off + tb::kSlackFloats * 4;
+    static constexpr size_t combo_off = bars_off + 8 * ((NB + 1) / 2 * 2);
+    static constexpr size_t abort_off = combo_off + sizeof(Combo) * K * ZP;
+    static constexpr size_t bytes = abort_off + 16;
+};
+
 // K: halo (max colour half-sweeps per pass); W, HH: loaded plane size;
-// NT: threads per CTA.
-template <int KIND, int K, int W, int HH, int NT>
+// ZP: planes per time step; NT: threads per CTA.
+template <int KIND, int K, int W, int HH, int ZP, int NT>
 __global__ void __launch_bounds__(NT, 1) k_rbgs_tb(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b, TbArgs a) {
+    using L = TbLayout<K, W, HH, ZP>;
     constexpr int HX = ((K + 3) / 4) * 4;
     constexpr int TX = W - 2 * HX;
     constexpr int TY = HH - 2 * K;
-    constexpr int D = tb::kPrefetch;
-    constexpr int R = K + D + 2;   // x planes: j-K-1 .. j+D
-    constexpr int RB = K + D + 1;  // b planes: j-K .. j+D
-    constexpr int NB = D + 1;      // barriers: planes j .. j+D
-    constexpr int PLANE = W * HH;
+    constexpr int D = L::D, R = L::R, RB = L::RB, NB = L::NB, PLANE = L::PLANE;
     constexpr int SEGS = W / 32;
     constexpr int NWARPS = NT / 32;
-    static_assert(W % 32 == 0 && TX > 0 && TY > 0, "tile shape");
+    constexpr int PG = NWARPS / SEGS;
+    constexpr int MP = ((HH - 2) / 2 + PG - 1) / PG;  // row pairs per warp per stage, at most
+    static_assert(W % 32 == 0 && TX > 0 && TY > 0 && TX % 4 == 0 && HH % 2 == 0, "tile shape");
+    static_assert(NWARPS % SEGS == 0, "warps must split evenly over x segments");
+    // a masked lane reads at most row 2 PG MP + K of a plane (its last pair's
+    // upper row plus one): that many rows must fit in a plane plus the slack
+    static_assert((2 * PG * MP + K + 1) * W <= PLANE + tb::kSlackFloats, "slack for masked reads");
 
     extern __shared__ __align__(128) float smem[];
-    float* xs = smem;                 // R planes
-    float* bs = smem + R * PLANE;     // RB planes
-    uint64_t* bars = reinterpret_cast<uint64_t*>(bs + RB * PLANE);
+    float* xs = smem;
+    float* bs = smem + R * PLANE;
+    char* base = reinterpret_cast<char*>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + L::bars_off);
+    Combo* combo = reinterpret_cast<Combo*>(base + L::combo_off);
+    int* abort_flag = reinterpret_cast<int*>(base + L::abort_off);
 
     const Dims d = a.d;
     const int x0 = static_cast<int>(blockIdx.x) * TX;
@@ -154,152 +320,190 @@ __global__ void __launch_bounds__(NT, 1) k_rbgs_tb(const __grid_constant__ CUten
     const int z0 = static_cast<int>(blockIdx.z) * a.z_chunk;
     if (z0 >= d.nz) return;
     const int z1 = min(z0 + a.z_chunk, d.nz);
-    const int xo = x0 - HX, yo = y0 - K;  // plane origin in grid coordinates
+    const int xo = x0 - HX, yo = y0 - K;
     const bool px = a.g.periodic[0] != 0, py = a.g.periodic[1] != 0, pz = a.g.periodic[2] != 0;
     const int k_run = a.k_run;
     const int zs = pz ? z0 - k_run : max(z0 - k_run, 0);
-    const int ze = pz ? z1 - 1 + k_run : min(z1 - 1 + k_run, d.nz - 1);  // inclusive
+    const int ze = pz ? z1 - 1 + k_run : min(z1 - 1 + k_run, d.nz - 1);
     const int nplanes = ze - zs + 1;
-    const bool wraps = (px && (xo < 0 || xo + W > d.nx)) || (py && (yo < 0 || yo + HH > d.ny));
+    const bool out_x = xo < 0 || xo + W > d.nx, out_y = yo < 0 || yo + HH > d.ny;
+    const bool wraps = (px && out_x) || (py && out_y);
+    const bool mask_x = !px && out_x, mask_y = !py && out_y;
+    const bool fill = mask_x || mask_y;
     const bool use_tma = a.tma_ok && !wraps;
     const bool zero_x = a.src == nullptr;
     const int tid = static_cast<int>(threadIdx.x);
     const int warp = tid >> 5, lane = tid & 31;
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * a.coef;
+    const float recip = 1.0f / divisor;
 
     if (tid == 0) {
         for (int i = 0; i < NB; ++i) tb::mbar_init(&bars[i], 1);
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // the slack is read by masked lanes only; keep it finite
+    for (int i = tid; i < tb::kSlackFloats; i += NT) reinterpret_cast<float*>(base + L::slack_off)[i] = 0.0f;
     __syncthreads();
 
-    auto plane_z = [&](int pi) {  // grid z of stream plane pi
-        int z = zs + pi;
+    auto plane_z = [&](int pi) {
+        const int z = zs + pi;
         return pz ? wrap_index(z, d.nz) : z;
     };
 
-    // Enqueue the loads of stream plane pi (x into its ring slot, b into its).
-    auto issue = [&](int pi) {
-        if (pi >= nplanes) {
+    // Enqueue the loads of time step `step` (stream planes ZP*step ..).
+    auto issue = [&](int step) {
+        const int first = ZP * step;
+        if (first >= nplanes) {
             if (!use_tma) tb::cp_async_commit();
             return;
         }
-        float* xdst = xs + (pi % R) * PLANE;
-        float* bdst = bs + (pi % RB) * PLANE;
-        const int z = plane_z(pi);
+        const int count = min(ZP, nplanes - first);
         if (zero_x)
-            for (int i = tid; i < PLANE; i += NT) xdst[i] = 0.0f;
+            for (int k = 0; k < count; ++k) {
+                float* xdst = xs + ((first + k) % R) * PLANE;
+                for (int i = tid; i < PLANE; i += NT) xdst[i] = 0.0f;
+            }
         if (use_tma) {
             if (tid == 0) {
                 tb::fence_proxy_async();
-                uint64_t* bar = &bars[pi % NB];
-                tb::mbar_expect_tx(bar, (zero_x ? 1u : 2u) * PLANE * 4u);
-                if (!zero_x) tb::tma_load_plane(xdst, &map_x, xo, yo, z, bar);
-                tb::tma_load_plane(bdst, &map_b, xo, yo, z, bar);
+                uint64_t* bar = &bars[step % NB];
+                tb::mbar_expect_tx(bar, static_cast<unsigned>(count) * (zero_x ? 1u : 2u) * PLANE * 4u);
+                for (int k = 0; k < count; ++k) {
+                    const int pi = first + k, z = plane_z(pi);
+                    if (!zero_x) tb::tma_load_plane(xs + (pi % R) * PLANE, &map_x, xo, yo, z, bar);
+                    tb::tma_load_plane(bs + (pi % RB) * PLANE, &map_b, xo, yo, z, bar);
+                }
             }
         } else {
-            const size_t zoff = static_cast<size_t>(z) * d.ny * d.nx;
-            for (int i = tid; i < PLANE; i += NT) {
-                int gx = xo + i % W, gy = yo + i / W;
-                if (px) gx = wrap_index(gx, d.nx);
-                if (py) gy = wrap_index(gy, d.ny);
-                const bool in = static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny);
-                const size_t off = in ? zoff + static_cast<size_t>(gy) * d.nx + gx : 0;
-                if (!zero_x) tb::cp_async4(xdst + i, a.src + off, in);
-                tb::cp_async4(bdst + i, a.b + off, in);
+            for (int k = 0; k < count; ++k) {
+                const int pi = first + k;
+                float* xdst = xs + (pi % R) * PLANE;
+                float* bdst = bs + (pi % RB) * PLANE;
+                const size_t zoff = static_cast<size_t>(plane_z(pi)) * d.ny * d.nx;
+                for (int i = tid; i < PLANE; i += NT) {
+                    int gx = xo + i % W, gy = yo + i / W;
+                    if (px) gx = wrap_index(gx, d.nx);
+                    if (py) gy = wrap_index(gy, d.ny);
+                    const bool in = static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny);
+                    const size_t off = in ? zoff + static_cast<size_t>(gy) * d.nx + gx : 0;
+                    if (!zero_x) tb::cp_async4(xdst + i, a.src + off, in);
+                    tb::cp_async4(bdst + i, a.b + off, in);
+                }
             }
             tb::cp_async_commit();
         }
     };
 
-    for (int p = 0; p < D && p < nplanes; ++p) issue(p);
-    if (!use_tma)
-        for (int p = nplanes; p < D; ++p) tb::cp_async_commit();
+    // fixed work split and per-lane constants
+    const int seg = warp % SEGS, pg = warp / SEGS, hi = lane >> 4;
+    const int lx_lane = 32 * seg + 2 * (lane & 15);
+    const int lane_off = (hi + 2 * pg) * W + lx_lane;  // row hi + 2 pg, column lx_lane
+    const int lo_x = HX - K;                           // first column inside the dependency cone
+    const int gx_base = xo + lx_lane;
+    const int gy_base = yo + hi + 2 * pg;
 
-    const int row_lo_x = HX - K;  // first column inside the dependency cone
-    for (int j = 0; j < nplanes + k_run; ++j) {
-        // prefetch plane j + D (its slots held planes no longer needed)
+    // ghost cells for colour stage t of time step jj (its planes are resident)
+    auto fill_stage = [&](int jj, int t) {
+#pragma unroll
+        for (int k = 0; k < ZP; ++k) {
+            const int pi = ZP * jj - t - k;
+            if (pi < 0 || pi >= nplanes) continue;
+            fill_ghosts<W, HH>(xs + (pi % R) * PLANE, plane_z(pi), (t - 1) & 1, xo, yo, a, tid, NT);
+        }
+    };
+
+    const int steps = (nplanes - 1 + k_run + ZP - 1) / ZP + 1;  // the last plane leaves stage k_run at step ceil((nplanes-1+k_run)/ZP)
+    for (int t = 0; t < D; ++t) issue(t);
+
+    for (int j = 0; j < steps; ++j) {
         issue(j + D);
-        if (j < nplanes) {
+        // table of the CTA-uniform values of each (stage, plane) of this step
+        if (tid < k_run * ZP) {
+            const int s = tid / ZP + 1, k = tid % ZP;
+            const int pi = ZP * j - s - k;
+            Combo e{-1, 0, 0, 0, 0, 0, 0, 0};
+            if (pi >= 0 && pi < nplanes) {
+                const int gz = plane_z(pi);
+                e.x = (pi % R) * PLANE;
+                e.xm = ((pi + R - 1) % R) * PLANE;
+                e.xp = ((pi + 1) % R) * PLANE;
+                e.b = (pi % RB) * PLANE;
+                e.parity = ((s - 1) + yo + s + gz) & 1;  // colour + y parity of row s + z
+                e.zflags = (!pz && gz == 0 ? 1 : 0) | (!pz && gz == d.nz - 1 ? 2 : 0);
+            }
+            combo[tid] = e;
+        }
+        SFB_TB_MARK(t_wait);
+        if (ZP * j < nplanes) {
             if (use_tma) {
-                if (!tb::mbar_wait(&bars[j % NB], static_cast<unsigned>((j / NB) & 1))) {
-                    if (tid == 0) atomicExch(a.error, 1u);
-                    return;
+                // one thread polls; the barrier below publishes the data
+                if (tid == 0 && !tb::mbar_wait(&bars[j % NB], static_cast<unsigned>((j / NB) & 1))) {
+                    atomicExch(a.error, 1u);
+                    *abort_flag = 1;
                 }
             } else {
                 tb::cp_async_wait<D>();
             }
         }
         __syncthreads();
+        if (*abort_flag) return;
+        SFB_TB_ADD(0, t_wait);
+        SFB_TB_MARK(t_stage);
 
         for (int s = 1; s <= k_run; ++s) {
-            const int pi = j - s;
-            if (pi >= 0 && pi < nplanes) {
-                const int colour = (s - 1) & 1;
-                const int gz = plane_z(pi);
-                float* P = xs + (pi % R) * PLANE;
-                const float* Pm = xs + ((pi + R - 1) % R) * PLANE;
-                const float* Pp = xs + ((pi + 1) % R) * PLANE;
-                const float* B = bs + (pi % RB) * PLANE;
-                const bool gz_lo = !pz && gz == 0, gz_hi = !pz && gz == d.nz - 1;
-                const int rows = HH - 2 * s;
-                const int tasks = ((rows + 1) >> 1) * SEGS;
-                for (int t = warp; t < tasks; t += NWARPS) {
-                    const int row = s + 2 * (t / SEGS) + (lane >> 4);
-                    const int seg = t % SEGS;
-                    const int gy = yo + row;
-                    const int h = (colour + gy + gz) & 1;  // x parity of this colour in this row (xo is even)
-                    const int lx = 32 * seg + 2 * (lane & 15) + h;
-                    const int gx = xo + lx;
-                    if (row >= HH - s || lx < row_lo_x + s || lx >= W - row_lo_x - s) continue;
-                    if (!px && static_cast<unsigned>(gx) >= static_cast<unsigned>(d.nx)) continue;
-                    if (!py && static_cast<unsigned>(gy) >= static_cast<unsigned>(d.ny)) continue;
-                    const int c = row * W + lx;
-                    const float self = P[c];
-                    const float xm = (!px && gx == 0) ? tb::ghost<KIND>(a.g, XM, self) : P[c - 1];
-                    const float xp = (!px && gx == d.nx - 1) ? tb::ghost<KIND>(a.g, XP, self) : P[c + 1];
-                    const float ym = (!py && gy == 0) ? tb::ghost<KIND>(a.g, YM, self) : P[c - W];
-                    const float yp = (!py && gy == d.ny - 1) ? tb::ghost<KIND>(a.g, YP, self) : P[c + W];
-                    const float zm = gz_lo ? tb::ghost<KIND>(a.g, ZM, self) : Pm[c];
-                    const float zp = gz_hi ? tb::ghost<KIND>(a.g, ZP, self) : Pp[c];
-                    const float nb = xm + xp + ym + yp + zm + zp;
-                    P[c] = tb::update<KIND>(nb, B[c], a.coef);
-                }
-            }
+            const int npairs = (HH - 2 * s) >> 1;
+            stage_all<KIND, W, MP, PG, ZP>(combo + (s - 1) * ZP, xs, bs, s, npairs, pg, hi, lane_off, lx_lane, lo_x, mask_x, gx_base, d.nx, mask_y, gy_base, d.ny, a, divisor, recip);
+            // the next stage's colour is untouched by this one: fill its ghosts now
+            if (fill && s < k_run) fill_stage(j, s + 1);
             __syncthreads();
         }
+        SFB_TB_ADD(1, t_stage);
+        SFB_TB_MARK(t_out);
 
-        // plane j - k_run is final: write its interior
-        const int q = j - k_run;
-        if (q >= 0 && q < nplanes) {
+        // ghosts of the first stage of the next time step (its planes arrived
+        // in this one); the output below reads other planes
+        if (fill) fill_stage(j + 1, 1);
+        // planes ZP*j - k_run - k are final: write their interiors
+#pragma unroll
+        for (int k = 0; k < ZP; ++k) {
+            const int q = ZP * j - k_run - k;
+            if (q < 0 || q >= nplanes) continue;
             const int zq = zs + q;
-            if (zq >= z0 && zq < z1) {
-                const float* P = xs + (q % R) * PLANE;
-                const size_t zoff = static_cast<size_t>(zq) * d.ny * d.nx;
-                if (use_tma) {  // rows 16-byte aligned: float4 stores
-                    constexpr int V = TX / 4;
-                    for (int i = tid; i < TY * V; i += NT) {
-                        const int row = K + i / V, lx = HX + 4 * (i % V);
-                        const int gx = xo + lx, gy = yo + row;
-                        if (gy >= d.ny || gx >= d.nx) continue;
-                        float4 v = *reinterpret_cast<const float4*>(P + row * W + lx);
-                        v.x *= a.out_scale;
-                        v.y *= a.out_scale;
-                        v.z *= a.out_scale;
-                        v.w *= a.out_scale;
-                        *reinterpret_cast<float4*>(a.dst + zoff + static_cast<size_t>(gy) * d.nx + gx) = v;
-                    }
-                } else {
-                    for (int i = tid; i < TY * TX; i += NT) {
-                        const int row = K + i / TX, lx = HX + i % TX;
-                        const int gx = xo + lx, gy = yo + row;
-                        if (gy >= d.ny || gx >= d.nx) continue;
-                        a.dst[zoff + static_cast<size_t>(gy) * d.nx + gx] = P[row * W + lx] * a.out_scale;
-                    }
+            if (zq < z0 || zq >= z1) continue;
+            const float* P = xs + (q % R) * PLANE;
+            const size_t zoff = static_cast<size_t>(zq) * d.ny * d.nx;
+            if (use_tma) {  // rows 16-byte aligned: float4 stores
+                constexpr int V = TX / 4;
+                for (int i = tid; i < TY * V; i += NT) {
+                    const int row = K + i / V, lx = HX + 4 * (i % V);
+                    const int gx = xo + lx, gy = yo + row;
+                    if (gy >= d.ny || gx >= d.nx) continue;
+                    float4 v = *reinterpret_cast<const float4*>(P + row * W + lx);
+                    v.x *= a.out_scale;
+                    v.y *= a.out_scale;
+                    v.z *= a.out_scale;
+                    v.w *= a.out_scale;
+                    *reinterpret_cast<float4*>(a.dst + zoff + static_cast<size_t>(gy) * d.nx + gx) = v;
+                }
+            } else {
+                for (int i = tid; i < TY * TX; i += NT) {
+                    const int row = K + i / TX, lx = HX + i % TX;
+                    const int gx = xo + lx, gy = yo + row;
+                    if (gy >= d.ny || gx >= d.nx) continue;
+                    a.dst[zoff + static_cast<size_t>(gy) * d.nx + gx] = P[row * W + lx] * a.out_scale;
                 }
             }
         }
         __syncthreads();
+        SFB_TB_ADD(2, t_out);
     }
+#ifdef SFB_TB_PROFILE
+    if (threadIdx.x == 0) {
+        g_tb_profile[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)][3] = use_tma;
+        g_tb_profile[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)][4] += steps;
+    }
+#endif
     if (!use_tma) tb::cp_async_wait<0>();
 }
 

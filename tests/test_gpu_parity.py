@@ -213,3 +213,60 @@ def test_views_and_consumer_stream(sf, lib, cuda):
     fx, fy, fz = sim.fetch(sf.VIEW_VECTOR_FIELD, 2)
     np.testing.assert_array_equal(fx, case.forces[2][0])
     sim.close()
+
+
+def _tiled_scene(sf, n, walls, steps=3):
+    """Grids large enough for several xy tiles and z chunks of the blocked
+    stencil (TMA path when nx % 4 == 0, cp.async path otherwise)."""
+    nx, ny, nz = n
+    return sf.scenes.plume("tiled", n, dt=0.1, viscosity=1e-4, diffusion=1e-5, diffuse_iterations=5, pressure_iterations=7, sources=[(nx / 2, 6, nz / 2, 5.0, 10.0, 6.0), (nx / 4, 5, nz / 3, 4.0, 8.0, 3.0)], walls=walls, velocity_seed=2, steps=steps)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["walls_200x60x40", "benchmark_192x56x36", "walls_odd_181x47x29"])
+def test_tiled_grids_match_reference_library(kind, sf, lib, ref_lib, cuda):
+    if kind == "walls_200x60x40":
+        scene = _tiled_scene(sf, (200, 60, 40), sf.scenes.stam_walls())
+    elif kind == "benchmark_192x56x36":
+        scene = _tiled_scene(sf, (192, 56, 36), sf.scenes.benchmark_walls())
+    else:
+        scene = _tiled_scene(sf, (181, 47, 29), sf.scenes.stam_walls())
+    outs = []
+    for L in (lib, ref_lib):
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=L)
+        sf.scenes.run(sim, scene)
+        case = C.Case(kind, scene.config, scene.scalars, scene.vectors, scene.steps)
+        outs.append(C.collect_outputs(sim, sf, case))
+        sim.close()
+    err = errors(outs[0], outs[1], REF_FLOOR)
+    assert max(err.values()) <= REF_TOL, err
+    assert_bit_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_blocked_rbgs_matches_reference_library(name, sf, lib, ref_lib, cuda):
+    """The temporally blocked passes (two RBGS iterations per HBM pass)
+    reproduce the reference bit for bit."""
+    case = CASES[name]
+    opts = sf.default_options(lib)
+    opts.iterations_per_pass = 2
+    ours = run_lib(sf, lib, case, options=opts)
+    ref = run_lib(sf, ref_lib, case)
+    assert_bit_equal(ours, ref)
+
+
+@pytest.mark.gpu
+def test_blocked_rbgs_tiled_grid_matches_reference_library(sf, lib, ref_lib, cuda):
+    scene = _tiled_scene(sf, (200, 60, 40), sf.scenes.benchmark_walls())
+    outs = []
+    for L, o in ((lib, 2), (ref_lib, None)):
+        opts = None
+        if o is not None:
+            opts = sf.default_options(lib)
+            opts.iterations_per_pass = o
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=L, options=opts)
+        sf.scenes.run(sim, scene)
+        outs.append(C.collect_outputs(sim, sf, C.Case("t", scene.config, scene.scalars, scene.vectors, scene.steps)))
+        sim.close()
+    assert_bit_equal(outs[0], outs[1])

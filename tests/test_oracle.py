@@ -57,8 +57,9 @@ def test_fp32_instance_tracks_fp64(sf, orc):
 
 def test_mirror_symmetry(sf, orc):
     """A source centred in x under symmetric walls keeps the density mirror
-    symmetric in x and u_x antisymmetric (FP64)."""
-    sc = sf.scenes.plume("sym", (16, 12, 10), sources=[(8.0, 4.0, 5.0, 3.0, 10.0, 5.0)], diffuse_iterations=4, pressure_iterations=8)
+    symmetric in x and u_x antisymmetric (FP64). nx is odd so that the
+    mirror x -> nx-1-x keeps every cell's red-black colour."""
+    sc = sf.scenes.plume("sym", (15, 12, 10), sources=[(7.5, 4.0, 5.0, 3.0, 10.0, 5.0)], diffuse_iterations=4, pressure_iterations=8)
     o = orc.Oracle(sc.config, sc.scalars, sc.vectors, precision=64)
     sf.scenes.run(o, sc, steps=3)
     rho = o.get(orc.SCALAR, 1)
