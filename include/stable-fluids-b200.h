@@ -102,6 +102,22 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_enqueue_stage(void* cont
 
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_get_step_info(void* context, StableFluidsB200StepInfo* out_info);
 
+/* No counterpart in the reference. The FP64 relative Poisson residual
+ * ||b - A p|| / ||b|| (b = h^2 divergence, mean removed when no face is
+ * OUTFLOW; A p = sum of the 6 neighbours - 6 p with the pressure ghost rules)
+ * of caller-provided dense nx*ny*nz FP32 device arrays, written as
+ * {rel_residual, ||b||} to out_residual (2 doubles of device-accessible
+ * memory), enqueued on `stream`. It allocates nothing -- for callers that
+ * cannot call cudaMalloc at that point (allocation-free frame phases, fully
+ * pooled device memory, host callbacks): its scratch is a fixed 128 KiB
+ * device array owned by the library on every device that loads it.
+ * Limits: nz <= 4096 (larger grids return BACKEND_FAILURE); calls that
+ * overlap on the GPU race on the shared scratch (order them on one stream);
+ * the first call on a device looks up the scratch address, so make it before
+ * any stream capture. Same numbers as the step's residual measurement up to
+ * FP64 summation order. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_pressure_residual_noalloc(const float* pressure, const float* divergence, int32_t nx, int32_t ny, int32_t nz, float cell_size, const StableFluidsFlowBoundaryConfig* flow_boundary, double* out_residual, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

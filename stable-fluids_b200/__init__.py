@@ -129,6 +129,7 @@ B200_SYMBOLS = (
     "stable_fluids_b200_get_step_stats",
     "stable_fluids_b200_enqueue_stage",
     "stable_fluids_b200_get_step_info",
+    "stable_fluids_b200_pressure_residual_noalloc",
 )
 
 (STAGE_FORCES, STAGE_VELOCITY_ADVECTION, STAGE_VELOCITY_DIFFUSION, STAGE_DIVERGENCE, STAGE_PRESSURE,
@@ -156,6 +157,7 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_get_step_stats.argtypes = [P, POINTER(B200StepStats)]
         lib.stable_fluids_b200_enqueue_stage.argtypes = [P, c_uint32, POINTER(c_int32)]
         lib.stable_fluids_b200_get_step_info.argtypes = [P, POINTER(B200StepInfo)]
+        lib.stable_fluids_b200_pressure_residual_noalloc.argtypes = [P, P, c_int32, c_int32, c_int32, c_float, POINTER(FlowBoundary), P, P]
         for name in B200_SYMBOLS:
             getattr(lib, name).restype = c_int32
     return lib
