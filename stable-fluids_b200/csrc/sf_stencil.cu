@@ -118,10 +118,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         const dim3 cblock(32, 8, 1);
         const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
-        for (int it = 0; it < a.iterations; ++it) {
-            k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, 0, d, a.flow, a.scalar);
-            k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, 1, d, a.flow, a.scalar);
-        }
+        for (int it = 0; it < a.iterations; ++it)
+            for (int parity = 0; parity < 2; ++parity) k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, parity, d, a.flow, a.scalar);
         if (a.launches) *a.launches += 2 * a.iterations;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
