@@ -55,6 +55,7 @@ struct Context {
     StableFluidsSimulationConfig config{};
     StableFluidsB200Options options{};
     cudaStream_t stream = nullptr;
+    cudaStream_t body_stream = nullptr;  // captures the body of the residual-driven loop
     bool owns_stream = false;
     Dims dims{};
     size_t cells = 0;
@@ -88,6 +89,7 @@ struct Context {
         if (ready) cudaEventDestroy(ready);
         if (slab) cudaFree(slab);
         if (host_stats) cudaFreeHost(host_stats);
+        if (body_stream) cudaStreamDestroy(body_stream);
         if (owns_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -291,14 +293,69 @@ struct Stages {
     // 5. pressure from zero (:644-649) or from the previous step's pressure.
     void pressure() {
         const int init = c.options.warm_start == STABLE_FLUIDS_B200_WARM_START_PREVIOUS ? INIT_FROM_X : INIT_ZERO;
+        if (c.options.residual_tolerance > 0.0f && capturing()) {
+            pressure_until_converged(init);
+            return;
+        }
         ok(launch_stencil(stencil(KIND_PRESSURE, init, c.config.pressure_iterations, h() * h(), c.pressure, c.divergence), c.stream), 0);
     }
 
+    bool capturing() const {
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        return cudaStreamIsCapturing(c.stream, &st) == cudaSuccess && st == cudaStreamCaptureStatusActive;
+    }
+
+    // Residual-driven solve: measure rel_res of the initial pressure, then a
+    // WHILE graph node repeats {check_interval iterations, FP64 residual} while
+    // rel_res > tolerance and fewer than max_pressure_iterations have run
+    // (the count is rounded up to a multiple of the interval).
+    void pressure_until_converged(int init) {
+        const int interval = c.options.residual_check_interval;
+        const int max_it = ((c.options.max_pressure_iterations + interval - 1) / interval) * interval;
+        const int singular = c.flow.any_outflow ? 0 : 1;
+        const double tol = static_cast<double>(c.options.residual_tolerance);
+        if (init == INIT_ZERO) ok(cudaMemsetAsync(c.pressure, 0, c.field_bytes, c.stream), 0);
+        ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+        ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
+        cudaStreamCaptureStatus st;
+        cudaGraph_t graph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraphConditionalHandle handle{};
+        if (!ok(cudaStreamGetCaptureInfo(c.stream, &st, nullptr, &graph, &deps, &ndeps), 0)) return;
+        if (!ok(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0), 0)) return;
+        ok(launch_residual_check(c.stats, c.dims, singular, -1, tol, max_it, handle, c.stream));
+        if (!ok(cudaStreamGetCaptureInfo(c.stream, &st, nullptr, &graph, &deps, &ndeps), 0)) return;
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        if (!ok(cudaGraphAddNode(&node, graph, deps, ndeps, &cp), 0)) return;
+        if (!ok(cudaStreamUpdateCaptureDependencies(c.stream, &node, 1, cudaStreamSetCaptureDependencies), 0)) return;
+        // the body, captured on the second stream
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        if (!ok(cudaStreamBeginCaptureToGraph(c.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), 0)) return;
+        const cudaStream_t main = c.stream;
+        c.stream = c.body_stream;
+        ok(launch_stencil(stencil(KIND_PRESSURE, INIT_FROM_X, interval, h() * h(), c.pressure, c.divergence), c.stream), 0);
+        ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
+        ok(launch_residual_check(c.stats, c.dims, singular, interval, tol, max_it, handle, c.stream));
+        c.stream = main;
+        cudaGraph_t captured = nullptr;
+        ok(cudaStreamEndCapture(c.body_stream, &captured), 0);
+        residual_measured = true;
+    }
+    bool residual_measured = false;
+
     // 6. projection (:650) + the FP64 residual of the pressure solve.
     void project() {
-        if (c.residual_enabled) ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
-        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, c.residual_enabled ? c.stats : nullptr, c.stream));
-        if (c.residual_enabled) ok(launch_residual_finalize(c.stats, c.dims, c.flow.any_outflow ? 0 : 1, c.config.pressure_iterations, c.stream));
+        // the residual-driven solve has measured the residual already
+        const bool measure = c.residual_enabled && !residual_measured;
+        if (measure) ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, measure ? c.stats : nullptr, c.stream));
+        if (measure) ok(launch_residual_finalize(c.stats, c.dims, c.flow.any_outflow ? 0 : 1, c.config.pressure_iterations, c.stream));
     }
 
     // 7. scalars: source, advection by the projected velocity, diffusion,
@@ -390,6 +447,7 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         c->owns_stream = true;
     }
+    if (cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
 
     {
         Range alloc("stable.create_context.alloc");

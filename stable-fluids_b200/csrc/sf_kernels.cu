@@ -249,6 +249,31 @@ __global__ void k_residual_finalize(DeviceStats* s, double n, int singular, int 
     if (iterations >= 0) s->iterations = iterations;
 }
 
+// Residual-driven pressure solve: turns the accumulated sums into rel_res,
+// counts the iterations run (reset < 0 sets the count to zero), zeroes the
+// sums for the next measurement, and continues the enclosing WHILE graph
+// node while rel_res > tol and fewer than max_iterations have run.
+__global__ void k_residual_check(DeviceStats* s, double n, int singular, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double r2 = s->sum_e2, b2 = s->sum_b2;
+    if (singular) {
+        const double mb = s->sum_b / n;
+        r2 = s->sum_e2 - 2.0 * mb * s->sum_e + n * mb * mb;
+        b2 = s->sum_b2 - n * mb * mb;
+    }
+    r2 = r2 < 0.0 ? 0.0 : r2;
+    b2 = b2 < 0.0 ? 0.0 : b2;
+    const double rel = b2 > 0.0 ? sqrt(r2) / sqrt(b2) : 0.0;
+    s->rhs_norm = sqrt(b2);
+    s->rel_residual = rel;
+    s->iterations = increment < 0 ? 0 : s->iterations + increment;
+    s->sum_e = s->sum_e2 = s->sum_b = s->sum_b2 = 0.0;
+    const bool more = rel > tol && s->iterations < max_iterations;
+    s->hit_cap = (rel > tol && !more) ? 1 : 0;
+    s->keep_going = more ? 1 : 0;
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
 // ----------------------------------------------------------- diagnostics --
 // Post-projection divergence (backend-cuda.cu:670) and |u| (:424-434) in one pass.
 __global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, Dims d, float h, FlowBC b) {
@@ -311,6 +336,12 @@ cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float
 cudaError_t launch_residual_finalize(DeviceStats* stats, Dims d, int singular, int iterations, cudaStream_t s) {
     const double n = static_cast<double>(d.nx) * static_cast<double>(d.ny) * static_cast<double>(d.nz);
     k_residual_finalize<<<1, 32, 0, s>>>(stats, n, singular, iterations);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s) {
+    const double n = static_cast<double>(d.nx) * static_cast<double>(d.ny) * static_cast<double>(d.nz);
+    k_residual_check<<<1, 32, 0, s>>>(stats, n, singular, increment, tol, max_iterations, handle);
     return cudaGetLastError();
 }
 

@@ -270,3 +270,53 @@ def test_blocked_rbgs_tiled_grid_matches_reference_library(sf, lib, ref_lib, cud
         outs.append(C.collect_outputs(sim, sf, C.Case("t", scene.config, scene.scalars, scene.vectors, scene.steps)))
         sim.close()
     assert_bit_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["walls_16x12x10", "benchmark_walls_16x12x16", "mixed_odd_17x9x13"])
+@pytest.mark.parametrize("scheme", [0, 1])
+@pytest.mark.parametrize("warm", [False, True])
+def test_residual_driven_solve_matches_oracle(name, scheme, warm, sf, lib, orc, cuda):
+    """Pressure iterated inside the step graph (WHILE node) until the FP64
+    relative residual <= 1e-3: same iteration counts, residuals and fields as
+    the oracle's loop."""
+    case = CASES[name]
+    tol, interval, cap = 1e-3, 4, 2000
+    opts = sf.default_options(lib)
+    opts.scheme = scheme
+    opts.residual_tolerance = tol
+    opts.residual_check_interval = interval
+    opts.max_pressure_iterations = cap
+    opts.warm_start = sf.WARM_START_PREVIOUS if warm else sf.WARM_START_ZERO
+    sim = sf.Simulation(case.config, case.scalars, case.vectors, lib=lib, options=opts)
+    o = orc.Oracle(case.config, case.scalars, case.vectors, precision=32, scheme=scheme)
+    o.set_solver(tolerance=tol, max_iterations=cap, check_interval=interval, warm_previous=warm)
+    for k in range(case.steps):
+        case.drive(sim, steps=1, start=k)
+        case.drive(o, steps=1, start=k)
+        st = sim.stats()
+        ost = o.stats()
+        info = (k, st.pressure_iterations, st.rel_residual, st.hit_cap, ost)
+        assert st.pressure_iterations == ost["iterations"], info
+        assert st.hit_cap == ost["hit_cap"], info
+        assert st.rel_residual <= tol or st.hit_cap == 1
+        assert abs(st.rel_residual - ost["rel_residual"]) <= 1e-6 * ost["rel_residual"] + 1e-12
+    ours = C.collect_outputs(sim, sf, case)
+    ref = C.collect_oracle(o, orc, case)
+    sim.close()
+    err = errors(ours, ref, ORACLE_FLOOR)
+    assert max(err.values()) <= ORACLE_TOL, err
+
+
+@pytest.mark.gpu
+def test_residual_driven_solve_stops_at_cap(sf, lib, cuda):
+    case = CASES["walls_16x12x10"]
+    opts = sf.default_options(lib)
+    opts.residual_tolerance = 1e-9
+    opts.residual_check_interval = 4
+    opts.max_pressure_iterations = 10  # rounded up to 12
+    sim = sf.Simulation(case.config, case.scalars, case.vectors, lib=lib, options=opts)
+    case.drive(sim, steps=1)
+    st = sim.stats()
+    sim.close()
+    assert st.hit_cap == 1 and st.pressure_iterations == 12 and st.rel_residual > 1e-9
