@@ -59,6 +59,10 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
+    p.add_argument("--equal-residual", default="rbgs-zero,rbgs-previous,jacobi-previous", help="solver variants timed at equal rel_res (empty: skip)")
+    p.add_argument("--residual-tolerance", type=float, default=1e-3)
+    p.add_argument("--residual-steps", type=int, default=3)
+    p.add_argument("--residual-cap", type=int, default=20000)
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -210,6 +214,41 @@ def e2e_run(sf, sim, scene, steps):
     return t, 3 * n * 4, n * 4
 
 
+def equal_residual(sf, scene, variants, tol, steps, cap, warmup):
+    """Steps/s of the plume when the pressure is iterated until the FP64
+    relative Poisson residual is <= tol (inside the step graph), for solver
+    variants scheme-warmstart; reports the iterations each step needed."""
+    import torch
+
+    out = {}
+    for v in variants:
+        scheme, warm = v.split("-")
+        opts = sf.default_options()
+        opts.scheme = sf.SCHEME_JACOBI if scheme == "jacobi" else sf.SCHEME_RBGS
+        opts.warm_start = {"zero": sf.WARM_START_ZERO, "previous": sf.WARM_START_PREVIOUS}[warm]
+        opts.residual_tolerance = tol
+        opts.residual_check_interval = 16
+        opts.max_pressure_iterations = cap
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts)
+        sf.scenes.apply_inputs(sim, scene, 0)
+        sim.step(warmup)
+        torch.cuda.synchronize()
+        its, res, total = [], [], 0.0
+        for _ in range(steps):
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(sim.stream)
+            sim.step(1)
+            end.record(sim.stream)
+            st = sim.stats()
+            total += start.elapsed_time(end) / 1000.0
+            its.append(st.pressure_iterations)
+            res.append(st.rel_residual)
+        sim.close()
+        out[v] = {"steps_per_s": steps / total, "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > tol for r in res)}
+    return out
+
+
 def cpu_baseline(sf, scene, steps):
     from oracle import oracle as orc
 
@@ -308,6 +347,9 @@ def main():
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c
+    if rank == 0 and world == 1 and args.equal_residual:
+        variants = [v for v in args.equal_residual.split(",") if v]
+        line["equal_residual"] = {"tolerance": args.residual_tolerance, "steps": args.residual_steps, "warmup": 2, "variants": equal_residual(sf, scene, variants, args.residual_tolerance, args.residual_steps, args.residual_cap, 2)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sf, scene, args.cpu_steps)
     sim.close()

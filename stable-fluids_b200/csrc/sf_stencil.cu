@@ -90,15 +90,36 @@ __global__ void __launch_bounds__(256) k_rbgs_colour(float* x, const float* __re
     }
 }
 
+// One Jacobi sweep, dst = update(src): thread (x, y) owns the cells of
+// kColourPlanes consecutive planes; interior cells read their neighbours
+// directly, boundary cells use the ghost rules.
 template <int KIND>
 __global__ void __launch_bounds__(256) k_jacobi(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, Dims d, FlowBC fb, ScalarBC sb) {
     const int cx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
-    const int z = static_cast<int>(blockIdx.z * blockDim.z + threadIdx.z);
-    if (cx >= d.nx || y >= d.ny || z >= d.nz) return;
-    const float nb = neighbour_sum<KIND>(src, cx, y, z, d, fb, sb);
-    const size_t i = lin(cx, y, z, d);
-    dst[i] = update<KIND>(nb, rhs[i], coef);
+    const int z0 = static_cast<int>(blockIdx.z) * kColourPlanes;
+    if (cx >= d.nx || y >= d.ny) return;
+    const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    const bool xy_interior = cx >= 1 && cx <= d.nx - 2 && y >= 1 && y <= d.ny - 2;
+#pragma unroll
+    for (int k = 0; k < kColourPlanes; ++k) {
+        const int z = z0 + k;
+        if (z >= d.nz) break;
+        const size_t i = lin(cx, y, z, d);
+        float nb;
+        if (xy_interior && z >= 1 && z <= d.nz - 2) {
+            const float* c = src + i;
+            nb = c[-1] + c[1] + c[-static_cast<ptrdiff_t>(sy)] + c[sy] + c[-static_cast<ptrdiff_t>(sz)] + c[sz];
+        } else {
+            nb = neighbour_sum<KIND>(src, cx, y, z, d, fb, sb);
+        }
+        const float num = tb::numerator<KIND>(nb, rhs[i], coef);
+        float q = tb::markstein_div(num, divisor, recip);
+        if (tb::needs_ieee_div(num)) q = num / divisor;
+        dst[i] = q;
+    }
 }
 
 __global__ void k_scale_field(float* __restrict__ q, float factor, size_t n) {
@@ -123,7 +144,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         if (a.launches) *a.launches += 2 * a.iterations;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
-        const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 3) / 4), static_cast<unsigned>((d.nz + 1) / 2));
+        const dim3 jblock(32, 8, 1);
+        const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
         // Choose the first source so that the last sweep lands in x.
         const float* src = a.x;
         if (a.init == INIT_FROM_B) src = a.b;
@@ -141,7 +163,7 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             const int left = a.iterations - it;  // sweeps still to run, this one included
             float* dst = (left & 1) ? a.x : a.scratch;
             if (dst == src) dst = (dst == a.x) ? a.scratch : a.x;
-            k_jacobi<KIND><<<grid, block, 0, s>>>(dst, src, a.b, a.coef, d, a.flow, a.scalar);
+            k_jacobi<KIND><<<grid, jblock, 0, s>>>(dst, src, a.b, a.coef, d, a.flow, a.scalar);
             src = dst;
         }
         if (a.launches) *a.launches += a.iterations;
