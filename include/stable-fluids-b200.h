@@ -49,7 +49,10 @@ typedef struct StableFluidsB200Options {
     int32_t max_pressure_iterations;  /* cap of the residual-driven solve */
     int32_t residual_check_interval;  /* iterations between residual checks (>= 1) */
     uint32_t compute_residual;        /* 1: measure rel_res after every pressure solve */
-    uint32_t reserved[9];
+    int32_t warm_start_trial_iterations; /* learned warm start: sweeps run on the learned and on the
+                                          * previous-pressure start before the one with the smaller
+                                          * rel_res is kept (0 = compare the starts themselves) */
+    uint32_t reserved[8];
 } StableFluidsB200Options;
 
 /* Statistics of the most recent step (device values copied to the host). */
@@ -101,6 +104,55 @@ typedef struct StableFluidsB200StepInfo {
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_enqueue_stage(void* context, uint32_t stage, int32_t* out_kernel_launches);
 
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_get_step_info(void* context, StableFluidsB200StepInfo* out_info);
+
+/* ---- Learned pressure warm start (no counterpart in the reference) ----
+ *
+ * A 3-level 3D U-Net (16/32/64 channels, two 3x3x3 convolutions + ReLU per
+ * level and side, 2x average pooling, nearest upsampling with skip
+ * concatenation, a final 3x3x3 convolution to one channel), BF16 weights and
+ * activations, FP32 accumulation on the tensor cores. Input: the pressure
+ * right-hand side b = h^2 div and the previous pressure, both scaled by
+ * 1 / rms(b); output: the scaled correction, p0 = p_prev + out * rms(b).
+ * Grid sides must be multiples of 4.
+ *
+ * Parameters are FP32, one block per layer in forward order (enc0a enc0b
+ * enc1a enc1b bott_a bott_b dec1a dec1b dec0a dec0b out): weights
+ * [27 taps][cout][cin] (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)) then cout biases,
+ * with (cin, cout) = (16,16) (16,16) (16,32) (32,32) (32,64) (64,64) (96,32)
+ * (32,32) (48,16) (16,16) (16,16); input channels 2..15 of the first layer
+ * and output channels 1..15 of the last are padding (zero, never updated).
+ *
+ * A network object serves one stream at a time (its activation buffers are
+ * shared by every call); all entry points except predict are synchronous.
+ */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_create(uint32_t seed, void** out_network);
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_destroy(void* network);
+/* Parameter count and (if out_host_values != null) a host copy of them. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_parameters(void* network, uint64_t* out_count, float* out_host_values);
+/* Loads parameters from host memory and resets the optimizer state. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_set_parameters(void* network, const float* host_values);
+/* out_pressure = the warm start computed from device arrays
+ * (previous_pressure may be null = zero, and may equal out_pressure),
+ * enqueued on `stream`. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_predict(void* network, const float* divergence, const float* previous_pressure, int32_t nx, int32_t ny, int32_t nz, float cell_size, float* out_pressure, void* stream);
+/* Mean squared error between the network output and the scaled correction
+ * towards target_pressure, (target - previous) / rms(b), and (if
+ * out_host_gradients != null) its gradient with respect to every parameter,
+ * in the parameter layout. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_gradients(void* network, const float* divergence, const float* previous_pressure, const float* target_pressure, int32_t nx, int32_t ny, int32_t nz, float cell_size, double* out_loss, float* out_host_gradients, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on that loss; *out_loss is the
+ * loss before the step. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_train_step(void* network, const float* divergence, const float* previous_pressure, const float* target_pressure, int32_t nx, int32_t ny, int32_t nz, float cell_size, float learning_rate, double* out_loss, void* stream);
+/* Uses `network` for the pressure warm start of a context created with
+ * warm_start = LEARNED and rebuilds its step graph (null detaches). Until a
+ * network is attached such a context starts from the previous pressure and
+ * reports used_fallback = 1. With a network, each step predicts a start,
+ * runs warm_start_trial_iterations sweeps on it and on the previous
+ * pressure, and continues from the one with the smaller residual
+ * (used_fallback = 1 when that is the previous pressure); the sweeps of the
+ * trial count towards the step's iterations. The network must outlive the
+ * attachment and must not be used on another stream while the context steps. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network);
 
 /* No counterpart in the reference. The FP64 relative Poisson residual
  * ||b - A p|| / ||b|| (b = h^2 divergence, mean removed when no face is

@@ -103,7 +103,7 @@ class B200Options(ctypes.Structure):
         ("scheme", c_uint32), ("warm_start", c_uint32), ("iterations_per_pass", c_int32),
         ("residual_tolerance", c_float), ("max_pressure_iterations", c_int32),
         ("residual_check_interval", c_int32), ("compute_residual", c_uint32),
-        ("reserved", c_uint32 * 9),
+        ("warm_start_trial_iterations", c_int32), ("reserved", c_uint32 * 8),
     ]
 
 
@@ -130,6 +130,14 @@ B200_SYMBOLS = (
     "stable_fluids_b200_enqueue_stage",
     "stable_fluids_b200_get_step_info",
     "stable_fluids_b200_pressure_residual_noalloc",
+    "stable_fluids_b200_network_create",
+    "stable_fluids_b200_network_destroy",
+    "stable_fluids_b200_network_parameters",
+    "stable_fluids_b200_network_set_parameters",
+    "stable_fluids_b200_network_predict",
+    "stable_fluids_b200_network_gradients",
+    "stable_fluids_b200_network_train_step",
+    "stable_fluids_b200_attach_network",
 )
 
 (STAGE_FORCES, STAGE_VELOCITY_ADVECTION, STAGE_VELOCITY_DIFFUSION, STAGE_DIVERGENCE, STAGE_PRESSURE,
@@ -158,6 +166,14 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_enqueue_stage.argtypes = [P, c_uint32, POINTER(c_int32)]
         lib.stable_fluids_b200_get_step_info.argtypes = [P, POINTER(B200StepInfo)]
         lib.stable_fluids_b200_pressure_residual_noalloc.argtypes = [P, P, c_int32, c_int32, c_int32, c_float, POINTER(FlowBoundary), P, P]
+        lib.stable_fluids_b200_network_create.argtypes = [c_uint32, POINTER(c_void_p)]
+        lib.stable_fluids_b200_network_destroy.argtypes = [P]
+        lib.stable_fluids_b200_network_parameters.argtypes = [P, POINTER(c_uint64), P]
+        lib.stable_fluids_b200_network_set_parameters.argtypes = [P, P]
+        lib.stable_fluids_b200_network_predict.argtypes = [P, P, P, c_int32, c_int32, c_int32, c_float, P, P]
+        lib.stable_fluids_b200_network_gradients.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, POINTER(c_double), P, P]
+        lib.stable_fluids_b200_network_train_step.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, c_float, POINTER(c_double), P]
+        lib.stable_fluids_b200_attach_network.argtypes = [P, P]
         for name in B200_SYMBOLS:
             getattr(lib, name).restype = c_int32
     return lib
@@ -186,9 +202,10 @@ def default_options(lib: ctypes.CDLL | None = None) -> B200Options:
 
 from .simulation import Simulation, StableFluidsError  # noqa: E402  (needs the structs above)
 from . import scenes  # noqa: E402
+from .warmstart import WarmStartNetwork, LAYERS as NETWORK_LAYERS  # noqa: E402
 
 __all__ = [
-    "Simulation", "StableFluidsError", "load_library", "default_options", "scenes",
+    "Simulation", "StableFluidsError", "load_library", "default_options", "scenes", "WarmStartNetwork", "NETWORK_LAYERS",
     "SimulationConfig", "ScalarFieldDesc", "VectorFieldDesc", "ContextCreateDesc", "FlowBoundary", "FlowFace",
     "ScalarBoundary", "ScalarFace", "ViewRequest", "View", "B200Options", "B200StepStats", "B200StepInfo",
 ]

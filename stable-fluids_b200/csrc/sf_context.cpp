@@ -25,6 +25,7 @@
 
 #include "sf_launch.h"
 #include "sf_types.h"
+#include "sf_unet.h"
 #include "stable-fluids-3d.h"
 #include "stable-fluids-b200.h"
 
@@ -73,6 +74,12 @@ struct Context {
     float* scratch = nullptr;
     DeviceStats* stats = nullptr;
     DeviceStats* host_stats = nullptr;  // pinned
+    // learned warm start: the network (not owned), the plain candidate and
+    // its Jacobi scratch, and the plain candidate's residual sums
+    net::Net* network = nullptr;
+    float* alt = nullptr;
+    float* alt_scratch = nullptr;
+    DeviceStats* alt_stats = nullptr;
     std::vector<ScalarField> scalars;
     std::vector<VectorField> vectors;
 
@@ -163,6 +170,7 @@ void apply_env_overrides(StableFluidsB200Options& o) {
         const std::string_view s(v);
         if (s == "previous" || s == "1") o.warm_start = STABLE_FLUIDS_B200_WARM_START_PREVIOUS;
         else if (s == "zero" || s == "0") o.warm_start = STABLE_FLUIDS_B200_WARM_START_ZERO;
+        else if (s == "learned" || s == "2") o.warm_start = STABLE_FLUIDS_B200_WARM_START_LEARNED;
     }
     if (env_flag("STABLE_FLUIDS_B200_COMPUTE_RESIDUAL")) o.compute_residual = 1;
 }
@@ -176,11 +184,13 @@ void default_options(StableFluidsB200Options& o) {
     o.max_pressure_iterations = 0;
     o.residual_check_interval = 8;
     o.compute_residual = 0;
+    o.warm_start_trial_iterations = 8;
 }
 
 bool validate_options(const StableFluidsB200Options& o) {
     if (o.scheme > STABLE_FLUIDS_B200_SCHEME_JACOBI) return false;
-    if (o.warm_start > STABLE_FLUIDS_B200_WARM_START_PREVIOUS) return false;  // learned: not in this build yet
+    if (o.warm_start > STABLE_FLUIDS_B200_WARM_START_LEARNED) return false;
+    if (o.warm_start_trial_iterations < 0) return false;
     if (o.iterations_per_pass < 0) return false;
     if (!(o.residual_tolerance >= 0.0f) || !std::isfinite(o.residual_tolerance)) return false;
     if (o.residual_tolerance > 0.0f && (o.max_pressure_iterations <= 0 || o.residual_check_interval <= 0)) return false;
@@ -290,14 +300,44 @@ struct Stages {
     // 4. divergence (:643).
     void divergence() { ok(launch_divergence(c.divergence, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.stream)); }
 
-    // 5. pressure from zero (:644-649) or from the previous step's pressure.
+    // 5. pressure from zero (:644-649), from the previous step's pressure, or
+    //    from the learned warm start.
     void pressure() {
-        const int init = c.options.warm_start == STABLE_FLUIDS_B200_WARM_START_PREVIOUS ? INIT_FROM_X : INIT_ZERO;
-        if (c.options.residual_tolerance > 0.0f && capturing()) {
-            pressure_until_converged(init);
+        const int init = c.options.warm_start == STABLE_FLUIDS_B200_WARM_START_ZERO ? INIT_ZERO : INIT_FROM_X;
+        const bool residual_driven = c.options.residual_tolerance > 0.0f && capturing();
+        int done = 0;  // iterations already run on the start that was kept
+        if (c.options.warm_start == STABLE_FLUIDS_B200_WARM_START_LEARNED && c.network != nullptr) done = learned_start(residual_driven);
+        if (residual_driven) {
+            pressure_until_converged(init, done);
             return;
         }
-        ok(launch_stencil(stencil(KIND_PRESSURE, init, c.config.pressure_iterations, h() * h(), c.pressure, c.divergence), c.stream), 0);
+        const int left = c.config.pressure_iterations - done;
+        if (left > 0) ok(launch_stencil(stencil(KIND_PRESSURE, init, left, h() * h(), c.pressure, c.divergence), c.stream), 0);
+    }
+
+    // Learned warm start: the network predicts a start from (div, previous
+    // pressure) in place; the previous pressure is kept as the plain
+    // candidate. Both get the trial sweeps, both residuals are measured, and
+    // the one with the smaller residual stays in c.pressure (its sums in
+    // c.stats, the decision in used_fallback). Returns the sweeps run.
+    int learned_start(bool residual_driven) {
+        int trial = c.options.warm_start_trial_iterations;
+        if (!residual_driven) trial = std::min(trial, c.config.pressure_iterations);
+        ok(cudaMemcpyAsync(c.alt, c.pressure, c.field_bytes, cudaMemcpyDeviceToDevice, c.stream), 0);
+        int predicted = 0;
+        if (ok(net::predict(c.network, c.divergence, h() * h(), c.pressure, c.pressure, c.dims, c.stream, &predicted), 0)) launches += predicted;
+        if (trial > 0) {
+            ok(launch_stencil(stencil(KIND_PRESSURE, INIT_FROM_X, trial, h() * h(), c.pressure, c.divergence), c.stream), 0);
+            auto a = stencil(KIND_PRESSURE, INIT_FROM_X, trial, h() * h(), c.alt, c.divergence);
+            a.scratch = c.alt_scratch;
+            ok(launch_stencil(a, c.stream), 0);
+        }
+        ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+        ok(cudaMemsetAsync(c.alt_stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+        ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
+        ok(launch_residual_sums(c.alt, c.divergence, c.dims, h() * h(), c.flow, c.alt_stats, c.stream));
+        ok(launch_warm_start_select(c.stats, c.alt_stats, c.dims, c.flow.any_outflow ? 0 : 1, c.pressure, c.alt, c.stream), 2);
+        return trial;
     }
 
     bool capturing() const {
@@ -309,14 +349,18 @@ struct Stages {
     // WHILE graph node repeats {check_interval iterations, FP64 residual} while
     // rel_res > tolerance and fewer than max_pressure_iterations have run
     // (the count is rounded up to a multiple of the interval).
-    void pressure_until_converged(int init) {
+    // `done` iterations have run already (learned warm start), with the sums
+    // of the current pressure in c.stats.
+    void pressure_until_converged(int init, int done) {
         const int interval = c.options.residual_check_interval;
         const int max_it = ((c.options.max_pressure_iterations + interval - 1) / interval) * interval;
         const int singular = c.flow.any_outflow ? 0 : 1;
         const double tol = static_cast<double>(c.options.residual_tolerance);
-        if (init == INIT_ZERO) ok(cudaMemsetAsync(c.pressure, 0, c.field_bytes, c.stream), 0);
-        ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
-        ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
+        if (done == 0) {
+            if (init == INIT_ZERO) ok(cudaMemsetAsync(c.pressure, 0, c.field_bytes, c.stream), 0);
+            ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+            ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
+        }
         cudaStreamCaptureStatus st;
         cudaGraph_t graph = nullptr;
         const cudaGraphNode_t* deps = nullptr;
@@ -324,7 +368,7 @@ struct Stages {
         cudaGraphConditionalHandle handle{};
         if (!ok(cudaStreamGetCaptureInfo(c.stream, &st, nullptr, &graph, &deps, &ndeps), 0)) return;
         if (!ok(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0), 0)) return;
-        ok(launch_residual_check(c.stats, c.dims, singular, -1, tol, max_it, handle, c.stream));
+        ok(launch_residual_check(c.stats, c.dims, singular, 1, done, tol, max_it, handle, c.stream));
         if (!ok(cudaStreamGetCaptureInfo(c.stream, &st, nullptr, &graph, &deps, &ndeps), 0)) return;
         cudaGraphNodeParams cp{};
         cp.type = cudaGraphNodeTypeConditional;
@@ -341,7 +385,7 @@ struct Stages {
         c.stream = c.body_stream;
         ok(launch_stencil(stencil(KIND_PRESSURE, INIT_FROM_X, interval, h() * h(), c.pressure, c.divergence), c.stream), 0);
         ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
-        ok(launch_residual_check(c.stats, c.dims, singular, interval, tol, max_it, handle, c.stream));
+        ok(launch_residual_check(c.stats, c.dims, singular, 0, interval, tol, max_it, handle, c.stream));
         c.stream = main;
         cudaGraph_t captured = nullptr;
         ok(cudaStreamEndCapture(c.body_stream, &captured), 0);
@@ -392,6 +436,34 @@ struct Stages {
         return e;
     }
 };
+
+// The whole step as one graph (:608-675), replacing any previous one.
+// Thread-local capture so other host threads' CUDA calls are unaffected.
+cudaError_t build_graph(Context& c) {
+    Range range("stable.create_context.graph");
+    if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+    c.exec = nullptr;
+    c.graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    Stages st{c};
+    const cudaError_t rec = st.whole_step();
+    c.step_kernels = st.launches;
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(c.stream, &g);
+    c.graph = g;
+    if (rec != cudaSuccess || end != cudaSuccess || g == nullptr) {
+        cudaGetLastError();
+        return rec != cudaSuccess ? rec : (end != cudaSuccess ? end : cudaErrorStreamCaptureInvalidated);
+    }
+    if ((e = cudaGraphInstantiate(&c.exec, c.graph, 0)) != cudaSuccess) {
+        c.exec = nullptr;
+        cudaGetLastError();
+        return e;
+    }
+    return cudaSuccess;
+}
 
 StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const StableFluidsB200Options* options_in, bool env, void** out_context, StableFluidsScalarFieldHandle* out_s, uint32_t cap_s, StableFluidsVectorFieldHandle* out_v, uint32_t cap_v) {
     Range range("stable.create_context");
@@ -461,6 +533,11 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         plan.add(reinterpret_cast<void**>(&c->magnitude), fb);
         plan.add(reinterpret_cast<void**>(&c->scratch), fb);
         plan.add(reinterpret_cast<void**>(&c->stats), sizeof(DeviceStats));
+        if (options.warm_start == STABLE_FLUIDS_B200_WARM_START_LEARNED) {
+            plan.add(reinterpret_cast<void**>(&c->alt), fb);
+            plan.add(reinterpret_cast<void**>(&c->alt_scratch), fb);
+            plan.add(reinterpret_cast<void**>(&c->alt_stats), sizeof(DeviceStats));
+        }
         for (auto& f : c->scalars) {
             plan.add(reinterpret_cast<void**>(&f.data), fb);
             plan.add(reinterpret_cast<void**>(&f.temp), fb);
@@ -503,27 +580,7 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         }
     }
 
-    {
-        // The whole step as one graph (:608-675). Thread-local capture so
-        // other host threads' CUDA calls are unaffected.
-        Range graph("stable.create_context.graph");
-        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        Stages st{*c};
-        const cudaError_t rec = st.whole_step();
-        c->step_kernels = st.launches;
-        cudaGraph_t g = nullptr;
-        const cudaError_t end = cudaStreamEndCapture(c->stream, &g);
-        c->graph = g;
-        if (rec != cudaSuccess || end != cudaSuccess || g == nullptr) {
-            cudaGetLastError();
-            return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        }
-        if (cudaGraphInstantiate(&c->exec, c->graph, 0) != cudaSuccess) {
-            c->exec = nullptr;
-            cudaGetLastError();
-            return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        }
-    }
+    if (build_graph(*c) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (cudaGetLastError() != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     *out_context = c.release();
     return STABLE_FLUIDS_RESULT_OK;
@@ -664,7 +721,9 @@ StableFluidsResult stable_fluids_b200_get_step_stats(void* context, StableFluids
     o.rhs_norm = c.residual_enabled ? d.rhs_norm : 0.0;
     o.pressure_iterations = c.residual_enabled ? d.iterations : c.config.pressure_iterations;
     o.hit_cap = d.hit_cap;
-    o.used_fallback = d.used_fallback;
+    // a learned-start context without a network runs the previous-pressure start
+    const bool learned = c.options.warm_start == STABLE_FLUIDS_B200_WARM_START_LEARNED;
+    o.used_fallback = learned ? (c.network == nullptr ? 1 : d.used_fallback) : 0;
     *out_stats = o;
     return STABLE_FLUIDS_RESULT_OK;
 }
@@ -694,6 +753,27 @@ StableFluidsResult stable_fluids_b200_enqueue_stage(void* context, uint32_t stag
     }
     if (st.e != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (out_kernel_launches) *out_kernel_launches = st.launches;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network) {
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    if (c.options.warm_start != STABLE_FLUIDS_B200_WARM_START_LEARNED) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto* n = static_cast<sfb::net::Net*>(network);
+    if (cudaStreamSynchronize(c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    // the network's buffers for this grid are allocated before the capture
+    if (n != nullptr && sfb::net::prepare(n, c.dims) != cudaSuccess) {
+        cudaGetLastError();
+        return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    sfb::net::Net* const previous = c.network;
+    c.network = n;
+    if (sfb::build_graph(c) != cudaSuccess) {
+        c.network = previous;
+        sfb::build_graph(c);  // put the previous step graph back
+        return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
     return STABLE_FLUIDS_RESULT_OK;
 }
 

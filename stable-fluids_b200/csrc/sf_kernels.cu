@@ -234,8 +234,7 @@ __global__ void __launch_bounds__(256) k_residual_sums(const float* __restrict__
 
 // rel_res = ||b - A p|| / ||b||, with b's mean removed when the pressure
 // operator is singular (no OUTFLOW face: constants are in its null space).
-__global__ void k_residual_finalize(DeviceStats* s, double n, int singular, int iterations) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ double relative_residual(const DeviceStats* s, double n, int singular, double* rhs_norm) {
     double r2 = s->sum_e2, b2 = s->sum_b2;
     if (singular) {
         const double mb = s->sum_b / n;
@@ -244,34 +243,57 @@ __global__ void k_residual_finalize(DeviceStats* s, double n, int singular, int 
     }
     r2 = r2 < 0.0 ? 0.0 : r2;
     b2 = b2 < 0.0 ? 0.0 : b2;
-    s->rhs_norm = sqrt(b2);
-    s->rel_residual = b2 > 0.0 ? sqrt(r2) / sqrt(b2) : 0.0;
+    if (rhs_norm) *rhs_norm = sqrt(b2);
+    return b2 > 0.0 ? sqrt(r2) / sqrt(b2) : 0.0;
+}
+
+__global__ void k_residual_finalize(DeviceStats* s, double n, int singular, int iterations) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double rhs = 0.0;
+    s->rel_residual = relative_residual(s, n, singular, &rhs);
+    s->rhs_norm = rhs;
     if (iterations >= 0) s->iterations = iterations;
 }
 
 // Residual-driven pressure solve: turns the accumulated sums into rel_res,
-// counts the iterations run (reset < 0 sets the count to zero), zeroes the
-// sums for the next measurement, and continues the enclosing WHILE graph
+// counts the iterations run (reset: the count becomes `increment`), zeroes
+// the sums for the next measurement, and continues the enclosing WHILE graph
 // node while rel_res > tol and fewer than max_iterations have run.
-__global__ void k_residual_check(DeviceStats* s, double n, int singular, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle) {
+__global__ void k_residual_check(DeviceStats* s, double n, int singular, int reset, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double r2 = s->sum_e2, b2 = s->sum_b2;
-    if (singular) {
-        const double mb = s->sum_b / n;
-        r2 = s->sum_e2 - 2.0 * mb * s->sum_e + n * mb * mb;
-        b2 = s->sum_b2 - n * mb * mb;
-    }
-    r2 = r2 < 0.0 ? 0.0 : r2;
-    b2 = b2 < 0.0 ? 0.0 : b2;
-    const double rel = b2 > 0.0 ? sqrt(r2) / sqrt(b2) : 0.0;
-    s->rhs_norm = sqrt(b2);
+    double rhs = 0.0;
+    const double rel = relative_residual(s, n, singular, &rhs);
+    s->rhs_norm = rhs;
     s->rel_residual = rel;
-    s->iterations = increment < 0 ? 0 : s->iterations + increment;
+    s->iterations = reset ? increment : s->iterations + increment;
     s->sum_e = s->sum_e2 = s->sum_b = s->sum_b2 = 0.0;
     const bool more = rel > tol && s->iterations < max_iterations;
     s->hit_cap = (rel > tol && !more) ? 1 : 0;
     s->keep_going = more ? 1 : 0;
     cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// Learned warm start, after the trial sweeps on both candidates: the learned
+// candidate (in p, sums in `learned`) is replaced by the plain one (in alt,
+// sums in `plain`) when its relative residual is larger.
+__global__ void k_warm_start_select(const DeviceStats* learned, const DeviceStats* plain, double n, int singular, float* __restrict__ p, const float* __restrict__ alt, size_t cells) {
+    if (!(relative_residual(learned, n, singular, nullptr) > relative_residual(plain, n, singular, nullptr))) return;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < cells; i += static_cast<size_t>(gridDim.x) * blockDim.x) p[i] = alt[i];
+}
+
+// Records the decision of k_warm_start_select and, on a fallback, adopts the
+// plain candidate's residual sums (so that a residual-driven loop continues
+// from the right value).
+__global__ void k_warm_start_commit(DeviceStats* learned, const DeviceStats* plain, double n, int singular) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const bool fallback = relative_residual(learned, n, singular, nullptr) > relative_residual(plain, n, singular, nullptr);
+    learned->used_fallback = fallback ? 1 : 0;
+    if (fallback) {
+        learned->sum_e = plain->sum_e;
+        learned->sum_e2 = plain->sum_e2;
+        learned->sum_b = plain->sum_b;
+        learned->sum_b2 = plain->sum_b2;
+    }
 }
 
 // ----------------------------------------------------------- diagnostics --
@@ -339,9 +361,17 @@ cudaError_t launch_residual_finalize(DeviceStats* stats, Dims d, int singular, i
     return cudaGetLastError();
 }
 
-cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s) {
+cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int reset, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s) {
     const double n = static_cast<double>(d.nx) * static_cast<double>(d.ny) * static_cast<double>(d.nz);
-    k_residual_check<<<1, 32, 0, s>>>(stats, n, singular, increment, tol, max_iterations, handle);
+    k_residual_check<<<1, 32, 0, s>>>(stats, n, singular, reset, increment, tol, max_iterations, handle);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* plain, Dims d, int singular, float* p, const float* alt, cudaStream_t s) {
+    const size_t cells = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny) * static_cast<size_t>(d.nz);
+    const double n = static_cast<double>(cells);
+    k_warm_start_select<<<linear_grid(cells, 256), 256, 0, s>>>(learned, plain, n, singular, p, alt, cells);
+    k_warm_start_commit<<<1, 32, 0, s>>>(learned, plain, n, singular);
     return cudaGetLastError();
 }
 

@@ -59,7 +59,10 @@ cudaError_t launch_project(float* vx, float* vy, float* vz, void* packed, const 
 cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
 cudaError_t launch_residual_finalize(DeviceStats* stats, Dims d, int singular, int iterations, cudaStream_t s);
 // One check of the residual-driven pressure solve (see k_residual_check).
-cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s);
+cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int reset, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s);
+// Learned warm start: keeps the candidate in p or replaces it by alt,
+// whichever has the smaller relative residual (two kernels).
+cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* plain, Dims d, int singular, float* p, const float* alt, cudaStream_t s);
 cudaError_t launch_post_diagnostics(float* div, float* mag, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s);
 
 }  // namespace sfb

@@ -122,9 +122,186 @@ __global__ void __launch_bounds__(256) k_jacobi(float* __restrict__ dst, const f
     }
 }
 
+// ------------------------------------------------- vectorised z-marching --
+// Both schemes again, for grids with nx % 4 == 0 and 16-byte aligned fields:
+// a thread owns 4 consecutive cells of a row (one float4) and marches through
+// kVecPlanes-deep z chunks, carrying the planes below / at / above in
+// registers, so every field value is loaded once per sweep from L2/HBM (plus
+// the x and y neighbours, which hit L1). Face ghosts come from the kind's
+// GhostRule (periodic wrap, copy of the face cell, constant, reflection) --
+// the same values as the load_* ghost rules for a face neighbour -- applied
+// with selects, so boundary threads take the same path as interior ones.
+// Arithmetic, neighbour order and division are those of k_rbgs_colour /
+// k_jacobi, so results are bit-identical.
+struct VecGhost {
+    int ox_lo, ox_hi;  // x offsets of the row's x- / x+ neighbours from x0 (wrap or self on a face)
+    int oy_lo, oy_hi;  // y offsets of the y- / y+ rows
+    bool gx_lo, gx_hi, gy_lo, gy_hi;  // apply the face ghost
+};
+
+__device__ __forceinline__ VecGhost vec_ghost(int x0, int y, const Dims& d, const GhostRule& g) {
+    const int sy = d.nx;
+    VecGhost v{-1, 4, -sy, sy, false, false, false, false};
+    if (x0 == 0) {
+        v.ox_lo = g.periodic[0] ? d.nx - 1 : 0;
+        v.gx_lo = !g.periodic[0];
+    }
+    if (x0 + 4 == d.nx) {
+        v.ox_hi = g.periodic[0] ? -x0 : 3;
+        v.gx_hi = !g.periodic[0];
+    }
+    if (y == 0) {
+        v.oy_lo = g.periodic[1] ? (d.ny - 1) * sy : 0;
+        v.gy_lo = !g.periodic[1];
+    }
+    if (y == d.ny - 1) {
+        v.oy_hi = g.periodic[1] ? -(d.ny - 1) * sy : 0;
+        v.gy_hi = !g.periodic[1];
+    }
+    return v;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+__device__ __forceinline__ float4 ghost4(const GhostRule& g, int face, float4 self) {
+    return make_float4(tb::ghost(g, face, self.x), tb::ghost(g, face, self.y), tb::ghost(g, face, self.z), tb::ghost(g, face, self.w));
+}
+
+template <int KIND>
+__device__ __forceinline__ float vec_update(float nb, float rhs, float coef, float divisor, float recip) {
+    const float num = tb::numerator<KIND>(nb, rhs, coef);
+    float q = tb::markstein_div(num, divisor, recip);
+    if (tb::needs_ieee_div(num)) q = num / divisor;
+    return q;
+}
+
+// The plane below the chunk's first plane (or its ghost at z = 0).
+__device__ __forceinline__ float4 vec_below(const float* x, int i, int z, const Dims& d, const GhostRule& g, float4 cur) {
+    const int sz = d.nx * d.ny;
+    if (z > 0) return ld4(x + i - sz);
+    if (g.periodic[2]) return ld4(x + i + (d.nz - 1) * sz);
+    return ghost4(g, ZM, cur);
+}
+
+__device__ __forceinline__ float4 vec_above(const float* x, int i, int z, const Dims& d, const GhostRule& g, float4 cur) {
+    const int sz = d.nx * d.ny;
+    if (z + 1 < d.nz) return ld4(x + i + sz);
+    if (g.periodic[2]) return ld4(x + i - (d.nz - 1) * sz);
+    return ghost4(g, ZP, cur);
+}
+
+constexpr int kVecRows = 4;  // rows per CTA; 32 x kVecRows threads
+
+// One Jacobi sweep dst = update(src).
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    if (x0 >= d.nx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    const VecGhost v = vec_ghost(x0, y, d, g);
+    const int sz = d.nx * d.ny;
+    int i = x0 + d.nx * (y + d.ny * zb);
+    float4 cur = ld4(src + i);
+    float4 below = vec_below(src, i, zb, d, g, cur);
+#pragma unroll 2
+    for (int z = zb; z < ze; ++z, i += sz) {
+        const float4 above = vec_above(src, i, z, d, g, cur);
+        float a = src[i + v.ox_lo], b = src[i + v.ox_hi];
+        float4 c = ld4(src + i + v.oy_lo), e = ld4(src + i + v.oy_hi);
+        const float4 r = ld4(rhs + i);
+        if (v.gx_lo) a = tb::ghost(g, XM, a);
+        if (v.gx_hi) b = tb::ghost(g, XP, b);
+        if (v.gy_lo) c = ghost4(g, YM, c);
+        if (v.gy_hi) e = ghost4(g, YP, e);
+        float4 o;
+        o.x = vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip);
+        o.y = vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip);
+        o.z = vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip);
+        o.w = vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip);
+        *reinterpret_cast<float4*>(dst + i) = o;
+        below = cur;
+        cur = above;
+    }
+}
+
+// One colour of an RBGS iteration, in place: in each float4 the two cells
+// with (x + y + z + parity) even are updated; the other two are stored back
+// unchanged (no thread of this launch changes them, so rewriting the value
+// just read is harmless and keeps every store a full 16 bytes).
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec(float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    if (x0 >= d.nx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    const VecGhost v = vec_ghost(x0, y, d, g);
+    const int sz = d.nx * d.ny;
+    int i = x0 + d.nx * (y + d.ny * zb);
+    float4 cur = ld4(x + i);
+    float4 below = vec_below(x, i, zb, d, g, cur);
+#pragma unroll 2
+    for (int z = zb; z < ze; ++z, i += sz) {
+        const float4 above = vec_above(x, i, z, d, g, cur);
+        float a = x[i + v.ox_lo], b = x[i + v.ox_hi];
+        float4 c = ld4(x + i + v.oy_lo), e = ld4(x + i + v.oy_hi);
+        const float4 r = ld4(rhs + i);
+        if (v.gx_lo) a = tb::ghost(g, XM, a);
+        if (v.gx_hi) b = tb::ghost(g, XP, b);
+        if (v.gy_lo) c = ghost4(g, YM, c);
+        if (v.gy_hi) e = ghost4(g, YP, e);
+        const bool even = ((y + z + parity) & 1) == 0;  // cells 0 and 2 of the float4 (else 1 and 3)
+        const float n_lo = even ? a + cur.y + c.x + e.x + below.x + above.x : cur.x + cur.z + c.y + e.y + below.y + above.y;
+        const float n_hi = even ? cur.y + cur.w + c.z + e.z + below.z + above.z : cur.z + b + c.w + e.w + below.w + above.w;
+        const float q_lo = vec_update<KIND>(n_lo, even ? r.x : r.y, coef, divisor, recip);
+        const float q_hi = vec_update<KIND>(n_hi, even ? r.z : r.w, coef, divisor, recip);
+        const float4 o = even ? make_float4(q_lo, cur.y, q_hi, cur.w) : make_float4(cur.x, q_lo, cur.z, q_hi);
+        *reinterpret_cast<float4*>(x + i) = o;
+        below = cur;
+        cur = above;
+    }
+}
+
+// Launch shape of the vectorised kernels: z chunks sized so that the grid
+// fills the resident CTA slots of all SMs about once.
+struct VecShape {
+    dim3 grid;
+    int z_chunk;
+};
+
+template <typename Kernel>
+VecShape vec_shape(const Dims& d, Kernel kernel) {
+    static int per_sm = [&] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 32 * kVecRows, 0) != cudaSuccess || n < 1) n = 4;
+        return n;
+    }();
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int bx = (d.nx / 4 + 31) / 32, by = (d.ny + kVecRows - 1) / kVecRows;
+    const long long slots = static_cast<long long>(sms) * per_sm;
+    long long chunks = (slots + static_cast<long long>(bx) * by - 1) / (static_cast<long long>(bx) * by);
+    if (chunks < 1) chunks = 1;
+    int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
+    if (z_chunk < 4) z_chunk = d.nz < 4 ? d.nz : 4;
+    const int bz = (d.nz + z_chunk - 1) / z_chunk;
+    return {dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), static_cast<unsigned>(bz)), z_chunk};
+}
+
+bool vec_ok(const StencilArgs& a) {
+    const auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    const size_t cells = static_cast<size_t>(a.dims.nx) * a.dims.ny * a.dims.nz;
+    return a.dims.nx % 4 == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
+}
+
 __global__ void k_scale_field(float* __restrict__ q, float factor, size_t n) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = q[i] * factor;
 }
+
+GhostRule ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb);
 
 template <int KIND>
 cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
@@ -137,13 +314,23 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(a.x, a.b, bytes, cudaMemcpyDeviceToDevice, s);
         else if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
         if (e != cudaSuccess) return e;
-        const dim3 cblock(32, 8, 1);
-        const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
-        for (int it = 0; it < a.iterations; ++it)
-            for (int parity = 0; parity < 2; ++parity) k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, parity, d, a.flow, a.scalar);
+        if (vec_ok(a)) {
+            const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
+            const VecShape vs = vec_shape(d, k_rbgs_vec<KIND>);
+            for (int it = 0; it < a.iterations; ++it)
+                for (int parity = 0; parity < 2; ++parity) k_rbgs_vec<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(a.x, a.b, a.coef, parity, vs.z_chunk, d, g);
+        } else {
+            const dim3 cblock(32, 8, 1);
+            const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
+            for (int it = 0; it < a.iterations; ++it)
+                for (int parity = 0; parity < 2; ++parity) k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, parity, d, a.flow, a.scalar);
+        }
         if (a.launches) *a.launches += 2 * a.iterations;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
+        const bool vec = vec_ok(a);
+        const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
+        const VecShape vs = vec ? vec_shape(d, k_jacobi_vec<KIND>) : VecShape{};
         const dim3 jblock(32, 8, 1);
         const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
         // Choose the first source so that the last sweep lands in x.
@@ -163,7 +350,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             const int left = a.iterations - it;  // sweeps still to run, this one included
             float* dst = (left & 1) ? a.x : a.scratch;
             if (dst == src) dst = (dst == a.x) ? a.scratch : a.x;
-            k_jacobi<KIND><<<grid, jblock, 0, s>>>(dst, src, a.b, a.coef, d, a.flow, a.scalar);
+            if (vec) k_jacobi_vec<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
+            else k_jacobi<KIND><<<grid, jblock, 0, s>>>(dst, src, a.b, a.coef, d, a.flow, a.scalar);
             src = dst;
         }
         if (a.launches) *a.launches += a.iterations;

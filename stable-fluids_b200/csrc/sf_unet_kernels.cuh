@@ -1,0 +1,348 @@
+// sf_unet_kernels.cuh -- kernels of the warm-start network: 3x3x3 convolution
+// as an implicit GEMM on the tensor cores (BF16 operands, FP32 accumulation),
+// its data and weight gradients, 2x average pooling, 2x nearest upsampling,
+// and the element-wise pieces of training.
+//
+// Activations are channels-last BF16: element (voxel v, channel c) at
+// v * C + c, v = x + nx (y + ny z), C a multiple of 16 (padded with zeros).
+// Weights are BF16 [tap][cout][cin] with tap = (dz+1)*9 + (dy+1)*3 + (dx+1),
+// plus an FP32 master copy for the optimizer. Zero padding at the grid edge.
+//
+// Tensor-core instruction: mma.sync m16n8k16 BF16 x BF16 -> FP32. A fragment
+// rows are 16 output voxels (one x row of the tile), its K columns 16 input
+// channels of one tap; B holds the weights of 8 output channels.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sf_types.h"
+
+namespace sfb::net {
+
+constexpr int kTileX = 16, kTileY = 4;  // output voxels per CTA (one m16 tile per warp, 4 warps)
+constexpr int kHaloX = kTileX + 2, kHaloY = kTileY + 2;
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+enum Epilogue : int { EPI_RELU_BF16 = 0, EPI_LINEAR_BF16 = 1, EPI_LINEAR_F32_CH0 = 2 };
+
+// out[v][co] = epi(bias[co] + sum_tap sum_ci w[tap][co][ci] in[v + off(tap)][ci])
+// CIN, COUT: channel counts (CIN % 16 == 0, COUT % 8 == 0). Grid:
+// (ceil(nx/16), ceil(ny/4), nz), 128 threads. out_ch: channel stride of the
+// output tensor (>= COUT; lets a layer write into a wider concatenated tensor
+// at channel offset out_off).
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(128) k_conv3d(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias, void* __restrict__ out, int out_ch, int out_off, Dims d) {
+    static_assert(CIN % 16 == 0 && COUT % 8 == 0, "channel padding");
+    constexpr int NT = COUT / 8;
+    extern __shared__ __align__(16) __nv_bfloat16 tile[];  // [3][kHaloY][kHaloX][CIN]
+    const int x0 = static_cast<int>(blockIdx.x) * kTileX, y0 = static_cast<int>(blockIdx.y) * kTileY, z = static_cast<int>(blockIdx.z);
+    const int tid = static_cast<int>(threadIdx.x), warp = tid >> 5, lane = tid & 31;
+    // input halo tile, 16-byte vectors, zeros outside the grid
+    constexpr int VEC = CIN / 8;
+    for (int i = tid; i < 3 * kHaloY * kHaloX * VEC; i += 128) {
+        const int c8 = i % VEC, hx = (i / VEC) % kHaloX, hy = (i / VEC / kHaloX) % kHaloY, hz = i / VEC / kHaloX / kHaloY;
+        const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z + hz - 1;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny) && static_cast<unsigned>(gz) < static_cast<unsigned>(d.nz))
+            v = *reinterpret_cast<const uint4*>(in + (static_cast<size_t>(gx) + static_cast<size_t>(d.nx) * (gy + static_cast<size_t>(d.ny) * gz)) * CIN + c8 * 8);
+        *reinterpret_cast<uint4*>(tile + ((hz * kHaloY + hy) * kHaloX + hx) * CIN + c8 * 8) = v;
+    }
+    __syncthreads();
+    const int g = lane >> 2, t = lane & 3;
+    float acc[NT][4];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
+    for (int tap = 0; tap < 27; ++tap) {
+        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+        const __nv_bfloat16* arow = tile + ((dz * kHaloY + warp + dy) * kHaloX + dx) * CIN;  // voxel x = 0 of this warp's row, shifted by the tap
+        const __nv_bfloat16* wt = w + static_cast<size_t>(tap) * COUT * CIN;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; ++kc) {
+            const int k0 = kc * 16 + 2 * t;
+            const uint32_t a0 = ld32(arow + g * CIN + k0), a1 = ld32(arow + (g + 8) * CIN + k0);
+            const uint32_t a2 = ld32(arow + g * CIN + k0 + 8), a3 = ld32(arow + (g + 8) * CIN + k0 + 8);
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                const __nv_bfloat16* wb = wt + (n * 8 + g) * CIN + k0;
+                mma_bf16(acc[n], a0, a1, a2, a3, __ldg(reinterpret_cast<const unsigned int*>(wb)), __ldg(reinterpret_cast<const unsigned int*>(wb + 8)));
+            }
+        }
+    }
+    // epilogue: rows g and g + 8 of the warp's 16 voxels, columns 2t, 2t + 1 of each n tile
+    const int gy = y0 + warp;
+    if (gy >= d.ny) return;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const int gx = x0 + g + 8 * half;
+        if (gx >= d.nx) continue;
+        const size_t v = static_cast<size_t>(gx) + static_cast<size_t>(d.nx) * (gy + static_cast<size_t>(d.ny) * z);
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            const int co = n * 8 + 2 * t;
+            float r0 = acc[n][2 * half] + (bias ? bias[co] : 0.0f);
+            float r1 = acc[n][2 * half + 1] + (bias ? bias[co + 1] : 0.0f);
+            if constexpr (EPI == EPI_RELU_BF16) {
+                r0 = fmaxf(r0, 0.0f);
+                r1 = fmaxf(r1, 0.0f);
+            }
+            if constexpr (EPI == EPI_LINEAR_F32_CH0) {
+                if (co == 0) static_cast<float*>(out)[v] = r0;
+            } else {
+                *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(out) + v * out_ch + out_off + co) = __floats2bfloat162_rn(r0, r1);
+            }
+        }
+    }
+}
+
+// Weight gradient: dw[tap][co][ci] += sum_v dout[v][co] in[v + off(tap)][ci],
+// dbias[co] += sum_v dout[v][co]. GEMM per tap with M = COUT, N = CIN,
+// K = voxels; the operand tiles are stored channel-major in shared memory so
+// that K pairs are contiguous. Grid: (27, chunks); each CTA covers a z range
+// of the grid for its tap and adds its FP32 partial sums atomically.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_conv3d_wgrad(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ dout, float* __restrict__ dw, float* __restrict__ dbias, Dims d, int z_per_cta) {
+    static_assert(CIN % 8 == 0 && COUT % 16 == 0, "channel padding");
+    constexpr int MT = COUT / 16, NTL = CIN / 8;  // m tiles, n tiles
+    constexpr int TILES = MT * NTL;
+    constexpr int PER_WARP = (TILES + 3) / 4;
+    constexpr int V = 64;  // voxels per chunk: one row of 64 x (K = 4 x 16)
+    __shared__ __align__(16) __nv_bfloat16 sa[COUT][V + 8];
+    __shared__ __align__(16) __nv_bfloat16 sb[CIN][V + 8];
+    const int tap = static_cast<int>(blockIdx.x);
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const int tid = static_cast<int>(threadIdx.x), warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    float acc[PER_WARP][4];
+#pragma unroll
+    for (int i = 0; i < PER_WARP; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
+    float bsum = 0.0f;
+    const int zb = static_cast<int>(blockIdx.y) * z_per_cta, ze = min(zb + z_per_cta, d.nz);
+    for (int z = zb; z < ze; ++z)
+        for (int y = 0; y < d.ny; ++y)
+            for (int xc = 0; xc < d.nx; xc += V) {
+                __syncthreads();
+                for (int i = tid; i < V * COUT; i += 128) {
+                    const int c = i % COUT, vx = i / COUT, gx = xc + vx;
+                    sa[c][vx] = gx < d.nx ? dout[(static_cast<size_t>(gx) + static_cast<size_t>(d.nx) * (y + static_cast<size_t>(d.ny) * z)) * COUT + c] : __float2bfloat16(0.0f);
+                }
+                const int sy = y + dy, sz = z + dz;
+                for (int i = tid; i < V * CIN; i += 128) {
+                    const int c = i % CIN, vx = i / CIN, sx = xc + vx + dx;
+                    const bool inb = xc + vx < d.nx && static_cast<unsigned>(sx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(sy) < static_cast<unsigned>(d.ny) && static_cast<unsigned>(sz) < static_cast<unsigned>(d.nz);
+                    sb[c][vx] = inb ? in[(static_cast<size_t>(sx) + static_cast<size_t>(d.nx) * (sy + static_cast<size_t>(d.ny) * sz)) * CIN + c] : __float2bfloat16(0.0f);
+                }
+                __syncthreads();
+                if (tap == 13 && tid < COUT)
+                    for (int vx = 0; vx < V; ++vx) bsum += __bfloat162float(sa[tid][vx]);
+#pragma unroll
+                for (int kc = 0; kc < V / 16; ++kc) {
+#pragma unroll
+                    for (int i = 0; i < PER_WARP; ++i) {
+                        const int tile_id = warp * PER_WARP + i;
+                        if (tile_id >= TILES) continue;
+                        const int mt = tile_id / NTL, nt = tile_id % NTL;
+                        const int k0 = kc * 16 + 2 * t;
+                        const uint32_t a0 = ld32(&sa[mt * 16 + g][k0]), a1 = ld32(&sa[mt * 16 + g + 8][k0]);
+                        const uint32_t a2 = ld32(&sa[mt * 16 + g][k0 + 8]), a3 = ld32(&sa[mt * 16 + g + 8][k0 + 8]);
+                        const uint32_t b0 = ld32(&sb[nt * 8 + g][k0]), b1 = ld32(&sb[nt * 8 + g][k0 + 8]);
+                        mma_bf16(acc[i], a0, a1, a2, a3, b0, b1);
+                    }
+                }
+            }
+#pragma unroll
+    for (int i = 0; i < PER_WARP; ++i) {
+        const int tile_id = warp * PER_WARP + i;
+        if (tile_id >= TILES) continue;
+        const int mt = tile_id / NTL, nt = tile_id % NTL;
+        float* base = dw + static_cast<size_t>(tap) * COUT * CIN;
+        const int co = mt * 16 + g, ci = nt * 8 + 2 * t;
+        atomicAdd(base + co * CIN + ci, acc[i][0]);
+        atomicAdd(base + co * CIN + ci + 1, acc[i][1]);
+        atomicAdd(base + (co + 8) * CIN + ci, acc[i][2]);
+        atomicAdd(base + (co + 8) * CIN + ci + 1, acc[i][3]);
+    }
+    if (tap == 13 && tid < COUT && dbias) atomicAdd(dbias + tid, bsum);
+}
+
+template <int CIN>
+constexpr size_t conv_smem_bytes() { return static_cast<size_t>(3) * kHaloY * kHaloX * CIN * sizeof(__nv_bfloat16); }
+
+// ------------------------------------------------------ element-wise pieces --
+
+// Network input: channel 0 = b * scale, channel 1 = p_prev * scale, the
+// other 14 channels zero (16-channel padded tensor). scale = 1 / rms(b) is
+// read from *scale.
+__global__ void k_pack_input(const float* __restrict__ b, const float* __restrict__ p_prev, const float* __restrict__ scale, float b_factor, __nv_bfloat16* __restrict__ out, size_t n) {
+    const float s = *scale;
+    for (size_t v = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; v < n; v += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        __nv_bfloat162 pair = __floats2bfloat162_rn(b[v] * b_factor * s, p_prev ? p_prev[v] * s : 0.0f);
+        uint4 z4 = make_uint4(0, 0, 0, 0);
+        uint4 first = z4;
+        first.x = *reinterpret_cast<uint32_t*>(&pair);
+        reinterpret_cast<uint4*>(out + v * 16)[0] = first;
+        reinterpret_cast<uint4*>(out + v * 16)[1] = z4;
+    }
+}
+
+// scale = 1 / rms(b_factor * b) from the FP64 sum of squares in *sumsq.
+__global__ void k_finish_scale(const double* __restrict__ sumsq, double n, float* __restrict__ scale) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const double rms = sqrt(*sumsq / n);
+        *scale = rms > 0.0 ? static_cast<float>(1.0 / rms) : 1.0f;
+    }
+}
+
+__global__ void k_sum_squares(const float* __restrict__ b, float b_factor, size_t n, double* __restrict__ out) {
+    double acc = 0.0;
+    for (size_t v = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; v < n; v += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const double x = static_cast<double>(b[v]) * b_factor;
+        acc += x * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// p0 = p_prev + delta / scale (the network predicts the scaled correction).
+// p_prev may alias p0 (element-wise, each thread reads before it writes).
+__global__ void k_unpack_output(const float* __restrict__ delta, const float* p_prev, const float* __restrict__ scale, float* p0, size_t n) {
+    const float inv = 1.0f / *scale;
+    for (size_t v = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; v < n; v += static_cast<size_t>(gridDim.x) * blockDim.x) p0[v] = (p_prev ? p_prev[v] : 0.0f) + delta[v] * inv;
+}
+
+// 2x2x2 average pooling (even dims of the fine grid); channel stride in_ch.
+__global__ void k_pool2(const __nv_bfloat16* __restrict__ in, int in_ch, int in_off, __nv_bfloat16* __restrict__ out, int C, Dims coarse) {
+    const size_t n = static_cast<size_t>(coarse.nx) * coarse.ny * coarse.nz * C;
+    const int fnx = coarse.nx * 2, fny = coarse.ny * 2;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        const size_t v = i / C;
+        const int x = static_cast<int>(v % coarse.nx), y = static_cast<int>((v / coarse.nx) % coarse.ny), z = static_cast<int>(v / coarse.nx / coarse.ny);
+        float s = 0.0f;
+        for (int k = 0; k < 8; ++k) {
+            const size_t fv = static_cast<size_t>(2 * x + (k & 1)) + static_cast<size_t>(fnx) * (2 * y + ((k >> 1) & 1) + static_cast<size_t>(fny) * (2 * z + (k >> 2)));
+            s += __bfloat162float(in[fv * in_ch + in_off + c]);
+        }
+        out[i] = __float2bfloat16(0.125f * s);
+    }
+}
+
+// Backward of the pooling: each fine voxel gets 1/8 of its parent's gradient,
+// added to (accumulate) or written into the fine gradient tensor.
+__global__ void k_pool2_backward(const __nv_bfloat16* __restrict__ gcoarse, int C, Dims coarse, __nv_bfloat16* __restrict__ gfine, int fine_ch, int fine_off, int accumulate) {
+    const int fnx = coarse.nx * 2, fny = coarse.ny * 2, fnz = coarse.nz * 2;
+    const size_t n = static_cast<size_t>(fnx) * fny * fnz * C;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        const size_t fv = i / C;
+        const int x = static_cast<int>(fv % fnx), y = static_cast<int>((fv / fnx) % fny), z = static_cast<int>(fv / fnx / fny);
+        const size_t cv = static_cast<size_t>(x / 2) + static_cast<size_t>(coarse.nx) * (y / 2 + static_cast<size_t>(coarse.ny) * (z / 2));
+        float gval = 0.125f * __bfloat162float(gcoarse[cv * C + c]);
+        __nv_bfloat16* dst = gfine + fv * fine_ch + fine_off + c;
+        if (accumulate) gval += __bfloat162float(*dst);
+        *dst = __float2bfloat16(gval);
+    }
+}
+
+// Nearest 2x upsampling of a coarse tensor into channels [out_off, out_off+C)
+// of a fine tensor with channel stride out_ch.
+__global__ void k_upsample2(const __nv_bfloat16* __restrict__ in, int C, Dims coarse, __nv_bfloat16* __restrict__ out, int out_ch, int out_off) {
+    const int fnx = coarse.nx * 2, fny = coarse.ny * 2, fnz = coarse.nz * 2;
+    const size_t n = static_cast<size_t>(fnx) * fny * fnz * C;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        const size_t fv = i / C;
+        const int x = static_cast<int>(fv % fnx), y = static_cast<int>((fv / fnx) % fny), z = static_cast<int>(fv / fnx / fny);
+        const size_t cv = static_cast<size_t>(x / 2) + static_cast<size_t>(coarse.nx) * (y / 2 + static_cast<size_t>(coarse.ny) * (z / 2));
+        out[fv * out_ch + out_off + c] = in[cv * C + c];
+    }
+}
+
+// Backward of the upsampling: the coarse gradient is the sum over its 8
+// children of channels [off, off + C) of the fine gradient.
+__global__ void k_upsample2_backward(const __nv_bfloat16* __restrict__ gfine, int fine_ch, int off, int C, Dims coarse, __nv_bfloat16* __restrict__ gcoarse) {
+    const size_t n = static_cast<size_t>(coarse.nx) * coarse.ny * coarse.nz * C;
+    const int fnx = coarse.nx * 2, fny = coarse.ny * 2;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        const size_t v = i / C;
+        const int x = static_cast<int>(v % coarse.nx), y = static_cast<int>((v / coarse.nx) % coarse.ny), z = static_cast<int>(v / coarse.nx / coarse.ny);
+        float s = 0.0f;
+        for (int k = 0; k < 8; ++k) {
+            const size_t fv = static_cast<size_t>(2 * x + (k & 1)) + static_cast<size_t>(fnx) * (2 * y + ((k >> 1) & 1) + static_cast<size_t>(fny) * (2 * z + (k >> 2)));
+            s += __bfloat162float(gfine[fv * fine_ch + off + c]);
+        }
+        gcoarse[i] = __float2bfloat16(s);
+    }
+}
+
+// Copies channels [src_off, src_off + C) of src into [dst_off, ...) of dst.
+__global__ void k_copy_channels(const __nv_bfloat16* __restrict__ src, int src_ch, int src_off, __nv_bfloat16* __restrict__ dst, int dst_ch, int dst_off, int C, size_t voxels, int accumulate) {
+    const size_t n = voxels * C;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        const size_t v = i / C;
+        float val = __bfloat162float(src[v * src_ch + src_off + c]);
+        __nv_bfloat16* d = dst + v * dst_ch + dst_off + c;
+        if (accumulate) val += __bfloat162float(*d);
+        *d = __float2bfloat16(val);
+    }
+}
+
+// g *= (act > 0): the gradient through a ReLU whose output is act.
+__global__ void k_relu_backward(__nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ act, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        if (!(__bfloat162float(act[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
+}
+
+// Mean squared error of the FP32 output against the target; writes the
+// gradient (channel 0 of a 16-channel BF16 tensor) and adds the loss sum.
+__global__ void k_mse(const float* __restrict__ out, const float* __restrict__ target, size_t n, __nv_bfloat16* __restrict__ grad16, double* __restrict__ loss_sum) {
+    double acc = 0.0;
+    const float k = 2.0f / static_cast<float>(n);
+    for (size_t v = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; v < n; v += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float e = out[v] - target[v];
+        acc += static_cast<double>(e) * e;
+        uint4 z4 = make_uint4(0, 0, 0, 0);
+        __nv_bfloat162 first = __floats2bfloat162_rn(k * e, 0.0f);
+        uint4 f = z4;
+        f.x = *reinterpret_cast<uint32_t*>(&first);
+        reinterpret_cast<uint4*>(grad16 + v * 16)[0] = f;
+        reinterpret_cast<uint4*>(grad16 + v * 16)[1] = z4;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, acc);
+}
+
+// Adam on FP32 master weights; refreshes the BF16 copy and the transposed,
+// tap-flipped BF16 copy used by the data-gradient convolution.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v, __nv_bfloat16* __restrict__ w16, __nv_bfloat16* __restrict__ w16t, int cout, int cin, size_t n, float lr, float b1, float b2, float eps, float bc1, float bc2) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+        w[i] = wi;
+        if (w16) {
+            w16[i] = __float2bfloat16(wi);
+            const int tap = static_cast<int>(i / (static_cast<size_t>(cout) * cin));
+            const int co = static_cast<int>((i / cin) % cout), ci = static_cast<int>(i % cin);
+            w16t[(static_cast<size_t>(26 - tap) * cin + ci) * cout + co] = __float2bfloat16(wi);
+        }
+    }
+}
+
+}  // namespace sfb::net

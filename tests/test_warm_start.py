@@ -1,0 +1,204 @@
+"""The learned pressure warm start on the GPU, through the C ABI:
+  - the network's forward pass and parameter gradients against the NumPy
+    oracle (oracle/unet.py, itself pinned by finite differences) in its
+    BF16-emulating mode, and against the plain FP64 network;
+  - training on pairs generated by the library reduces the loss and yields
+    starts with a smaller Poisson residual than the previous pressure on
+    held-out steps;
+  - inside the step graph: the selection rule (never worse than the
+    previous-pressure start after the trial sweeps), the no-network fallback
+    and the kernel count.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import unet
+
+pytestmark = pytest.mark.gpu
+
+# Tolerances against the BF16-emulating oracle: the library and the oracle
+# round the same tensors to BF16, but accumulate in FP32 vs FP64 and so round
+# a few values to the neighbouring BF16 number.
+PRED_TOL = 1e-2       # relative L2 error of the predicted correction
+LOSS_TOL = 1e-3       # relative error of the loss
+GRAD_TOL = 3e-2       # relative L2 error of each layer's gradient
+# Against the FP64 network (what BF16 storage costs the gradient).
+GRAD_TOL_FP64 = 1e-1
+
+
+def random_parameters(seed):
+    rng = np.random.default_rng(seed)
+    params = np.zeros(sum(27 * ci * co + co for _, ci, co in unet.LAYERS), np.float32)
+    for name, (w, bias) in unet.split(params).items():
+        w[...] = rng.standard_normal(w.shape) * np.sqrt(2.0 / (27 * w.shape[2]))
+        bias[...] = 0.05 * rng.standard_normal(bias.shape)
+    return params
+
+
+def random_fields(shape, seed):
+    rng = np.random.default_rng(seed)
+    b = rng.standard_normal(shape).astype(np.float32)
+    p_prev = (0.1 * rng.standard_normal(shape)).astype(np.float32)
+    p_target = (p_prev + 0.05 * rng.standard_normal(shape)).astype(np.float32)
+    return b, p_prev, p_target
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def net(sf, lib, cuda):
+    n = sf.WarmStartNetwork(seed=0, lib=lib)
+    yield n
+    n.close()
+
+
+@pytest.mark.parametrize("shape", [(8, 12, 20), (16, 16, 16), (4, 8, 36)])
+def test_predict_matches_oracle(net, shape):
+    params = random_parameters(1)
+    net.set_parameters(params)
+    b, p_prev, _ = random_fields(shape, 2)
+    h = 0.5
+    got = net.predict(b, p_prev, h).cpu().numpy()
+    ref = unet.UNet(params, bf16=True).predict(b, p_prev, np.float32(h * h))
+    assert rel(got - p_prev, ref - p_prev) <= PRED_TOL
+    # a null previous pressure means zero
+    got0 = net.predict(b, None, h).cpu().numpy()
+    ref0 = unet.UNet(params, bf16=True).predict(b, None, np.float32(h * h))
+    assert rel(got0, ref0) <= PRED_TOL
+
+
+@pytest.mark.parametrize("shape", [(8, 12, 20), (16, 16, 16)])
+def test_gradients_match_oracle(net, shape):
+    params = random_parameters(3)
+    net.set_parameters(params)
+    b, p_prev, p_target = random_fields(shape, 4)
+    loss, grad = net.gradients(b, p_prev, p_target, 1.0)
+    l16, g16 = unet.UNet(params, bf16=True).loss_and_gradients(b, p_prev, p_target, 1.0)
+    l64, g64 = unet.UNet(params).loss_and_gradients(b, p_prev, p_target, 1.0)
+    assert abs(loss - l16) <= LOSS_TOL * l16
+    got, ref = unet.split(grad), unet.split(g16)
+    for name, _, _ in unet.LAYERS:
+        for k in range(2):
+            if np.linalg.norm(ref[name][k]) > 0:
+                assert rel(got[name][k], ref[name][k]) <= GRAD_TOL, (name, k)
+    assert rel(grad, g64) <= GRAD_TOL_FP64
+    # padding entries get no gradient
+    assert np.all(got["enc0a"][0][:, :, 2:] == 0)
+    assert np.all(got["out"][0][:, 1:, :] == 0) and np.all(got["out"][1][1:] == 0)
+
+
+def test_set_parameters_round_trip(net):
+    params = random_parameters(5)
+    net.set_parameters(params)
+    assert np.array_equal(net.parameters(), params)
+    with pytest.raises(ValueError):
+        net.set_parameters(params[:-1])
+
+
+def test_rejects_grids_not_divisible_by_four(net):
+    b = np.zeros((8, 8, 10), np.float32)
+    with pytest.raises(RuntimeError):
+        net.predict(b, None, 1.0)
+
+
+# ------------------------------------------------------------ in the step --
+
+def scene_32(sf, steps=40):
+    n = 32
+    return sf.scenes.plume("plume-32^3", (n, n, n), dt=0.1, viscosity=1e-4, diffusion=1e-5, diffuse_iterations=4, pressure_iterations=60,
+                           sources=[(12.0, 6.0, 14.0, 4.0, 10.0, 6.0), (21.0, 6.0, 18.0, 3.0, 10.0, 3.0)], steps=steps)
+
+
+def jacobi_options(sf, lib, warm_start, trial=0, residual=True):
+    o = sf.default_options(lib)
+    o.scheme = sf.SCHEME_JACOBI
+    o.warm_start = warm_start
+    o.warm_start_trial_iterations = trial
+    o.compute_residual = 1 if residual else 0
+    return o
+
+
+def residual(lib, sf, p, div, scene, torch):
+    out = torch.zeros(2, dtype=torch.float64, device=p.device)
+    cfg = scene.config
+    rc = lib.stable_fluids_b200_pressure_residual_noalloc(p.data_ptr(), div.data_ptr(), cfg.nx, cfg.ny, cfg.nz, cfg.cell_size, ctypes.byref(cfg.flow_boundary), out.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return float(out[0])
+
+
+def test_learned_context_without_network_is_previous(sf, lib, cuda):
+    scene = scene_32(sf, steps=6)
+    res = {}
+    for ws in (sf.WARM_START_PREVIOUS, sf.WARM_START_LEARNED):
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=jacobi_options(sf, lib, ws))
+        sf.scenes.run(sim, scene)
+        res[ws] = (sim.fetch(sf.VIEW_FLOW_PRESSURE), sim.stats())
+        sim.close()
+    assert np.array_equal(res[sf.WARM_START_PREVIOUS][0], res[sf.WARM_START_LEARNED][0])
+    assert res[sf.WARM_START_LEARNED][1].used_fallback == 1
+    assert res[sf.WARM_START_PREVIOUS][1].used_fallback == 0
+
+
+def test_selection_never_worse_than_previous(sf, lib, cuda, net):
+    """With the trial as long as the solve, the kept start is the better of
+    the learned and the previous-pressure candidates, so the first step's
+    residual is at most the previous-pressure run's."""
+    net.set_parameters(random_parameters(7))
+    scene = scene_32(sf, steps=3)
+    out = {}
+    for ws in (sf.WARM_START_PREVIOUS, sf.WARM_START_LEARNED):
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=jacobi_options(sf, lib, ws, trial=scene.config.pressure_iterations))
+        if ws == sf.WARM_START_LEARNED:
+            before = sim.info().kernels_per_step
+            net.attach(sim)
+            assert sim.info().kernels_per_step >= before + 21 + 2
+        stats = []
+        for k in range(scene.steps):
+            sf.scenes.apply_inputs(sim, scene, k)
+            sim.step(1)
+            stats.append(sim.stats())
+        out[ws] = stats
+        sim.close()
+    learned, previous = out[sf.WARM_START_LEARNED], out[sf.WARM_START_PREVIOUS]
+    assert learned[0].used_fallback in (0, 1)
+    assert learned[0].rel_residual <= previous[0].rel_residual
+    assert learned[0].pressure_iterations == previous[0].pressure_iterations
+
+
+def test_training_gives_better_starts(sf, lib, cuda):
+    """Train on pairs from one plume run and check on held-out steps of the
+    same run that the predicted start has a smaller residual than the
+    previous pressure (the start the network replaces)."""
+    torch = cuda
+    scene = scene_32(sf, steps=40)
+    cfg = scene.config
+
+    def make():
+        o = jacobi_options(sf, lib, sf.WARM_START_PREVIOUS, residual=False)
+        s = sf.Simulation(cfg, scene.scalars, scene.vectors, lib=lib, options=o)
+        for k in range(2):
+            sf.scenes.apply_inputs(s, scene, k)
+        return s
+
+    pairs = list(sf.warmstart.training_pairs(make, steps=24, skip=2))
+    train, held = pairs[0::2], pairs[1::2]  # held-out steps interleave with the training ones
+    with sf.WarmStartNetwork(seed=11, lib=lib) as n:
+        first = [n.gradients(b, p, t, cfg.cell_size)[0] for b, p, t in train[:4]]
+        for epoch in range(20):
+            for b, p, t in train:
+                n.train_step(b, p, t, cfg.cell_size, 2e-3)
+        last = [n.gradients(b, p, t, cfg.cell_size)[0] for b, p, t in train[:4]]
+        assert np.mean(last) < 0.7 * np.mean(first)
+        ratios = []
+        for b, p, t in held:
+            p0 = n.predict(b, p, cfg.cell_size)
+            ratios.append(residual(lib, sf, p0, b, scene, torch) / residual(lib, sf, p, b, scene, torch))
+        print("held-out residual ratios (learned / previous):", np.round(ratios, 3))
+        assert sum(r < 1.0 for r in ratios) >= len(held) - 1, ratios
+        assert np.exp(np.mean(np.log(ratios))) < 0.9, ratios
