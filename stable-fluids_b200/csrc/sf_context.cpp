@@ -397,9 +397,14 @@ struct Stages {
     void project() {
         // the residual-driven solve has measured the residual already
         const bool measure = c.residual_enabled && !residual_measured;
-        if (measure) ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
-        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, measure ? c.stats : nullptr, c.stream));
-        if (measure) ok(launch_residual_finalize(c.stats, c.dims, c.flow.any_outflow ? 0 : 1, c.config.pressure_iterations, c.stream));
+        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, nullptr, c.stream));
+        if (measure) {
+            // projection reads p and div without changing them: the residual
+            // of the solve is measured after it, by one separate pass
+            ok(cudaMemsetAsync(c.stats, 0, offsetof(DeviceStats, rel_residual), c.stream), 0);
+            ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
+            ok(launch_residual_finalize(c.stats, c.dims, c.flow.any_outflow ? 0 : 1, c.config.pressure_iterations, c.stream));
+        }
     }
 
     // 7. scalars: source, advection by the projected velocity, diffusion,

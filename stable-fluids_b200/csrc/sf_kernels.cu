@@ -351,6 +351,7 @@ cudaError_t launch_project(float* vx, float* vy, float* vz, void* packed, const 
 }
 
 cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
+    if (launch_residual_sums_vec(p, div, d, h2, b, stats, s)) return cudaGetLastError();
     k_residual_sums<<<cell_grid(d), cell_block(), 0, s>>>(p, div, d, h2, b, stats);
     return cudaGetLastError();
 }

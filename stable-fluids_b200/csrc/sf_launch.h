@@ -57,6 +57,10 @@ cudaError_t launch_divergence(float* div, const float* vx, const float* vy, cons
 // the FP64 residual sums of the pressure system into stats.
 cudaError_t launch_project(float* vx, float* vy, float* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
 cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
+// The same sums with the vectorised z-marching layout; false (nothing
+// launched) when the grid or the pointers do not suit it (nx % 4, 16-byte
+// alignment).
+bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
 cudaError_t launch_residual_finalize(DeviceStats* stats, Dims d, int singular, int iterations, cudaStream_t s);
 // One check of the residual-driven pressure solve (see k_residual_check).
 cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int reset, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s);

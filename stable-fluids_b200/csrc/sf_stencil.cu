@@ -297,6 +297,73 @@ bool vec_ok(const StencilArgs& a) {
     return a.dims.nx % 4 == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
 }
 
+// FP64 sums of the pressure residual e = h^2 div - (sum6(p) - 6 p) and of
+// b = h^2 div (the four sums of k_residual_sums, same per-cell arithmetic),
+// with the z-marching float4 layout above; one atomic per sum per CTA.
+__device__ __forceinline__ double vec_warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __restrict__ p, const float* __restrict__ div, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
+    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
+    if (x0 < d.nx && y < d.ny) {
+        const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+        const VecGhost v = vec_ghost(x0, y, d, g);
+        const int sz = d.nx * d.ny;
+        int i = x0 + d.nx * (y + d.ny * zb);
+        float4 cur = ld4(p + i);
+        float4 below = vec_below(p, i, zb, d, g, cur);
+        for (int z = zb; z < ze; ++z, i += sz) {
+            const float4 above = vec_above(p, i, z, d, g, cur);
+            float a = p[i + v.ox_lo], b = p[i + v.ox_hi];
+            float4 c = ld4(p + i + v.oy_lo), e = ld4(p + i + v.oy_hi);
+            const float4 r = ld4(div + i);
+            if (v.gx_lo) a = tb::ghost(g, XM, a);
+            if (v.gx_hi) b = tb::ghost(g, XP, b);
+            if (v.gy_lo) c = ghost4(g, YM, c);
+            if (v.gy_hi) e = ghost4(g, YP, e);
+            const float xm[4] = {a, cur.x, cur.y, cur.z}, xp[4] = {cur.y, cur.z, cur.w, b};
+            const float ym[4] = {c.x, c.y, c.z, c.w}, yp[4] = {e.x, e.y, e.z, e.w};
+            const float zm[4] = {below.x, below.y, below.z, below.w}, zp[4] = {above.x, above.y, above.z, above.w};
+            const float pc[4] = {cur.x, cur.y, cur.z, cur.w}, rc[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double nb = static_cast<double>(xm[k]) + static_cast<double>(xp[k]) + static_cast<double>(ym[k]) + static_cast<double>(yp[k]) + static_cast<double>(zm[k]) + static_cast<double>(zp[k]);
+                const double bb = static_cast<double>(h2) * static_cast<double>(rc[k]);
+                const double ee = bb - (nb - 6.0 * static_cast<double>(pc[k]));
+                se += ee;
+                se2 += ee * ee;
+                sb += bb;
+                sb2 += bb * bb;
+            }
+            below = cur;
+            cur = above;
+        }
+    }
+    __shared__ double part[4][kVecRows];
+    se = vec_warp_sum(se);
+    se2 = vec_warp_sum(se2);
+    sb = vec_warp_sum(sb);
+    sb2 = vec_warp_sum(sb2);
+    if (threadIdx.x == 0) {
+        part[0][threadIdx.y] = se;
+        part[1][threadIdx.y] = se2;
+        part[2][threadIdx.y] = sb;
+        part[3][threadIdx.y] = sb2;
+    }
+    __syncthreads();
+    if (threadIdx.y == 0 && threadIdx.x < 4) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < kVecRows; ++w) t += part[threadIdx.x][w];
+        double* dst = threadIdx.x == 0 ? &stats->sum_e : threadIdx.x == 1 ? &stats->sum_e2 : threadIdx.x == 2 ? &stats->sum_b : &stats->sum_b2;
+        atomicAdd(dst, t);
+    }
+}
+
 __global__ void k_scale_field(float* __restrict__ q, float factor, size_t n) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = q[i] * factor;
 }
@@ -520,6 +587,15 @@ bool tb_supported(const StencilArgs& a) {
 }
 
 }  // namespace
+
+bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
+    const auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    const size_t cells = static_cast<size_t>(d.nx) * d.ny * d.nz;
+    if (d.nx % 4 != 0 || cells >= (1ull << 31) || !al(p) || !al(div)) return false;
+    const VecShape vs = vec_shape(d, k_residual_vec);
+    k_residual_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(p, div, h2, vs.z_chunk, d, ghost_rule(KIND_PRESSURE, b, ScalarBC{}), stats);
+    return true;
+}
 
 cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
     if (a.blocked && tb_supported(a)) {
