@@ -1,27 +1,46 @@
-"""Benchmark: steps/s of the stable-fluids step at 256^3 on B200.
+"""Benchmark: steps/s of the stable-fluids step at 256^3 on B200, with the
+pressure iterated until the FP64 relative Poisson residual is <= 1e-3:
+learned warm start vs plain Jacobi at equal residual.
 
 Workload (one "step" = one stable_fluids_step_cuda call = one step-graph
 launch): the seeded 256^3 buoyant plume -- dt 0.1, viscosity 1e-4, density
-diffusion 1e-5, 20 diffusion and 80 pressure iterations, Stam walls, two
-Gaussian sources (radius 8) with upward forces U[1, 10] (seed 1) -- run with
-the reference-compatible red-black Gauss-Seidel scheme, whose results match
-the reference backend's. The working set (~1.2 GB) is far larger than L2, so
-no flush is needed between steps.
+diffusion 1e-5, 20 diffusion iterations, Stam walls, two Gaussian sources
+(radius 8) with upward forces U[1, 10] (seed 1). The pressure solve runs
+inside the step graph until rel_res = ||b - A p|| / ||b|| <= 1e-3 (checked
+every 16 sweeps). The working set (> 1 GB) is far larger than L2, so no
+flush is needed between steps.
 
-  value : whole-job steps/s with inputs resident on the device, CUDA events on
-          the simulation stream, max over ranks.
-  e2e   : the same steps through the public C ABI with host buffers: every
-          step uploads the force field from pinned host memory
+Solver variants, all timed the same way (W untimed steps, then K steps):
+  learned  : Jacobi sweeps from the learned warm start (the network is
+             trained inside this run, before any timing, on pairs the solver
+             generates at 128^3; its trial-and-select against the previous
+             pressure runs every step) -- the headline `value`;
+  plain    : Jacobi sweeps from zero (the reference's start: it resets the
+             pressure every step) -- the comparison the metric names;
+  previous : Jacobi sweeps from the previous step's pressure;
+  rbgs     : red-black Gauss-Seidel from zero, the reference's own arithmetic.
+
+  value : whole-job steps/s of the learned variant, inputs resident on the
+          device, CUDA events on the simulation stream, max over ranks.
+  e2e   : the learned variant through the public C ABI with host buffers:
+          every step uploads the force field from pinned host memory
           (stable_fluids_update_vector_field_cuda with host pointers) and
-          reads the density field back to pinned host memory.
-  roofline : the dominant kernel family (the pressure solve), timed with
-          CUDA events on the context stream through the stage hook.
-  cpu_baseline : the reference step sequence transcribed to C++/OpenMP
-          (oracle/, FP32), on a bounded sample of the same workload.
+          reads the density back to pinned host memory.
+  roofline : the dominant kernel, the Jacobi pressure sweep (12 B/cell),
+          timed with CUDA events on the context stream; the network's
+          convolutions are reported beside it against the bf16 peak.
+  fixed_iterations : the reference's own configuration (80 red-black
+          pressure iterations per step) for a like-for-like kernel comparison.
+  cpu_baseline : the FP32 C++/OpenMP transcription of the step (oracle/) on a
+          bounded sample, scaled to the metric's unit.
 
 --impl reference runs the reference's own implementation of the path -- its
-CUDA backend compiled unmodified from backend-cuda.cu (oracle/_ref) -- on the
-same scene through the same C ABI. The reference has no CPU implementation.
+CUDA backend compiled unmodified from backend-cuda.cu (oracle/_ref; the
+reference has no CPU implementation) -- on the same scene through the same
+C ABI. The reference cannot iterate to a residual, so it runs with the fixed
+pressure-iteration count that the reference arithmetic (red-black from zero,
+bit-identical in this library) needs to reach 1e-3 in every timed step,
+found by a calibration run before timing.
 
 Multi-GPU (torchrun, N>1): the step does not shard; each rank runs its own
 replica of the workload ("scaling": "weak").
@@ -44,25 +63,31 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "steps/s at 256³: learned-warm-start vs plain Jacobi at equal ‖∇·u‖ residual"
+CHECK_INTERVAL = 16
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
-    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("b200", "reference"), default="b200")
     p.add_argument("--size", type=int, default=256)
-    p.add_argument("--scheme", choices=("rbgs", "jacobi"), default="rbgs")
-    p.add_argument("--iterations-per-pass", type=int, default=0)
-    p.add_argument("--e2e-steps", type=int, default=30)
-    p.add_argument("--cpu-steps", type=int, default=1)
+    p.add_argument("--tolerance", type=float, default=1e-3)
+    p.add_argument("--cap", type=int, default=100000, help="pressure-iteration cap of the residual-driven solve")
+    p.add_argument("--variants", default="learned,plain,previous,rbgs")
+    p.add_argument("--trial", type=int, default=CHECK_INTERVAL, help="learned start: sweeps of the trial against the previous pressure")
+    p.add_argument("--train-size", type=int, default=128)
+    p.add_argument("--train-scenes", type=int, default=6)
+    p.add_argument("--train-steps", type=int, default=32, help="pairs per training scene")
+    p.add_argument("--train-sweeps", type=int, default=1000, help="Jacobi sweeps of the target solve")
+    p.add_argument("--train-epochs", type=int, default=4)
+    p.add_argument("--train-seconds", type=float, default=90.0)
+    p.add_argument("--learning-rate", type=float, default=1e-3)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--fixed-steps", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
-    p.add_argument("--equal-residual", default="rbgs-zero,rbgs-previous,jacobi-previous", help="solver variants timed at equal rel_res (empty: skip)")
-    p.add_argument("--residual-tolerance", type=float, default=1e-3)
-    p.add_argument("--residual-steps", type=int, default=3)
-    p.add_argument("--residual-cap", type=int, default=20000)
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -117,7 +142,7 @@ class Clocks:
         return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(args):
+def dist_setup():
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -129,7 +154,7 @@ def dist_setup(args):
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     else:
         torch.cuda.set_device(0)
     return world, rank, local
@@ -142,48 +167,145 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a host float over the ranks (identity for one rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device if device is not None else "cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
-def time_steps(sim, steps, world):
+def solver_options(sf, variant, tol, cap, trial):
+    o = sf.default_options()
+    o.scheme = sf.SCHEME_RBGS if variant == "rbgs" else sf.SCHEME_JACOBI
+    o.warm_start = {"learned": sf.WARM_START_LEARNED, "plain": sf.WARM_START_ZERO, "previous": sf.WARM_START_PREVIOUS, "rbgs": sf.WARM_START_ZERO}[variant]
+    o.residual_tolerance = tol
+    o.residual_check_interval = CHECK_INTERVAL
+    o.max_pressure_iterations = cap
+    o.warm_start_trial_iterations = trial
+    return o
+
+
+def launches_per_step(info_kernels, iterations, trial_done, scheme_rbgs):
+    """Kernels one residual-driven step launches: the captured step counts
+    the loop body once; each further pass of the body launches the interval's
+    sweeps (2 per red-black iteration) + the residual sum + the check."""
+    body = CHECK_INTERVAL * (2 if scheme_rbgs else 1) + 2
+    passes = max((iterations - trial_done) // CHECK_INTERVAL, 1)
+    return info_kernels + (passes - 1) * body
+
+
+def run_variant(sf, scene, variant, args, world, device, net=None):
+    """W untimed steps then K timed steps (CUDA events per step on the
+    simulation stream, summed); per-step iterations and residuals."""
     import torch
 
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    barrier(world)
+    opts = solver_options(sf, variant, args.tolerance, args.cap, args.trial)
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=device)
+    if variant == "learned":
+        net.attach(sim)
+    sf.scenes.apply_inputs(sim, scene, 0)
+    sim.step(args.warmup)
     torch.cuda.synchronize()
-    start.record(sim.stream)
-    sim.step(steps)
-    end.record(sim.stream)
+    info = sim.info()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    its, res, fallback = [], [], []
+    barrier(world)
+    for k in range(args.steps):
+        events[k][0].record(sim.stream)
+        sim.step(1)
+        events[k][1].record(sim.stream)
+        st = sim.stats()  # waits for the step
+        its.append(st.pressure_iterations)
+        res.append(st.rel_residual)
+        fallback.append(st.used_fallback)
     torch.cuda.synchronize()
     barrier(world)
-    return start.elapsed_time(end) / 1000.0
+    t = sum(a.elapsed_time(b) for a, b in events) / 1000.0
+    t = max_over_ranks(t, world)
+    trial_done = args.trial if variant == "learned" else 0
+    launches = sum(launches_per_step(info.kernels_per_step, i, trial_done, variant == "rbgs") for i in its)
+    out = {"steps_per_s": world * args.steps / t, "ms_per_step": 1000.0 * t / args.steps, "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > args.tolerance for r in res), "gpu_launches": launches}
+    if variant == "learned":
+        out["used_fallback"] = fallback
+        out["trial_sweeps"] = args.trial
+    return sim, out
 
 
-def time_stage(sim, stage, repeats):
-    """Average duration of one kernel of a stage, CUDA events on the context
-    stream (the stage is enqueued directly on it)."""
+def train_network(sf, args, device):
+    """Pairs from seeded 128^3 training plumes (targets: the scene's own
+    Jacobi solve of --train-sweeps sweeps from the previous pressure), then
+    Adam; everything on the GPU through the library."""
+    t0 = time.perf_counter()
+    pairs = []
+    for k in range(args.train_scenes):
+        scene = sf.scenes.training_scene(k, n=args.train_size, pressure_iterations=args.train_sweeps)
+        pairs += sf.warmstart.generate_pairs(sf, scene, steps=args.train_steps, skip=2)
+    t_pairs = time.perf_counter() - t0
+    net = sf.WarmStartNetwork(seed=0, device=device)
+    h = float(sf.scenes.training_scene(0, n=args.train_size).config.cell_size)
+    history = sf.warmstart.train(net, pairs, h, epochs=args.train_epochs, learning_rate=args.learning_rate, deadline=time.perf_counter() + args.train_seconds)
+    info = {"pairs": len(pairs), "grid": [args.train_size] * 3, "target_sweeps": args.train_sweeps, "epochs_run": len(history), "loss_per_epoch": history,
+            "pair_generation_s": t_pairs, "training_s": time.perf_counter() - t0 - t_pairs}
+    del pairs
+    return net, info
+
+
+def time_pressure_sweep(sf, scene, device):
+    """Average duration of one Jacobi pressure sweep (k_jacobi_vec), CUDA
+    events on the context stream: the fixed-count pressure stage of a Jacobi
+    context enqueued directly (80 sweeps per stage)."""
     import torch
 
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    sim.enqueue_stage(stage)  # warm
+    o = sf.default_options()
+    o.scheme = sf.SCHEME_JACOBI
+    o.warm_start = sf.WARM_START_PREVIOUS
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=o, device=device)
+    sf.scenes.apply_inputs(sim, scene, 0)
+    sim.step(1)
+    sim.enqueue_stage(sf.STAGE_PRESSURE)
     torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches = 0
     start.record(sim.stream)
-    for _ in range(repeats):
-        launches += sim.enqueue_stage(stage)
+    for _ in range(3):
+        launches += sim.enqueue_stage(sf.STAGE_PRESSURE)
     end.record(sim.stream)
     torch.cuda.synchronize()
-    return start.elapsed_time(end) / 1000.0, launches
+    sim.close()
+    return start.elapsed_time(end) / 1000.0 / max(launches, 1)
+
+
+def time_network(net, n, device, repeats=3):
+    """Duration of one prediction at n^3 (CUDA events on the network stream)."""
+    import torch
+
+    b = torch.randn(n, n, n, device=device)
+    p = 0.1 * torch.randn(n, n, n, device=device)
+    out = torch.empty_like(b)
+    lib = net.lib
+    args = (net.handle, b.data_ptr(), p.data_ptr(), n, n, n, 1.0 / n, out.data_ptr(), net.stream.cuda_stream)
+    lib.stable_fluids_b200_network_predict(*args)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(net.stream)
+    for _ in range(repeats):
+        lib.stable_fluids_b200_network_predict(*args)
+    end.record(net.stream)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end) / 1000.0 / repeats
+
+
+def network_flops(n):
+    """Multiply-adds x 2 of one prediction at n^3, counting only real
+    channels (2 input channels of the first layer, 1 output channel)."""
+    v0, v1, v2 = n ** 3, (n // 2) ** 3, (n // 4) ** 3
+    macs = 27 * (v0 * (2 * 16 + 16 * 16 + 48 * 16 + 16 * 16 + 16 * 1) + v1 * (16 * 32 + 32 * 32 + 96 * 32 + 32 * 32) + v2 * (32 * 64 + 64 * 64))
+    return 2.0 * macs
 
 
 def e2e_run(sf, sim, scene, steps):
@@ -214,145 +336,182 @@ def e2e_run(sf, sim, scene, steps):
     return t, 3 * n * 4, n * 4
 
 
-def equal_residual(sf, scene, variants, tol, steps, cap, warmup):
-    """Steps/s of the plume when the pressure is iterated until the FP64
-    relative Poisson residual is <= tol (inside the step graph), for solver
-    variants scheme-warmstart; reports the iterations each step needed."""
+def fixed_iterations(sf, lib, scene, steps, warmup, device, world):
+    """The reference's configuration as it is: 80 red-black pressure
+    iterations from zero per step (results bit-identical to the reference)."""
     import torch
 
-    out = {}
-    for v in variants:
-        scheme, warm = v.split("-")
-        opts = sf.default_options()
-        opts.scheme = sf.SCHEME_JACOBI if scheme == "jacobi" else sf.SCHEME_RBGS
-        opts.warm_start = {"zero": sf.WARM_START_ZERO, "previous": sf.WARM_START_PREVIOUS}[warm]
-        opts.residual_tolerance = tol
-        opts.residual_check_interval = 16
-        opts.max_pressure_iterations = cap
-        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts)
-        sf.scenes.apply_inputs(sim, scene, 0)
-        sim.step(warmup)
-        torch.cuda.synchronize()
-        its, res, total = [], [], 0.0
-        for _ in range(steps):
-            start = torch.cuda.Event(enable_timing=True)
-            end = torch.cuda.Event(enable_timing=True)
-            start.record(sim.stream)
-            sim.step(1)
-            end.record(sim.stream)
-            st = sim.stats()
-            total += start.elapsed_time(end) / 1000.0
-            its.append(st.pressure_iterations)
-            res.append(st.rel_residual)
-        sim.close()
-        out[v] = {"steps_per_s": steps / total, "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > tol for r in res)}
-    return out
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, device=device)
+    sf.scenes.apply_inputs(sim, scene, 0)
+    sim.step(warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(sim.stream)
+    sim.step(steps)
+    end.record(sim.stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(start.elapsed_time(end) / 1000.0, world)
+    sim.close()
+    return {"steps_per_s": world * steps / t, "ms_per_step": 1000.0 * t / steps, "steps": steps, "pressure_iterations": scene.config.pressure_iterations, "scheme": "rbgs"}
 
 
-def cpu_baseline(sf, scene, steps):
+def cpu_baseline(sf, scene, plain_iterations):
+    """The FP32 C++/OpenMP transcription of the step (oracle/) on all host
+    cores: one step without pressure sweeps and one with 16 Jacobi sweeps,
+    scaled to the plain variant's mean sweep count."""
     from oracle import oracle as orc
 
     threads = orc.set_threads(os.cpu_count() or 1)
-    o = orc.Oracle(scene.config, scene.scalars, scene.vectors, precision=32)
-    sf.scenes.apply_inputs(o, scene, 0)
-    t0 = time.perf_counter()
-    o.step(steps)
-    t = time.perf_counter() - t0
-    o.close()
+    times = {}
+    for p in (0, 16):
+        cfg = type(scene.config).from_buffer_copy(scene.config)
+        cfg.pressure_iterations = p
+        o = orc.Oracle(cfg, scene.scalars, scene.vectors, precision=32, scheme=orc.JACOBI)
+        sf.scenes.apply_inputs(o, scene, 0)
+        t0 = time.perf_counter()
+        o.step(1)
+        times[p] = time.perf_counter() - t0
+        o.close()
+    sweep = max(times[16] - times[0], 0.0) / 16
     n = scene.config.nx
-    return {"value": steps / t, "unit": "steps/s", "cores": threads, "kind": "port", "sample": f"{steps} step(s) of the {n}^3 workload, FP32 C++/OpenMP transcription of backend-cuda.cu's step sequence"}
+    value = 1.0 / (times[0] + plain_iterations * sweep)
+    return {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"1 step of the {n}^3 plume without pressure sweeps ({times[0]:.2f} s) and 1 with 16 Jacobi sweeps ({times[16]:.2f} s) on {threads} threads; steps/s = 1 / (t_step + N x t_sweep) with N = {plain_iterations:.0f}, the mean sweep count of the plain variant (same arithmetic)"}
+
+
+def reference_arm(sf, args, scene, world, rank, local):
+    """The reference backend (oracle/_ref) at equal residual: calibrate the
+    iteration count with this library's red-black solve from zero (the
+    reference's arithmetic, bit-identical), then time the reference with that
+    fixed count."""
+    import torch
+
+    from oracle import oracle as orc
+
+    if rank != 0:
+        return None
+    # calibration (untimed): iterations the reference arithmetic needs in each step
+    opts = solver_options(sf, "rbgs", args.tolerance, args.cap, 0)
+    cal = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=local)
+    sf.scenes.apply_inputs(cal, scene, 0)
+    needed = []
+    for _ in range(args.warmup + args.steps):
+        cal.step(1)
+        needed.append(cal.stats().pressure_iterations)
+    cal.close()
+    iterations = max(needed[args.warmup:])
+    lib = sf.load_library(orc.REF_LIB_PATH)
+    cfg = type(scene.config).from_buffer_copy(scene.config)
+    cfg.pressure_iterations = iterations
+    sim = sf.Simulation(cfg, scene.scalars, scene.vectors, lib=lib, device=local)
+    sf.scenes.apply_inputs(sim, scene, 0)
+    sim.step(args.warmup)
+    torch.cuda.synchronize()
+    with Clocks(local, not args.no_clocks) as clk:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(sim.stream)
+        sim.step(args.steps)
+        end.record(sim.stream)
+        torch.cuda.synchronize()
+    t = start.elapsed_time(end) / 1000.0
+    sim.close()
+    value = args.steps / t
+    n = args.size
+    config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g}, 1 scalar + 1 force field, Stam walls", "grid": [n, n, n],
+              "solver": f"reference red-black Gauss-Seidel from zero, {iterations} iterations per step (the most any timed step needs for rel_res <= {args.tolerance:g}; per-step needs {needed[args.warmup:]})",
+              "l2": "working set > L2 (no flush needed)", "parallelism": "single GPU"}
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)",
+            "config": config, "cell_updates_per_s": value * n ** 3,
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": f"{args.steps} steps; the reference has no CPU implementation, so its own CUDA backend (backend-cuda.cu built unmodified for sm_100a) runs on the GPU"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["fixed_iterations"] = fixed_iterations(sf, lib, scene, args.fixed_steps, args.warmup, local, 1)
+    c = clk.summary()
+    if c:
+        line["clocks"] = c
+    return line
 
 
 def main():
     args = parse()
     import torch
 
-    world, rank, local = dist_setup(args)
+    world, rank, local = dist_setup()
     sf = importlib.import_module("stable-fluids_b200")
     scene = sf.scenes.config1(n=args.size)
     n = args.size
-    config = {"workload": f"plume {n}^3 FP32, 20 diffusion + 80 pressure iterations, 1 scalar + 1 force field, Stam walls",
-              "grid": [n, n, n], "scheme": args.scheme, "l2": "working set > L2 (no flush needed)", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
-        from oracle import oracle as orc
+        line = reference_arm(sf, args, scene, world, rank, local)
+        if line is not None:
+            print(json.dumps(line))
+        if world > 1:
+            import torch.distributed as dist
 
-        if world > 1 and rank != 0:
-            return
-        lib = sf.load_library(orc.REF_LIB_PATH)
-        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib)
-        sf.scenes.apply_inputs(sim, scene, 0)
-        sim.step(args.warmup)
-        torch.cuda.synchronize()
-        with Clocks(local, not args.no_clocks) as clk:
-            t = time_steps(sim, args.steps, 1)
-        value = args.steps / t
-        line = {"metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)",
-                "config": config, "cell_updates_per_s": value * n ** 3,
-                "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": f"{args.steps} steps; the reference has no CPU implementation, so its own CUDA backend (backend-cuda.cu built unmodified for sm_100a) runs on the GPU"},
-                "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        c = clk.summary()
-        if c:
-            line["clocks"] = c
-        print(json.dumps(line))
-        sim.close()
+            dist.destroy_process_group()
         return
 
-    opts = sf.default_options()
-    opts.scheme = sf.SCHEME_JACOBI if args.scheme == "jacobi" else sf.SCHEME_RBGS
-    opts.iterations_per_pass = args.iterations_per_pass
-    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=local)
-    sf.scenes.apply_inputs(sim, scene, 0)
-    sim.step(args.warmup)
-    torch.cuda.synchronize()
-    info = sim.info()
+    variants = [v for v in args.variants.split(",") if v]
+    if "learned" not in variants:
+        variants.insert(0, "learned")
+    net, train_info = train_network(sf, args, local)
 
+    results, sims = {}, {}
     with Clocks(local, not args.no_clocks and rank == 0) as clk:
-        t = time_steps(sim, args.steps, world)
-    t = max_over_ranks(t, world)
-    value = world * args.steps / t
+        for v in variants:
+            sim, out = run_variant(sf, scene, v, args, world, local, net if v == "learned" else None)
+            results[v] = out
+            if v == "learned":
+                sims[v] = sim
+            else:
+                sim.close()
+    learned = results["learned"]
+    value = learned["steps_per_s"]
 
-    # roofline of the dominant kernel family: the pressure solve
+    # roofline: the Jacobi sweep dominates every variant's step
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except (OSError, ValueError):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    tc_peak = float(peaks.get("bf16_tflops", 1590.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    t_stage, launches = time_stage(sim, sf.STAGE_PRESSURE, 3)
-    per_launch = t_stage / max(launches, 1)
+    sweep_s = time_pressure_sweep(sf, scene, local)
     cells = n ** 3
-    if args.scheme == "jacobi" or not info.blocked:
-        bytes_per_launch = (12 if args.scheme == "jacobi" else 6) * cells
-        unit_note = "one Jacobi sweep: read x + rhs, write x = 12 B/cell" if args.scheme == "jacobi" else "one red-black colour sweep: read n/2 other colour + n/2 rhs, write n/2 = 6 B/cell"
-    else:
-        bytes_per_launch = 12 * cells
-        unit_note = "one temporally blocked pass: read p + rhs, write p = 12 B/cell"
-    achieved = bytes_per_launch / per_launch / 1e9
-    roofline = {"bound": "hbm", "kernel": "pressure stencil", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": None, "bytes_per_launch": bytes_per_launch, "launch_us": per_launch * 1e6, "unit_of_work": unit_note}
+    bytes_per_sweep = 12 * cells
+    achieved = bytes_per_sweep / sweep_s / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_jacobi_vec (Jacobi pressure sweep)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": None, "bytes_per_launch": bytes_per_sweep, "launch_us": sweep_s * 1e6, "unit_of_work": "one Jacobi sweep of 256^3 cells: read p + rhs, write p = 12 B/cell"}
+    net_s = time_network(net, n, torch.device("cuda", local))
+    flops = network_flops(n)
+    roofline_network = {"bound": "tensor", "kernel": "warm-start network prediction (all layers)", "achieved": flops / net_s / 1e12, "peak": tc_peak, "peak_source": peak_src, "unit": "TFLOP/s",
+                        "frac": flops / net_s / 1e12 / tc_peak, "flop_per_launch": flops, "launch_ms": net_s * 1e3, "unit_of_work": "one prediction at 256^3, real channels only"}
 
     e2e = None
     if args.e2e_steps > 0:
-        te, h2d, d2h = e2e_run(sf, sim, scene, args.e2e_steps)
+        te, h2d, d2h = e2e_run(sf, sims["learned"], scene, args.e2e_steps)
         te = max_over_ranks(te, world)
         e2e = {"value": world * args.e2e_steps / te, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps}
+    sims["learned"].close()
+    fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world)
 
-    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
+    config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
+              "grid": [n, n, n], "solver": "Jacobi sweeps from the learned warm start", "l2": "working set > L2 (no flush needed)",
+              "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
-            "cell_updates_per_s": value * cells, "gpu_launches": info.kernels_per_step * args.steps, "kernels_per_step": info.kernels_per_step,
-            "roofline": roofline, "e2e": e2e}
+            "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"],
+            "speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
+            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed}
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c
-    if rank == 0 and world == 1 and args.equal_residual:
-        variants = [v for v in args.equal_residual.split(",") if v]
-        line["equal_residual"] = {"tolerance": args.residual_tolerance, "steps": args.residual_steps, "warmup": 2, "variants": equal_residual(sf, scene, variants, args.residual_tolerance, args.residual_steps, args.residual_cap, 2)}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sf, scene, args.cpu_steps)
-    sim.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and "plain" in results:
+        line["cpu_baseline"] = cpu_baseline(sf, scene, statistics.mean(results["plain"]["pressure_iterations"]))
+    net.close()
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -155,6 +155,20 @@ def config1(steps=50, seed=1, n=256) -> Scene:
     return plume(f"config1-{n}^3", (n, n, n), dt=0.1, viscosity=1e-4, diffusion=1e-5, diffuse_iterations=20, pressure_iterations=80, sources=sources, steps=steps)
 
 
+def training_scene(seed: int, n: int = 128, pressure_iterations: int = 1000) -> Scene:
+    """Learned warm start, training scenes: an n^3 plume (config-0
+    coefficients) with 1-4 Gaussian sources of radius U[4, 12] cells at
+    seeded floor positions, each with an upward force U[1, 10]; the pressure
+    solve is the target generator (`pressure_iterations` sweeps)."""
+    rng = np.random.default_rng(1000 + seed)
+    sources = []
+    for _ in range(int(rng.integers(1, 5))):
+        r = float(rng.uniform(4.0, 12.0))
+        cx, cz = rng.uniform(r + 2, n - r - 2, size=2)
+        sources.append((float(cx), 4 + r, float(cz), r, 10.0, float(rng.uniform(1.0, 10.0))))
+    return plume(f"train-{seed}-{n}^3", (n, n, n), dt=0.1, viscosity=1e-4, diffusion=1e-5, diffuse_iterations=20, pressure_iterations=pressure_iterations, sources=sources, steps=1)
+
+
 def apply_inputs(sim, scene: Scene, step_index: int):
     """Uploads the scene's source and force for step `step_index` (the
     impulse only on step 0). `sim` is anything with set_scalar_source and

@@ -203,3 +203,39 @@ def training_pairs(make_simulation, steps: int, skip: int = 0):
     finally:
         sim.synchronize()
         sim.close()
+
+
+def generate_pairs(sf, scene, steps: int, skip: int = 2, lib=None):
+    """(b, p_prev, p_target) device tensors from `steps` steps of `scene`
+    after `skip` plain ones, with the scene's pressure solve (Jacobi sweeps
+    from the previous pressure) as the target generator."""
+    def make():
+        o = sf.default_options(lib)
+        o.scheme = sf.SCHEME_JACOBI
+        o.warm_start = sf.WARM_START_PREVIOUS
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=o)
+        sf.scenes.apply_inputs(sim, scene, 0)
+        return sim
+
+    return list(training_pairs(make, steps=steps, skip=skip))
+
+
+def train(net, pairs, cell_size: float, epochs: int, learning_rate: float, seed: int = 0, deadline: float | None = None):
+    """Adam over `pairs` in shuffled order for `epochs` epochs (or until the
+    perf_counter `deadline`); returns the per-epoch mean losses."""
+    import time
+
+    rng = np.random.default_rng(seed)
+    history = []
+    for _ in range(epochs):
+        order = rng.permutation(len(pairs))
+        losses = []
+        for k in order:
+            b, p, t = pairs[k]
+            losses.append(net.train_step(b, p, t, cell_size, learning_rate))
+            if deadline is not None and time.perf_counter() > deadline:
+                break
+        history.append(float(np.mean(losses)))
+        if deadline is not None and time.perf_counter() > deadline:
+            break
+    return history
