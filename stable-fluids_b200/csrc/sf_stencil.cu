@@ -84,9 +84,7 @@ __global__ void __launch_bounds__(256) k_rbgs_colour(float* x, const float* __re
 #pragma unroll
     for (int k = 0; k < kColourPlanes; ++k) {
         if (!ok[k]) continue;
-        float q = tb::markstein_div(num[k], divisor, recip);
-        if (tb::needs_ieee_div(num[k])) q = num[k] / divisor;
-        x[idx[k]] = q;
+        x[idx[k]] = tb::update_div<KIND>(num[k], divisor, recip);
     }
 }
 
@@ -116,9 +114,7 @@ __global__ void __launch_bounds__(256) k_jacobi(float* __restrict__ dst, const f
             nb = neighbour_sum<KIND>(src, cx, y, z, d, fb, sb);
         }
         const float num = tb::numerator<KIND>(nb, rhs[i], coef);
-        float q = tb::markstein_div(num, divisor, recip);
-        if (tb::needs_ieee_div(num)) q = num / divisor;
-        dst[i] = q;
+        dst[i] = tb::update_div<KIND>(num, divisor, recip);
     }
 }
 
@@ -169,10 +165,7 @@ __device__ __forceinline__ float4 ghost4(const GhostRule& g, int face, float4 se
 
 template <int KIND>
 __device__ __forceinline__ float vec_update(float nb, float rhs, float coef, float divisor, float recip) {
-    const float num = tb::numerator<KIND>(nb, rhs, coef);
-    float q = tb::markstein_div(num, divisor, recip);
-    if (tb::needs_ieee_div(num)) q = num / divisor;
-    return q;
+    return tb::update_div<KIND>(tb::numerator<KIND>(nb, rhs, coef), divisor, recip);
 }
 
 // The plane below the chunk's first plane (or its ghost at z = 0).
@@ -264,8 +257,9 @@ __global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec(float* x, const floa
     }
 }
 
-// Launch shape of the vectorised kernels: z chunks sized so that the grid
-// fills the resident CTA slots of all SMs about once.
+// Launch shape of the vectorised kernels: as many z chunks as fit the
+// resident CTA slots of all SMs in one wave (a partial second wave costs
+// more than the longer march per CTA).
 struct VecShape {
     dim3 grid;
     int z_chunk;
@@ -283,7 +277,7 @@ VecShape vec_shape(const Dims& d, Kernel kernel) {
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int bx = (d.nx / 4 + 31) / 32, by = (d.ny + kVecRows - 1) / kVecRows;
     const long long slots = static_cast<long long>(sms) * per_sm;
-    long long chunks = (slots + static_cast<long long>(bx) * by - 1) / (static_cast<long long>(bx) * by);
+    long long chunks = slots / (static_cast<long long>(bx) * by);  // one wave: every CTA resident at once
     if (chunks < 1) chunks = 1;
     int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
     if (z_chunk < 4) z_chunk = d.nz < 4 ? d.nz : 4;

@@ -156,6 +156,44 @@ __device__ __forceinline__ float markstein_div(float n, float d, float y) {
 }
 __device__ __forceinline__ bool needs_ieee_div(float n) { return !(fabsf(n) >= 0x1p-99f) && n != 0.0f; }
 
+// n / d for those numerators: the quotient of the FP64 operands rounded once
+// to FP64 and then to FP32. Double rounding through a format with at least
+// 2p + 2 bits (53 >= 2 * 24 + 2) is innocuous for division (S. Figueroa,
+// "When is double rounding innocuous?", SIGNUM Newsl. 30(3), 1995), so this
+// is the correctly rounded FP32 quotient -- checked against IEEE FP32
+// division for all 2^32 numerators with d = 6 -- and, unlike FP32 division
+// of a tiny numerator, it has no scaling slow path.
+__device__ __forceinline__ float tiny_div(float n, float d) { return static_cast<float>(__ddiv_rn(static_cast<double>(n), static_cast<double>(d))); }
+
+// n / 6 for the pressure update, correctly rounded for every FP32 n (checked
+// against IEEE division for all 2^32 numerators). Markstein's correction for
+// |n| >= 2^-99; below that, n scaled by 2^64 (exact) while the quotient is
+// normal, and for quotients in the subnormal range (|n| < 6 * 2^-126) the
+// exact integer rounding of N / 6 with N = |n| / 2^-149 (round half to even),
+// since every such quotient is a multiple of 2^-149.
+__device__ __forceinline__ float div6_tiny(float n) {
+    if (n == 0.0f) return n;
+    const float a = fabsf(n);
+    if (a >= 0x1.8p-124f) return markstein_div(__fmul_rn(n, 0x1p64f), 6.0f, 1.0f / 6.0f) * 0x1p-64f;
+    const uint32_t big = static_cast<uint32_t>(a * 0x1p100f * 0x1p49f);
+    uint32_t k = big / 6u;
+    const uint32_t r = big - 6u * k;
+    if (r > 3u || (r == 3u && (k & 1u))) ++k;
+    return copysignf(static_cast<float>(k) * 0x1p-100f * 0x1p-49f, n);
+}
+
+// The division of a stencil update by its divisor: exact n / 6 for the
+// pressure, Markstein with the FP64 fallback for the diffusion divisors.
+template <int KIND>
+__device__ __forceinline__ float update_div(float n, float divisor, float recip) {
+    float q = markstein_div(n, divisor, recip);
+    if (needs_ieee_div(n)) {
+        if constexpr (KIND == KIND_PRESSURE) q = div6_tiny(n);
+        else q = tiny_div(n, divisor);
+    }
+    return q;
+}
+
 // Numerator of the update in the reference's expression shape
 // (backend-cuda.cu:363, :406), so the compiler fuses it the same way.
 template <int KIND>
@@ -232,7 +270,7 @@ __device__ __forceinline__ void stage_all(const Combo* combo, float* xs, const f
             bool ok = lane_ok[k] && pair < npairs;
             if (mask_y) ok = ok && static_cast<unsigned>(gy_base + s + 2 * PG * m) < static_cast<unsigned>(ny);
             float q = tb::markstein_div(num[k][m], divisor, recip);
-            if (any_rare && tb::needs_ieee_div(num[k][m])) q = num[k][m] / divisor;
+            if (any_rare && tb::needs_ieee_div(num[k][m])) q = KIND == KIND_PRESSURE ? tb::div6_tiny(num[k][m]) : tb::tiny_div(num[k][m], divisor);
             if (ok) cell[k][m * STEP] = q;
         }
 }
