@@ -13,8 +13,10 @@
 // correction to the previous pressure: p0 = p_prev + out / scale. Grid sides
 // must be multiples of 4 (two poolings).
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
@@ -26,6 +28,7 @@
 #include "sf_types.h"
 #include "sf_unet.h"
 #include "sf_unet_kernels.cuh"
+#include "sf_unet_tc.cuh"
 #include "stable-fluids-b200.h"
 
 namespace sfb::net {
@@ -80,6 +83,7 @@ struct Net {
     float* v = nullptr;
     __nv_bfloat16* w16 = nullptr;   // BF16 weights [tap][cout][cin] per layer
     __nv_bfloat16* w16t = nullptr;  // BF16 transposed, tap-flipped weights [tap][cin][cout] (data gradient)
+    unsigned* error = nullptr;      // set by a convolution whose bounded wait gave up
     int adam_t = 0;
     // One buffer set per grid size, kept until the network is destroyed so
     // that step graphs holding their addresses stay valid.
@@ -96,28 +100,67 @@ struct Net {
         cudaFree(v);
         cudaFree(w16);
         cudaFree(w16t);
+        cudaFree(error);
     }
 };
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+int sm_count() {
+    static const int n = [] {
+        int dev = 0, v = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 148;
+        return v;
+    }();
+    return n;
+}
+
+// 3x3x3 convolution on the tensor cores (tc::k_conv3d_tc): tensor maps for
+// the channels-last input (boxes of 8 channels x (TX + 2) x (TY + 2) x 1
+// voxels) and the [27][COUT][CIN] weights (boxes of 8 input channels x COUT
+// x 27 taps), then one persistent CTA per SM.
 template <int CIN, int COUT, int EPI>
-cudaError_t conv(const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, void* out, int out_ch, int out_off, Dims d, cudaStream_t s) {
-    constexpr size_t smem = conv_smem_bytes<CIN>();
-    if constexpr (smem > 48 * 1024) {
-        const cudaError_t attr = cudaFuncSetAttribute(k_conv3d<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        if (attr != cudaSuccess) return attr;
-    }
-    const dim3 grid(static_cast<unsigned>((d.nx + kTileX - 1) / kTileX), static_cast<unsigned>((d.ny + kTileY - 1) / kTileY), static_cast<unsigned>(d.nz));
-    k_conv3d<CIN, COUT, EPI><<<grid, 128, smem, s>>>(in, w, bias, out, out_ch, out_off, d);
+cudaError_t conv(const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, void* out, int out_ch, int out_off, Dims d, cudaStream_t s, unsigned* error) {
+    using C = tc::Cfg<CIN, COUT>;
+    auto encode = tensor_map_encoder();
+    if (encode == nullptr) return cudaErrorNotSupported;
+    CUtensorMap map_in{}, map_w{};
+    const cuuint64_t gd[4] = {static_cast<cuuint64_t>(CIN), static_cast<cuuint64_t>(d.nx), static_cast<cuuint64_t>(d.ny), static_cast<cuuint64_t>(d.nz)};
+    const cuuint64_t gs[3] = {static_cast<cuuint64_t>(CIN) * 2, static_cast<cuuint64_t>(d.nx) * CIN * 2, static_cast<cuuint64_t>(d.ny) * d.nx * CIN * 2};
+    const cuuint32_t box[4] = {8u, static_cast<cuuint32_t>(tc::P), static_cast<cuuint32_t>(C::TY + 2), 1u};
+    const cuuint32_t es[4] = {1u, 1u, 1u, 1u};
+    if (encode(&map_in, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(in), gd, gs, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    const cuuint64_t wd[3] = {static_cast<cuuint64_t>(CIN), static_cast<cuuint64_t>(COUT), 27u};
+    const cuuint64_t ws[2] = {static_cast<cuuint64_t>(CIN) * 2, static_cast<cuuint64_t>(COUT) * CIN * 2};
+    const cuuint32_t wbox[3] = {8u, static_cast<cuuint32_t>(COUT), 27u};
+    if (encode(&map_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(w), wd, ws, wbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    auto kern = tc::k_conv3d_tc<CIN, COUT, EPI>;
+    const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
+    if (attr != cudaSuccess) return attr;
+    tc::ConvArgs a{out, bias, out_ch, out_off, d, (d.nx + tc::TX - 1) / tc::TX, (d.ny + C::TY - 1) / C::TY, error};
+    const int tiles = a.tiles_x * a.tiles_y * d.nz;
+    const int grid = tiles < sm_count() ? tiles : sm_count();
+    kern<<<grid, tc::kThreadsTC, C::BYTES, s>>>(map_in, map_w, a);
     return cudaGetLastError();
 }
 
 // Runtime dispatch of the (cin, cout) combinations the network uses.
-cudaError_t conv_any(int cin, int cout, int epi, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, void* out, int out_ch, int out_off, Dims d, cudaStream_t s) {
-#define SFB_CONV(CI, CO)                                                                                        \
-    if (cin == CI && cout == CO) {                                                                              \
-        if (epi == EPI_RELU_BF16) return conv<CI, CO, EPI_RELU_BF16>(in, w, bias, out, out_ch, out_off, d, s);     \
-        if (epi == EPI_LINEAR_BF16) return conv<CI, CO, EPI_LINEAR_BF16>(in, w, bias, out, out_ch, out_off, d, s); \
-        return conv<CI, CO, EPI_LINEAR_F32_CH0>(in, w, bias, out, out_ch, out_off, d, s);                          \
+cudaError_t conv_any(int cin, int cout, int epi, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, void* out, int out_ch, int out_off, Dims d, cudaStream_t s, unsigned* error) {
+#define SFB_CONV(CI, CO)                                                                                                     \
+    if (cin == CI && cout == CO) {                                                                                           \
+        if (epi == tc::RELU_BF16) return conv<CI, CO, tc::RELU_BF16>(in, w, bias, out, out_ch, out_off, d, s, error);          \
+        if (epi == tc::LINEAR_BF16) return conv<CI, CO, tc::LINEAR_BF16>(in, w, bias, out, out_ch, out_off, d, s, error);      \
+        return conv<CI, CO, tc::LINEAR_F32_CH0>(in, w, bias, out, out_ch, out_off, d, s, error);                               \
     }
     SFB_CONV(16, 16) SFB_CONV(16, 32) SFB_CONV(32, 32) SFB_CONV(32, 64) SFB_CONV(64, 64) SFB_CONV(96, 32) SFB_CONV(48, 16)  // forward
     SFB_CONV(32, 16) SFB_CONV(64, 32) SFB_CONV(32, 96) SFB_CONV(16, 48)                                                     // data gradients
@@ -175,6 +218,7 @@ Net* create_net(uint32_t seed) {
     const size_t fb = off * sizeof(float);
     if (cudaMalloc(&n->w, fb) != cudaSuccess || cudaMalloc(&n->g, fb) != cudaSuccess || cudaMalloc(&n->m, fb) != cudaSuccess || cudaMalloc(&n->v, fb) != cudaSuccess) return nullptr;
     if (cudaMalloc(&n->w16, off * sizeof(__nv_bfloat16)) != cudaSuccess || cudaMalloc(&n->w16t, off * sizeof(__nv_bfloat16)) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&n->error, sizeof(unsigned)) != cudaSuccess || cudaMemset(n->error, 0, sizeof(unsigned)) != cudaSuccess) return nullptr;
     // He initialisation over the real fan-in (the output layer 10x smaller);
     // padded input channels and padded output channels of the last layer are
     // zero; biases zero.
@@ -291,23 +335,23 @@ cudaError_t forward(Net* n, const float* b, float b_factor, const float* p_prev,
     k_finish_scale<<<1, 32, 0, s>>>(B.sums, static_cast<double>(B.n0), B.scale);
     k_pack_input<<<blocks_for(B.n0), 256, 0, s>>>(b, p_prev, B.scale, b_factor, B.in, B.n0);
     SFB_TRY(cudaGetLastError());
-    SFB_TRY(conv_any(16, 16, EPI_RELU_BF16, B.in, W(n, E0A), Bias(n, E0A), B.e0a, 16, 0, B.d0, s));
-    SFB_TRY(conv_any(16, 16, EPI_RELU_BF16, B.e0a, W(n, E0B), Bias(n, E0B), B.e0b, 16, 0, B.d0, s));
+    SFB_TRY(conv_any(16, 16, tc::RELU_BF16, B.in, W(n, E0A), Bias(n, E0A), B.e0a, 16, 0, B.d0, s, n->error));
+    SFB_TRY(conv_any(16, 16, tc::RELU_BF16, B.e0a, W(n, E0B), Bias(n, E0B), B.e0b, 16, 0, B.d0, s, n->error));
     k_pool2<<<blocks_for(B.n1 * 16), 256, 0, s>>>(B.e0b, 16, 0, B.p0, 16, B.d1);
-    SFB_TRY(conv_any(16, 32, EPI_RELU_BF16, B.p0, W(n, E1A), Bias(n, E1A), B.e1a, 32, 0, B.d1, s));
-    SFB_TRY(conv_any(32, 32, EPI_RELU_BF16, B.e1a, W(n, E1B), Bias(n, E1B), B.e1b, 32, 0, B.d1, s));
+    SFB_TRY(conv_any(16, 32, tc::RELU_BF16, B.p0, W(n, E1A), Bias(n, E1A), B.e1a, 32, 0, B.d1, s, n->error));
+    SFB_TRY(conv_any(32, 32, tc::RELU_BF16, B.e1a, W(n, E1B), Bias(n, E1B), B.e1b, 32, 0, B.d1, s, n->error));
     k_pool2<<<blocks_for(B.n2 * 32), 256, 0, s>>>(B.e1b, 32, 0, B.p1, 32, B.d2);
-    SFB_TRY(conv_any(32, 64, EPI_RELU_BF16, B.p1, W(n, BA), Bias(n, BA), B.ba, 64, 0, B.d2, s));
-    SFB_TRY(conv_any(64, 64, EPI_RELU_BF16, B.ba, W(n, BB), Bias(n, BB), B.bb, 64, 0, B.d2, s));
+    SFB_TRY(conv_any(32, 64, tc::RELU_BF16, B.p1, W(n, BA), Bias(n, BA), B.ba, 64, 0, B.d2, s, n->error));
+    SFB_TRY(conv_any(64, 64, tc::RELU_BF16, B.ba, W(n, BB), Bias(n, BB), B.bb, 64, 0, B.d2, s, n->error));
     k_upsample2<<<blocks_for(B.n1 * 64), 256, 0, s>>>(B.bb, 64, B.d2, B.cat1, 96, 0);
     k_copy_channels<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.e1b, 32, 0, B.cat1, 96, 64, 32, B.n1, 0);
-    SFB_TRY(conv_any(96, 32, EPI_RELU_BF16, B.cat1, W(n, D1A), Bias(n, D1A), B.d1a, 32, 0, B.d1, s));
-    SFB_TRY(conv_any(32, 32, EPI_RELU_BF16, B.d1a, W(n, D1B), Bias(n, D1B), B.d1b, 32, 0, B.d1, s));
+    SFB_TRY(conv_any(96, 32, tc::RELU_BF16, B.cat1, W(n, D1A), Bias(n, D1A), B.d1a, 32, 0, B.d1, s, n->error));
+    SFB_TRY(conv_any(32, 32, tc::RELU_BF16, B.d1a, W(n, D1B), Bias(n, D1B), B.d1b, 32, 0, B.d1, s, n->error));
     k_upsample2<<<blocks_for(B.n0 * 32), 256, 0, s>>>(B.d1b, 32, B.d1, B.cat0, 48, 0);
     k_copy_channels<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.e0b, 16, 0, B.cat0, 48, 32, 16, B.n0, 0);
-    SFB_TRY(conv_any(48, 16, EPI_RELU_BF16, B.cat0, W(n, D0A), Bias(n, D0A), B.d0a, 16, 0, B.d0, s));
-    SFB_TRY(conv_any(16, 16, EPI_RELU_BF16, B.d0a, W(n, D0B), Bias(n, D0B), B.d0b, 16, 0, B.d0, s));
-    SFB_TRY(conv_any(16, 16, EPI_LINEAR_F32_CH0, B.d0b, W(n, OUT), Bias(n, OUT), B.out, 1, 0, B.d0, s));
+    SFB_TRY(conv_any(48, 16, tc::RELU_BF16, B.cat0, W(n, D0A), Bias(n, D0A), B.d0a, 16, 0, B.d0, s, n->error));
+    SFB_TRY(conv_any(16, 16, tc::RELU_BF16, B.d0a, W(n, D0B), Bias(n, D0B), B.d0b, 16, 0, B.d0, s, n->error));
+    SFB_TRY(conv_any(16, 16, tc::LINEAR_F32_CH0, B.d0b, W(n, OUT), Bias(n, OUT), B.out, 1, 0, B.d0, s, n->error));
     return cudaGetLastError();
 }
 
@@ -321,45 +365,45 @@ cudaError_t backward(Net* n, cudaStream_t s) {
     SFB_TRY(cudaMemsetAsync(n->g, 0, n->nparams * sizeof(float), s));
     // out layer (linear)
     SFB_TRY(wgrad_any(16, 16, B.d0b, B.g16, GW(n, OUT), GB(n, OUT), B.d0, s));
-    SFB_TRY(conv_any(16, 16, EPI_LINEAR_BF16, B.g16, WT(n, OUT), nullptr, B.gd0b, 16, 0, B.d0, s));
+    SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.g16, WT(n, OUT), nullptr, B.gd0b, 16, 0, B.d0, s, n->error));
     // d0b, d0a (input of d0a: cat0 = [up(d1b) | e0b])
     k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gd0b, B.d0b, B.n0 * 16);
     SFB_TRY(wgrad_any(16, 16, B.d0a, B.gd0b, GW(n, D0B), GB(n, D0B), B.d0, s));
-    SFB_TRY(conv_any(16, 16, EPI_LINEAR_BF16, B.gd0b, WT(n, D0B), nullptr, B.gd0a, 16, 0, B.d0, s));
+    SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.gd0b, WT(n, D0B), nullptr, B.gd0a, 16, 0, B.d0, s, n->error));
     k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gd0a, B.d0a, B.n0 * 16);
     SFB_TRY(wgrad_any(48, 16, B.cat0, B.gd0a, GW(n, D0A), GB(n, D0A), B.d0, s));
-    SFB_TRY(conv_any(16, 48, EPI_LINEAR_BF16, B.gd0a, WT(n, D0A), nullptr, B.gcat0, 48, 0, B.d0, s));
+    SFB_TRY(conv_any(16, 48, tc::LINEAR_BF16, B.gd0a, WT(n, D0A), nullptr, B.gcat0, 48, 0, B.d0, s, n->error));
     k_upsample2_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gcat0, 48, 0, 32, B.d1, B.gd1b);
     // d1b, d1a (input of d1a: cat1 = [up(bb) | e1b])
     k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gd1b, B.d1b, B.n1 * 32);
     SFB_TRY(wgrad_any(32, 32, B.d1a, B.gd1b, GW(n, D1B), GB(n, D1B), B.d1, s));
-    SFB_TRY(conv_any(32, 32, EPI_LINEAR_BF16, B.gd1b, WT(n, D1B), nullptr, B.gd1a, 32, 0, B.d1, s));
+    SFB_TRY(conv_any(32, 32, tc::LINEAR_BF16, B.gd1b, WT(n, D1B), nullptr, B.gd1a, 32, 0, B.d1, s, n->error));
     k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gd1a, B.d1a, B.n1 * 32);
     SFB_TRY(wgrad_any(96, 32, B.cat1, B.gd1a, GW(n, D1A), GB(n, D1A), B.d1, s));
-    SFB_TRY(conv_any(32, 96, EPI_LINEAR_BF16, B.gd1a, WT(n, D1A), nullptr, B.gcat1, 96, 0, B.d1, s));
+    SFB_TRY(conv_any(32, 96, tc::LINEAR_BF16, B.gd1a, WT(n, D1A), nullptr, B.gcat1, 96, 0, B.d1, s, n->error));
     k_upsample2_backward<<<blocks_for(B.n2 * 64), 256, 0, s>>>(B.gcat1, 96, 0, 64, B.d2, B.gbb);
     // bottleneck
     k_relu_backward<<<blocks_for(B.n2 * 64), 256, 0, s>>>(B.gbb, B.bb, B.n2 * 64);
     SFB_TRY(wgrad_any(64, 64, B.ba, B.gbb, GW(n, BB), GB(n, BB), B.d2, s));
-    SFB_TRY(conv_any(64, 64, EPI_LINEAR_BF16, B.gbb, WT(n, BB), nullptr, B.gba, 64, 0, B.d2, s));
+    SFB_TRY(conv_any(64, 64, tc::LINEAR_BF16, B.gbb, WT(n, BB), nullptr, B.gba, 64, 0, B.d2, s, n->error));
     k_relu_backward<<<blocks_for(B.n2 * 64), 256, 0, s>>>(B.gba, B.ba, B.n2 * 64);
     SFB_TRY(wgrad_any(32, 64, B.p1, B.gba, GW(n, BA), GB(n, BA), B.d2, s));
-    SFB_TRY(conv_any(64, 32, EPI_LINEAR_BF16, B.gba, WT(n, BA), nullptr, B.gp1, 32, 0, B.d2, s));
+    SFB_TRY(conv_any(64, 32, tc::LINEAR_BF16, B.gba, WT(n, BA), nullptr, B.gp1, 32, 0, B.d2, s, n->error));
     // e1b receives the skip (channels 64..95 of cat1) and the pooled path
     k_copy_channels<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gcat1, 96, 64, B.ge1b, 32, 0, 32, B.n1, 0);
     k_pool2_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gp1, 32, B.d2, B.ge1b, 32, 0, 1);
     k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.ge1b, B.e1b, B.n1 * 32);
     SFB_TRY(wgrad_any(32, 32, B.e1a, B.ge1b, GW(n, E1B), GB(n, E1B), B.d1, s));
-    SFB_TRY(conv_any(32, 32, EPI_LINEAR_BF16, B.ge1b, WT(n, E1B), nullptr, B.ge1a, 32, 0, B.d1, s));
+    SFB_TRY(conv_any(32, 32, tc::LINEAR_BF16, B.ge1b, WT(n, E1B), nullptr, B.ge1a, 32, 0, B.d1, s, n->error));
     k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.ge1a, B.e1a, B.n1 * 32);
     SFB_TRY(wgrad_any(16, 32, B.p0, B.ge1a, GW(n, E1A), GB(n, E1A), B.d1, s));
-    SFB_TRY(conv_any(32, 16, EPI_LINEAR_BF16, B.ge1a, WT(n, E1A), nullptr, B.gp0, 16, 0, B.d1, s));
+    SFB_TRY(conv_any(32, 16, tc::LINEAR_BF16, B.ge1a, WT(n, E1A), nullptr, B.gp0, 16, 0, B.d1, s, n->error));
     // e0b: skip (channels 32..47 of cat0) + pooled path
     k_copy_channels<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gcat0, 48, 32, B.ge0b, 16, 0, 16, B.n0, 0);
     k_pool2_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gp0, 16, B.d1, B.ge0b, 16, 0, 1);
     k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.ge0b, B.e0b, B.n0 * 16);
     SFB_TRY(wgrad_any(16, 16, B.e0a, B.ge0b, GW(n, E0B), GB(n, E0B), B.d0, s));
-    SFB_TRY(conv_any(16, 16, EPI_LINEAR_BF16, B.ge0b, WT(n, E0B), nullptr, B.ge0a, 16, 0, B.d0, s));
+    SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.ge0b, WT(n, E0B), nullptr, B.ge0a, 16, 0, B.d0, s, n->error));
     k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.ge0a, B.e0a, B.n0 * 16);
     SFB_TRY(wgrad_any(16, 16, B.in, B.ge0a, GW(n, E0A), GB(n, E0A), B.d0, s));
     return cudaGetLastError();

@@ -1,16 +1,14 @@
-// sf_unet_kernels.cuh -- kernels of the warm-start network: 3x3x3 convolution
-// as an implicit GEMM on the tensor cores (BF16 operands, FP32 accumulation),
-// its data and weight gradients, 2x average pooling, 2x nearest upsampling,
-// and the element-wise pieces of training.
+// sf_unet_kernels.cuh -- kernels of the warm-start network besides the
+// tcgen05 convolution (sf_unet_tc.cuh): the weight gradient of a 3x3x3
+// convolution (mma.sync BF16 x BF16 -> FP32), 2x average pooling, 2x nearest
+// upsampling, and the element-wise pieces of training.
 //
 // Activations are channels-last BF16: element (voxel v, channel c) at
 // v * C + c, v = x + nx (y + ny z), C a multiple of 16 (padded with zeros).
 // Weights are BF16 [tap][cout][cin] with tap = (dz+1)*9 + (dy+1)*3 + (dx+1),
 // plus an FP32 master copy for the optimizer. Zero padding at the grid edge.
 //
-// Tensor-core instruction: mma.sync m16n8k16 BF16 x BF16 -> FP32. A fragment
-// rows are 16 output voxels (one x row of the tile), its K columns 16 input
-// channels of one tap; B holds the weights of 8 output channels.
+// Weight-gradient GEMM instruction: mma.sync m16n8k16 BF16 x BF16 -> FP32.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -22,9 +20,6 @@
 
 namespace sfb::net {
 
-constexpr int kTileX = 16, kTileY = 4;  // output voxels per CTA (one m16 tile per warp, 4 warps)
-constexpr int kHaloX = kTileX + 2, kHaloY = kTileY + 2;
-
 __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1) {
     asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
                  : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
@@ -32,77 +27,6 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
 }
 
 __device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
-
-enum Epilogue : int { EPI_RELU_BF16 = 0, EPI_LINEAR_BF16 = 1, EPI_LINEAR_F32_CH0 = 2 };
-
-// out[v][co] = epi(bias[co] + sum_tap sum_ci w[tap][co][ci] in[v + off(tap)][ci])
-// CIN, COUT: channel counts (CIN % 16 == 0, COUT % 8 == 0). Grid:
-// (ceil(nx/16), ceil(ny/4), nz), 128 threads. out_ch: channel stride of the
-// output tensor (>= COUT; lets a layer write into a wider concatenated tensor
-// at channel offset out_off).
-template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(128) k_conv3d(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias, void* __restrict__ out, int out_ch, int out_off, Dims d) {
-    static_assert(CIN % 16 == 0 && COUT % 8 == 0, "channel padding");
-    constexpr int NT = COUT / 8;
-    extern __shared__ __align__(16) __nv_bfloat16 tile[];  // [3][kHaloY][kHaloX][CIN]
-    const int x0 = static_cast<int>(blockIdx.x) * kTileX, y0 = static_cast<int>(blockIdx.y) * kTileY, z = static_cast<int>(blockIdx.z);
-    const int tid = static_cast<int>(threadIdx.x), warp = tid >> 5, lane = tid & 31;
-    // input halo tile, 16-byte vectors, zeros outside the grid
-    constexpr int VEC = CIN / 8;
-    for (int i = tid; i < 3 * kHaloY * kHaloX * VEC; i += 128) {
-        const int c8 = i % VEC, hx = (i / VEC) % kHaloX, hy = (i / VEC / kHaloX) % kHaloY, hz = i / VEC / kHaloX / kHaloY;
-        const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z + hz - 1;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny) && static_cast<unsigned>(gz) < static_cast<unsigned>(d.nz))
-            v = *reinterpret_cast<const uint4*>(in + (static_cast<size_t>(gx) + static_cast<size_t>(d.nx) * (gy + static_cast<size_t>(d.ny) * gz)) * CIN + c8 * 8);
-        *reinterpret_cast<uint4*>(tile + ((hz * kHaloY + hy) * kHaloX + hx) * CIN + c8 * 8) = v;
-    }
-    __syncthreads();
-    const int g = lane >> 2, t = lane & 3;
-    float acc[NT][4];
-#pragma unroll
-    for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
-    for (int tap = 0; tap < 27; ++tap) {
-        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-        const __nv_bfloat16* arow = tile + ((dz * kHaloY + warp + dy) * kHaloX + dx) * CIN;  // voxel x = 0 of this warp's row, shifted by the tap
-        const __nv_bfloat16* wt = w + static_cast<size_t>(tap) * COUT * CIN;
-#pragma unroll
-        for (int kc = 0; kc < CIN / 16; ++kc) {
-            const int k0 = kc * 16 + 2 * t;
-            const uint32_t a0 = ld32(arow + g * CIN + k0), a1 = ld32(arow + (g + 8) * CIN + k0);
-            const uint32_t a2 = ld32(arow + g * CIN + k0 + 8), a3 = ld32(arow + (g + 8) * CIN + k0 + 8);
-#pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                const __nv_bfloat16* wb = wt + (n * 8 + g) * CIN + k0;
-                mma_bf16(acc[n], a0, a1, a2, a3, __ldg(reinterpret_cast<const unsigned int*>(wb)), __ldg(reinterpret_cast<const unsigned int*>(wb + 8)));
-            }
-        }
-    }
-    // epilogue: rows g and g + 8 of the warp's 16 voxels, columns 2t, 2t + 1 of each n tile
-    const int gy = y0 + warp;
-    if (gy >= d.ny) return;
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        const int gx = x0 + g + 8 * half;
-        if (gx >= d.nx) continue;
-        const size_t v = static_cast<size_t>(gx) + static_cast<size_t>(d.nx) * (gy + static_cast<size_t>(d.ny) * z);
-#pragma unroll
-        for (int n = 0; n < NT; ++n) {
-            const int co = n * 8 + 2 * t;
-            float r0 = acc[n][2 * half] + (bias ? bias[co] : 0.0f);
-            float r1 = acc[n][2 * half + 1] + (bias ? bias[co + 1] : 0.0f);
-            if constexpr (EPI == EPI_RELU_BF16) {
-                r0 = fmaxf(r0, 0.0f);
-                r1 = fmaxf(r1, 0.0f);
-            }
-            if constexpr (EPI == EPI_LINEAR_F32_CH0) {
-                if (co == 0) static_cast<float*>(out)[v] = r0;
-            } else {
-                *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(out) + v * out_ch + out_off + co) = __floats2bfloat162_rn(r0, r1);
-            }
-        }
-    }
-}
 
 // Weight gradient: dw[tap][co][ci] += sum_v dout[v][co] in[v + off(tap)][ci],
 // dbias[co] += sum_v dout[v][co]. GEMM per tap with M = COUT, N = CIN,
@@ -174,8 +98,6 @@ __global__ void __launch_bounds__(128) k_conv3d_wgrad(const __nv_bfloat16* __res
     if (tap == 13 && tid < COUT && dbias) atomicAdd(dbias + tid, bsum);
 }
 
-template <int CIN>
-constexpr size_t conv_smem_bytes() { return static_cast<size_t>(3) * kHaloY * kHaloX * CIN * sizeof(__nv_bfloat16); }
 
 // ------------------------------------------------------ element-wise pieces --
 

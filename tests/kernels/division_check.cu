@@ -1,0 +1,46 @@
+// Exhaustive check, on the GPU, of the correctly rounded divisions the
+// stencil kernels use (tb::update_div in sf_stencil_tb.cuh) against IEEE
+// FP32 division (__fdiv_rn): every finite FP32 numerator for the pressure
+// divisor 6, and every 61st numerator for a few diffusion divisors 1 + 6a.
+// Prints "<divisor> <checked> <mismatches>" per divisor; exit status 1 on a
+// mismatch.
+#include <cstdio>
+
+#include "sf_stencil_tb.cuh"
+
+using namespace sfb;
+
+template <int KIND>
+__global__ void k_check(float divisor, unsigned long long stride, unsigned long long* counts) {
+    const float recip = 1.0f / divisor;
+    unsigned long long checked = 0, bad = 0;
+    for (unsigned long long u = (blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x) * stride; u < 0x100000000ull;
+         u += static_cast<unsigned long long>(gridDim.x) * blockDim.x * stride) {
+        const float n = __uint_as_float(static_cast<unsigned>(u));
+        if (!isfinite(n)) continue;
+        const float want = __fdiv_rn(n, divisor);
+        const float got = tb::update_div<KIND>(n, divisor, recip);
+        bad += __float_as_uint(want) != __float_as_uint(got);
+        ++checked;
+    }
+    atomicAdd(&counts[0], checked);
+    atomicAdd(&counts[1], bad);
+}
+
+int main() {
+    unsigned long long* counts = nullptr;
+    if (cudaMallocManaged(&counts, 2 * sizeof(unsigned long long)) != cudaSuccess) return 2;
+    const float diffusion[] = {1.0f + 6.0f * 1e-4f, 1.0f + 6.0f * 0.01f, 1.0f + 6.0f * 0.37f, 7.3f};
+    int failed = 0;
+    for (int k = 0; k < 5; ++k) {
+        counts[0] = counts[1] = 0;
+        const float d = k == 0 ? 6.0f : diffusion[k - 1];
+        if (k == 0) k_check<KIND_PRESSURE><<<148 * 8, 256>>>(d, 1, counts);
+        else k_check<KIND_SCALAR><<<148 * 8, 256>>>(d, 61, counts);
+        if (cudaDeviceSynchronize() != cudaSuccess) return 2;
+        std::printf("%.9g %llu %llu\n", d, counts[0], counts[1]);
+        failed |= counts[1] != 0;
+    }
+    cudaFree(counts);
+    return failed;
+}
