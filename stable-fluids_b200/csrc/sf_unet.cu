@@ -337,18 +337,18 @@ cudaError_t forward(Net* n, const float* b, float b_factor, const float* p_prev,
     SFB_TRY(cudaGetLastError());
     SFB_TRY(conv_any(16, 16, tc::RELU_BF16, B.in, W(n, E0A), Bias(n, E0A), B.e0a, 16, 0, B.d0, s, n->error));
     SFB_TRY(conv_any(16, 16, tc::RELU_BF16, B.e0a, W(n, E0B), Bias(n, E0B), B.e0b, 16, 0, B.d0, s, n->error));
-    k_pool2<<<blocks_for(B.n1 * 16), 256, 0, s>>>(B.e0b, 16, 0, B.p0, 16, B.d1);
+    k_pool2<<<row_grid(B.d1.nx, 2, B.d1.ny, B.d1.nz), 256, 0, s>>>(B.e0b, 16, 0, B.p0, 16, B.d1);
     SFB_TRY(conv_any(16, 32, tc::RELU_BF16, B.p0, W(n, E1A), Bias(n, E1A), B.e1a, 32, 0, B.d1, s, n->error));
     SFB_TRY(conv_any(32, 32, tc::RELU_BF16, B.e1a, W(n, E1B), Bias(n, E1B), B.e1b, 32, 0, B.d1, s, n->error));
-    k_pool2<<<blocks_for(B.n2 * 32), 256, 0, s>>>(B.e1b, 32, 0, B.p1, 32, B.d2);
+    k_pool2<<<row_grid(B.d2.nx, 4, B.d2.ny, B.d2.nz), 256, 0, s>>>(B.e1b, 32, 0, B.p1, 32, B.d2);
     SFB_TRY(conv_any(32, 64, tc::RELU_BF16, B.p1, W(n, BA), Bias(n, BA), B.ba, 64, 0, B.d2, s, n->error));
     SFB_TRY(conv_any(64, 64, tc::RELU_BF16, B.ba, W(n, BB), Bias(n, BB), B.bb, 64, 0, B.d2, s, n->error));
-    k_upsample2<<<blocks_for(B.n1 * 64), 256, 0, s>>>(B.bb, 64, B.d2, B.cat1, 96, 0);
-    k_copy_channels<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.e1b, 32, 0, B.cat1, 96, 64, 32, B.n1, 0);
+    k_upsample2<<<row_grid(B.d1.nx, 8, B.d1.ny, B.d1.nz), 256, 0, s>>>(B.bb, 64, B.d2, B.cat1, 96, 0);
+    k_copy_channels<<<blocks_for(B.n1 * 4), 256, 0, s>>>(B.e1b, 32, 0, B.cat1, 96, 64, 32, B.n1, 0);
     SFB_TRY(conv_any(96, 32, tc::RELU_BF16, B.cat1, W(n, D1A), Bias(n, D1A), B.d1a, 32, 0, B.d1, s, n->error));
     SFB_TRY(conv_any(32, 32, tc::RELU_BF16, B.d1a, W(n, D1B), Bias(n, D1B), B.d1b, 32, 0, B.d1, s, n->error));
-    k_upsample2<<<blocks_for(B.n0 * 32), 256, 0, s>>>(B.d1b, 32, B.d1, B.cat0, 48, 0);
-    k_copy_channels<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.e0b, 16, 0, B.cat0, 48, 32, 16, B.n0, 0);
+    k_upsample2<<<row_grid(B.d0.nx, 4, B.d0.ny, B.d0.nz), 256, 0, s>>>(B.d1b, 32, B.d1, B.cat0, 48, 0);
+    k_copy_channels<<<blocks_for(B.n0 * 2), 256, 0, s>>>(B.e0b, 16, 0, B.cat0, 48, 32, 16, B.n0, 0);
     SFB_TRY(conv_any(48, 16, tc::RELU_BF16, B.cat0, W(n, D0A), Bias(n, D0A), B.d0a, 16, 0, B.d0, s, n->error));
     SFB_TRY(conv_any(16, 16, tc::RELU_BF16, B.d0a, W(n, D0B), Bias(n, D0B), B.d0b, 16, 0, B.d0, s, n->error));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_F32_CH0, B.d0b, W(n, OUT), Bias(n, OUT), B.out, 1, 0, B.d0, s, n->error));
@@ -367,44 +367,44 @@ cudaError_t backward(Net* n, cudaStream_t s) {
     SFB_TRY(wgrad_any(16, 16, B.d0b, B.g16, GW(n, OUT), GB(n, OUT), B.d0, s));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.g16, WT(n, OUT), nullptr, B.gd0b, 16, 0, B.d0, s, n->error));
     // d0b, d0a (input of d0a: cat0 = [up(d1b) | e0b])
-    k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gd0b, B.d0b, B.n0 * 16);
+    k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.gd0b, B.d0b, B.n0 * 16);
     SFB_TRY(wgrad_any(16, 16, B.d0a, B.gd0b, GW(n, D0B), GB(n, D0B), B.d0, s));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.gd0b, WT(n, D0B), nullptr, B.gd0a, 16, 0, B.d0, s, n->error));
-    k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gd0a, B.d0a, B.n0 * 16);
+    k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.gd0a, B.d0a, B.n0 * 16);
     SFB_TRY(wgrad_any(48, 16, B.cat0, B.gd0a, GW(n, D0A), GB(n, D0A), B.d0, s));
     SFB_TRY(conv_any(16, 48, tc::LINEAR_BF16, B.gd0a, WT(n, D0A), nullptr, B.gcat0, 48, 0, B.d0, s, n->error));
-    k_upsample2_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gcat0, 48, 0, 32, B.d1, B.gd1b);
+    k_upsample2_backward<<<row_grid(B.d1.nx, 4, B.d1.ny, B.d1.nz), 256, 0, s>>>(B.gcat0, 48, 0, 32, B.d1, B.gd1b);
     // d1b, d1a (input of d1a: cat1 = [up(bb) | e1b])
-    k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gd1b, B.d1b, B.n1 * 32);
+    k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.gd1b, B.d1b, B.n1 * 32);
     SFB_TRY(wgrad_any(32, 32, B.d1a, B.gd1b, GW(n, D1B), GB(n, D1B), B.d1, s));
     SFB_TRY(conv_any(32, 32, tc::LINEAR_BF16, B.gd1b, WT(n, D1B), nullptr, B.gd1a, 32, 0, B.d1, s, n->error));
-    k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gd1a, B.d1a, B.n1 * 32);
+    k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.gd1a, B.d1a, B.n1 * 32);
     SFB_TRY(wgrad_any(96, 32, B.cat1, B.gd1a, GW(n, D1A), GB(n, D1A), B.d1, s));
     SFB_TRY(conv_any(32, 96, tc::LINEAR_BF16, B.gd1a, WT(n, D1A), nullptr, B.gcat1, 96, 0, B.d1, s, n->error));
-    k_upsample2_backward<<<blocks_for(B.n2 * 64), 256, 0, s>>>(B.gcat1, 96, 0, 64, B.d2, B.gbb);
+    k_upsample2_backward<<<row_grid(B.d2.nx, 8, B.d2.ny, B.d2.nz), 256, 0, s>>>(B.gcat1, 96, 0, 64, B.d2, B.gbb);
     // bottleneck
-    k_relu_backward<<<blocks_for(B.n2 * 64), 256, 0, s>>>(B.gbb, B.bb, B.n2 * 64);
+    k_relu_backward<<<blocks_for(B.n2 * 64 / 8), 256, 0, s>>>(B.gbb, B.bb, B.n2 * 64);
     SFB_TRY(wgrad_any(64, 64, B.ba, B.gbb, GW(n, BB), GB(n, BB), B.d2, s));
     SFB_TRY(conv_any(64, 64, tc::LINEAR_BF16, B.gbb, WT(n, BB), nullptr, B.gba, 64, 0, B.d2, s, n->error));
-    k_relu_backward<<<blocks_for(B.n2 * 64), 256, 0, s>>>(B.gba, B.ba, B.n2 * 64);
+    k_relu_backward<<<blocks_for(B.n2 * 64 / 8), 256, 0, s>>>(B.gba, B.ba, B.n2 * 64);
     SFB_TRY(wgrad_any(32, 64, B.p1, B.gba, GW(n, BA), GB(n, BA), B.d2, s));
     SFB_TRY(conv_any(64, 32, tc::LINEAR_BF16, B.gba, WT(n, BA), nullptr, B.gp1, 32, 0, B.d2, s, n->error));
     // e1b receives the skip (channels 64..95 of cat1) and the pooled path
-    k_copy_channels<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gcat1, 96, 64, B.ge1b, 32, 0, 32, B.n1, 0);
-    k_pool2_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.gp1, 32, B.d2, B.ge1b, 32, 0, 1);
-    k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.ge1b, B.e1b, B.n1 * 32);
+    k_copy_channels<<<blocks_for(B.n1 * 4), 256, 0, s>>>(B.gcat1, 96, 64, B.ge1b, 32, 0, 32, B.n1, 0);
+    k_pool2_backward<<<row_grid(B.d1.nx, 4, B.d1.ny, B.d1.nz), 256, 0, s>>>(B.gp1, 32, B.d2, B.ge1b, 32, 0, 1);
+    k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.ge1b, B.e1b, B.n1 * 32);
     SFB_TRY(wgrad_any(32, 32, B.e1a, B.ge1b, GW(n, E1B), GB(n, E1B), B.d1, s));
     SFB_TRY(conv_any(32, 32, tc::LINEAR_BF16, B.ge1b, WT(n, E1B), nullptr, B.ge1a, 32, 0, B.d1, s, n->error));
-    k_relu_backward<<<blocks_for(B.n1 * 32), 256, 0, s>>>(B.ge1a, B.e1a, B.n1 * 32);
+    k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.ge1a, B.e1a, B.n1 * 32);
     SFB_TRY(wgrad_any(16, 32, B.p0, B.ge1a, GW(n, E1A), GB(n, E1A), B.d1, s));
     SFB_TRY(conv_any(32, 16, tc::LINEAR_BF16, B.ge1a, WT(n, E1A), nullptr, B.gp0, 16, 0, B.d1, s, n->error));
     // e0b: skip (channels 32..47 of cat0) + pooled path
-    k_copy_channels<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gcat0, 48, 32, B.ge0b, 16, 0, 16, B.n0, 0);
-    k_pool2_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.gp0, 16, B.d1, B.ge0b, 16, 0, 1);
-    k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.ge0b, B.e0b, B.n0 * 16);
+    k_copy_channels<<<blocks_for(B.n0 * 2), 256, 0, s>>>(B.gcat0, 48, 32, B.ge0b, 16, 0, 16, B.n0, 0);
+    k_pool2_backward<<<row_grid(B.d0.nx, 2, B.d0.ny, B.d0.nz), 256, 0, s>>>(B.gp0, 16, B.d1, B.ge0b, 16, 0, 1);
+    k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.ge0b, B.e0b, B.n0 * 16);
     SFB_TRY(wgrad_any(16, 16, B.e0a, B.ge0b, GW(n, E0B), GB(n, E0B), B.d0, s));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.ge0b, WT(n, E0B), nullptr, B.ge0a, 16, 0, B.d0, s, n->error));
-    k_relu_backward<<<blocks_for(B.n0 * 16), 256, 0, s>>>(B.ge0a, B.e0a, B.n0 * 16);
+    k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.ge0a, B.e0a, B.n0 * 16);
     SFB_TRY(wgrad_any(16, 16, B.in, B.ge0a, GW(n, E0A), GB(n, E0A), B.d0, s));
     return cudaGetLastError();
 }

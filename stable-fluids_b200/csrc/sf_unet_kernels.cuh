@@ -142,89 +142,138 @@ __global__ void k_unpack_output(const float* __restrict__ delta, const float* p_
     for (size_t v = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; v < n; v += static_cast<size_t>(gridDim.x) * blockDim.x) p0[v] = (p_prev ? p_prev[v] : 0.0f) + delta[v] * inv;
 }
 
-// 2x2x2 average pooling (even dims of the fine grid); channel stride in_ch.
-__global__ void k_pool2(const __nv_bfloat16* __restrict__ in, int in_ch, int in_off, __nv_bfloat16* __restrict__ out, int C, Dims coarse) {
-    const size_t n = static_cast<size_t>(coarse.nx) * coarse.ny * coarse.nz * C;
-    const int fnx = coarse.nx * 2, fny = coarse.ny * 2;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const size_t v = i / C;
-        const int x = static_cast<int>(v % coarse.nx), y = static_cast<int>((v / coarse.nx) % coarse.ny), z = static_cast<int>(v / coarse.nx / coarse.ny);
-        float s = 0.0f;
-        for (int k = 0; k < 8; ++k) {
-            const size_t fv = static_cast<size_t>(2 * x + (k & 1)) + static_cast<size_t>(fnx) * (2 * y + ((k >> 1) & 1) + static_cast<size_t>(fny) * (2 * z + (k >> 2)));
-            s += __bfloat162float(in[fv * in_ch + in_off + c]);
-        }
-        out[i] = __float2bfloat16(0.125f * s);
+// The pooling / upsampling / copy kernels below move 8 channels (16 bytes)
+// per thread; channel counts, strides and offsets are multiples of 8. The
+// 2-D launches give blockIdx.y = y and blockIdx.z = z of the output grid and
+// threads over (x, 8-channel chunk) of one row.
+struct Bf8 {
+    float v[8];
+};
+__device__ __forceinline__ Bf8 load8(const __nv_bfloat16* p) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+    Bf8 r;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 f = __bfloat1622float2(h[k]);
+        r.v[2 * k] = f.x;
+        r.v[2 * k + 1] = f.y;
     }
+    return r;
+}
+__device__ __forceinline__ void store8(__nv_bfloat16* p, const Bf8& r) {
+    uint4 u;
+    __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) h[k] = __floats2bfloat162_rn(r.v[2 * k], r.v[2 * k + 1]);
+    *reinterpret_cast<uint4*>(p) = u;
+}
+
+inline dim3 row_grid(int nx, int chunks_per_voxel, int ny, int nz) { return dim3(static_cast<unsigned>((nx * chunks_per_voxel + 255) / 256), static_cast<unsigned>(ny), static_cast<unsigned>(nz)); }
+
+// 2x2x2 average pooling (even dims of the fine grid); channel stride in_ch.
+// Launch: row_grid(coarse.nx, C / 8, coarse.ny, coarse.nz), 256 threads.
+__global__ void k_pool2(const __nv_bfloat16* __restrict__ in, int in_ch, int in_off, __nv_bfloat16* __restrict__ out, int C, Dims coarse) {
+    const int c8n = C / 8;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= coarse.nx * c8n) return;
+    const int x = i / c8n, c = (i % c8n) * 8, y = static_cast<int>(blockIdx.y), z = static_cast<int>(blockIdx.z);
+    const int fnx = coarse.nx * 2, fny = coarse.ny * 2;
+    Bf8 s{};
+    for (int k = 0; k < 8; ++k) {
+        const size_t fv = static_cast<size_t>(2 * x + (k & 1)) + static_cast<size_t>(fnx) * (2 * y + ((k >> 1) & 1) + static_cast<size_t>(fny) * (2 * z + (k >> 2)));
+        const Bf8 a = load8(in + fv * in_ch + in_off + c);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s.v[j] += a.v[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s.v[j] *= 0.125f;
+    const size_t v = static_cast<size_t>(x) + static_cast<size_t>(coarse.nx) * (y + static_cast<size_t>(coarse.ny) * z);
+    store8(out + v * C + c, s);
 }
 
 // Backward of the pooling: each fine voxel gets 1/8 of its parent's gradient,
 // added to (accumulate) or written into the fine gradient tensor.
+// Launch: row_grid(fine nx, C / 8, fine ny, fine nz).
 __global__ void k_pool2_backward(const __nv_bfloat16* __restrict__ gcoarse, int C, Dims coarse, __nv_bfloat16* __restrict__ gfine, int fine_ch, int fine_off, int accumulate) {
-    const int fnx = coarse.nx * 2, fny = coarse.ny * 2, fnz = coarse.nz * 2;
-    const size_t n = static_cast<size_t>(fnx) * fny * fnz * C;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const size_t fv = i / C;
-        const int x = static_cast<int>(fv % fnx), y = static_cast<int>((fv / fnx) % fny), z = static_cast<int>(fv / fnx / fny);
-        const size_t cv = static_cast<size_t>(x / 2) + static_cast<size_t>(coarse.nx) * (y / 2 + static_cast<size_t>(coarse.ny) * (z / 2));
-        float gval = 0.125f * __bfloat162float(gcoarse[cv * C + c]);
-        __nv_bfloat16* dst = gfine + fv * fine_ch + fine_off + c;
-        if (accumulate) gval += __bfloat162float(*dst);
-        *dst = __float2bfloat16(gval);
+    const int c8n = C / 8, fnx = coarse.nx * 2, fny = coarse.ny * 2;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= fnx * c8n) return;
+    const int x = i / c8n, c = (i % c8n) * 8, y = static_cast<int>(blockIdx.y), z = static_cast<int>(blockIdx.z);
+    const size_t cv = static_cast<size_t>(x / 2) + static_cast<size_t>(coarse.nx) * (y / 2 + static_cast<size_t>(coarse.ny) * (z / 2));
+    Bf8 g = load8(gcoarse + cv * C + c);
+    __nv_bfloat16* dst = gfine + (static_cast<size_t>(x) + static_cast<size_t>(fnx) * (y + static_cast<size_t>(fny) * z)) * fine_ch + fine_off + c;
+    const Bf8 old = accumulate ? load8(dst) : Bf8{};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        g.v[j] = 0.125f * g.v[j];
+        if (accumulate) g.v[j] += old.v[j];
     }
+    store8(dst, g);
 }
 
 // Nearest 2x upsampling of a coarse tensor into channels [out_off, out_off+C)
-// of a fine tensor with channel stride out_ch.
+// of a fine tensor with channel stride out_ch. Launch: row_grid(fine nx, C / 8,
+// fine ny, fine nz).
 __global__ void k_upsample2(const __nv_bfloat16* __restrict__ in, int C, Dims coarse, __nv_bfloat16* __restrict__ out, int out_ch, int out_off) {
-    const int fnx = coarse.nx * 2, fny = coarse.ny * 2, fnz = coarse.nz * 2;
-    const size_t n = static_cast<size_t>(fnx) * fny * fnz * C;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const size_t fv = i / C;
-        const int x = static_cast<int>(fv % fnx), y = static_cast<int>((fv / fnx) % fny), z = static_cast<int>(fv / fnx / fny);
-        const size_t cv = static_cast<size_t>(x / 2) + static_cast<size_t>(coarse.nx) * (y / 2 + static_cast<size_t>(coarse.ny) * (z / 2));
-        out[fv * out_ch + out_off + c] = in[cv * C + c];
-    }
+    const int c8n = C / 8, fnx = coarse.nx * 2, fny = coarse.ny * 2;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= fnx * c8n) return;
+    const int x = i / c8n, c = (i % c8n) * 8, y = static_cast<int>(blockIdx.y), z = static_cast<int>(blockIdx.z);
+    const size_t cv = static_cast<size_t>(x / 2) + static_cast<size_t>(coarse.nx) * (y / 2 + static_cast<size_t>(coarse.ny) * (z / 2));
+    const size_t fv = static_cast<size_t>(x) + static_cast<size_t>(fnx) * (y + static_cast<size_t>(fny) * z);
+    *reinterpret_cast<uint4*>(out + fv * out_ch + out_off + c) = *reinterpret_cast<const uint4*>(in + cv * C + c);
 }
 
 // Backward of the upsampling: the coarse gradient is the sum over its 8
-// children of channels [off, off + C) of the fine gradient.
+// children of channels [off, off + C) of the fine gradient. Launch:
+// row_grid(coarse.nx, C / 8, coarse.ny, coarse.nz).
 __global__ void k_upsample2_backward(const __nv_bfloat16* __restrict__ gfine, int fine_ch, int off, int C, Dims coarse, __nv_bfloat16* __restrict__ gcoarse) {
-    const size_t n = static_cast<size_t>(coarse.nx) * coarse.ny * coarse.nz * C;
-    const int fnx = coarse.nx * 2, fny = coarse.ny * 2;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const size_t v = i / C;
-        const int x = static_cast<int>(v % coarse.nx), y = static_cast<int>((v / coarse.nx) % coarse.ny), z = static_cast<int>(v / coarse.nx / coarse.ny);
-        float s = 0.0f;
-        for (int k = 0; k < 8; ++k) {
-            const size_t fv = static_cast<size_t>(2 * x + (k & 1)) + static_cast<size_t>(fnx) * (2 * y + ((k >> 1) & 1) + static_cast<size_t>(fny) * (2 * z + (k >> 2)));
-            s += __bfloat162float(gfine[fv * fine_ch + off + c]);
-        }
-        gcoarse[i] = __float2bfloat16(s);
+    const int c8n = C / 8, fnx = coarse.nx * 2, fny = coarse.ny * 2;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= coarse.nx * c8n) return;
+    const int x = i / c8n, c = (i % c8n) * 8, y = static_cast<int>(blockIdx.y), z = static_cast<int>(blockIdx.z);
+    Bf8 s{};
+    for (int k = 0; k < 8; ++k) {
+        const size_t fv = static_cast<size_t>(2 * x + (k & 1)) + static_cast<size_t>(fnx) * (2 * y + ((k >> 1) & 1) + static_cast<size_t>(fny) * (2 * z + (k >> 2)));
+        const Bf8 a = load8(gfine + fv * fine_ch + off + c);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s.v[j] += a.v[j];
     }
+    const size_t v = static_cast<size_t>(x) + static_cast<size_t>(coarse.nx) * (y + static_cast<size_t>(coarse.ny) * z);
+    store8(gcoarse + v * C + c, s);
 }
 
-// Copies channels [src_off, src_off + C) of src into [dst_off, ...) of dst.
+// Copies channels [src_off, src_off + C) of src into [dst_off, ...) of dst
+// (adding to dst when accumulate), 8 channels per thread.
 __global__ void k_copy_channels(const __nv_bfloat16* __restrict__ src, int src_ch, int src_off, __nv_bfloat16* __restrict__ dst, int dst_ch, int dst_off, int C, size_t voxels, int accumulate) {
-    const size_t n = voxels * C;
+    const size_t c8n = static_cast<size_t>(C / 8), n = voxels * c8n;
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const size_t v = i / C;
-        float val = __bfloat162float(src[v * src_ch + src_off + c]);
+        const size_t v = i / c8n, c = (i % c8n) * 8;
         __nv_bfloat16* d = dst + v * dst_ch + dst_off + c;
-        if (accumulate) val += __bfloat162float(*d);
-        *d = __float2bfloat16(val);
+        if (accumulate) {
+            Bf8 a = load8(src + v * src_ch + src_off + c);
+            const Bf8 b = load8(d);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) a.v[j] += b.v[j];
+            store8(d, a);
+        } else {
+            *reinterpret_cast<uint4*>(d) = *reinterpret_cast<const uint4*>(src + v * src_ch + src_off + c);
+        }
     }
 }
 
-// g *= (act > 0): the gradient through a ReLU whose output is act.
+// g *= (act > 0): the gradient through a ReLU whose output is act; n is a
+// multiple of 8.
 __global__ void k_relu_backward(__nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ act, size_t n) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x)
-        if (!(__bfloat162float(act[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n / 8; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const Bf8 a = load8(act + 8 * i);
+        Bf8 v = load8(g + 8 * i);
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (!(a.v[j] > 0.0f)) v.v[j] = 0.0f;
+        store8(g + 8 * i, v);
+    }
 }
 
 // Mean squared error of the FP32 output against the target; writes the
