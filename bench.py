@@ -88,6 +88,8 @@ def parse():
     p.add_argument("--fixed-steps", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
+    p.add_argument("--fixed-pressure-iterations", type=int, default=0,
+                   help="profiling: run the variants with this fixed sweep count instead of the residual-driven solve (ncu cannot see kernels inside conditional graph nodes)")
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -183,6 +185,7 @@ def solver_options(sf, variant, tol, cap, trial):
     o = sf.default_options()
     o.scheme = sf.SCHEME_RBGS if variant == "rbgs" else sf.SCHEME_JACOBI
     o.warm_start = {"learned": sf.WARM_START_LEARNED, "plain": sf.WARM_START_ZERO, "previous": sf.WARM_START_PREVIOUS, "rbgs": sf.WARM_START_ZERO}[variant]
+    o.compute_residual = 1
     o.residual_tolerance = tol
     o.residual_check_interval = CHECK_INTERVAL
     o.max_pressure_iterations = cap
@@ -204,8 +207,12 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
     simulation stream, summed); per-step iterations and residuals."""
     import torch
 
-    opts = solver_options(sf, variant, args.tolerance, args.cap, args.trial)
-    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=device)
+    opts = solver_options(sf, variant, 0.0 if args.fixed_pressure_iterations else args.tolerance, args.cap, args.trial)
+    config = scene.config
+    if args.fixed_pressure_iterations:
+        config = type(scene.config).from_buffer_copy(scene.config)
+        config.pressure_iterations = args.fixed_pressure_iterations
+    sim = sf.Simulation(config, scene.scalars, scene.vectors, options=opts, device=device)
     if variant == "learned":
         net.attach(sim)
     sf.scenes.apply_inputs(sim, scene, 0)
@@ -228,7 +235,10 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
     t = sum(a.elapsed_time(b) for a, b in events) / 1000.0
     t = max_over_ranks(t, world)
     trial_done = args.trial if variant == "learned" else 0
-    launches = sum(launches_per_step(info.kernels_per_step, i, trial_done, variant == "rbgs") for i in its)
+    if args.fixed_pressure_iterations:
+        launches = info.kernels_per_step * args.steps
+    else:
+        launches = sum(launches_per_step(info.kernels_per_step, i, trial_done, variant == "rbgs") for i in its)
     out = {"steps_per_s": world * args.steps / t, "ms_per_step": 1000.0 * t / args.steps, "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > args.tolerance for r in res), "gpu_launches": launches}
     if variant == "learned":
         out["used_fallback"] = fallback
@@ -248,7 +258,7 @@ def train_network(sf, args, device):
     t_pairs = time.perf_counter() - t0
     net = sf.WarmStartNetwork(seed=0, device=device)
     h = float(sf.scenes.training_scene(0, n=args.train_size).config.cell_size)
-    history = sf.warmstart.train(net, pairs, h, epochs=args.train_epochs, learning_rate=args.learning_rate, deadline=time.perf_counter() + args.train_seconds)
+    history = sf.warmstart.train(net, pairs, h, epochs=args.train_epochs, learning_rate=args.learning_rate, deadline=time.perf_counter() + args.train_seconds) if pairs else []
     info = {"pairs": len(pairs), "grid": [args.train_size] * 3, "target_sweeps": args.train_sweeps, "epochs_run": len(history), "loss_per_epoch": history,
             "pair_generation_s": t_pairs, "training_s": time.perf_counter() - t0 - t_pairs}
     del pairs
@@ -454,9 +464,8 @@ def main():
         return
 
     variants = [v for v in args.variants.split(",") if v]
-    if "learned" not in variants:
-        variants.insert(0, "learned")
-    net, train_info = train_network(sf, args, local)
+    headline = "learned" if "learned" in variants else variants[0]  # profiling runs may leave the network out
+    net, train_info = train_network(sf, args, local) if "learned" in variants else (None, None)
 
     results, sims = {}, {}
     with Clocks(local, not args.no_clocks and rank == 0) as clk:
@@ -467,7 +476,7 @@ def main():
                 sims[v] = sim
             else:
                 sim.close()
-    learned = results["learned"]
+    learned = results[headline]
     value = learned["steps_per_s"]
 
     # roofline: the Jacobi sweep dominates every variant's step
@@ -485,21 +494,25 @@ def main():
     achieved = bytes_per_sweep / sweep_s / 1e9
     roofline = {"bound": "hbm", "kernel": "k_jacobi_vec (Jacobi pressure sweep)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": None, "bytes_per_launch": bytes_per_sweep, "launch_us": sweep_s * 1e6, "unit_of_work": "one Jacobi sweep of 256^3 cells: read p + rhs, write p = 12 B/cell"}
-    net_s = time_network(net, n, torch.device("cuda", local))
-    flops = network_flops(n)
-    roofline_network = {"bound": "tensor", "kernel": "warm-start network prediction (all layers)", "achieved": flops / net_s / 1e12, "peak": tc_peak, "peak_source": peak_src, "unit": "TFLOP/s",
-                        "frac": flops / net_s / 1e12 / tc_peak, "flop_per_launch": flops, "launch_ms": net_s * 1e3, "unit_of_work": "one prediction at 256^3, real channels only"}
+    roofline_network = None
+    if net is not None:
+        net_s = time_network(net, n, torch.device("cuda", local))
+        flops = network_flops(n)
+        roofline_network = {"bound": "tensor", "kernel": "warm-start network prediction (all layers)", "achieved": flops / net_s / 1e12, "peak": tc_peak, "peak_source": peak_src, "unit": "TFLOP/s",
+                            "frac": flops / net_s / 1e12 / tc_peak, "flop_per_launch": flops, "launch_ms": net_s * 1e3, "unit_of_work": f"one prediction at {n}^3, real channels only"}
 
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and "learned" in sims:
         te, h2d, d2h = e2e_run(sf, sims["learned"], scene, args.e2e_steps)
         te = max_over_ranks(te, world)
         e2e = {"value": world * args.e2e_steps / te, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps}
-    sims["learned"].close()
-    fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world)
+    for sim in sims.values():
+        sim.close()
+    fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
 
     config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
-              "grid": [n, n, n], "solver": "Jacobi sweeps from the learned warm start", "l2": "working set > L2 (no flush needed)",
+              "grid": [n, n, n], "solver": {"learned": "Jacobi sweeps from the learned warm start", "plain": "Jacobi sweeps from zero", "previous": "Jacobi sweeps from the previous pressure", "rbgs": "red-black Gauss-Seidel from zero"}[headline]
+            + (f", {args.fixed_pressure_iterations} sweeps per step (profiling)" if args.fixed_pressure_iterations else ""), "l2": "working set > L2 (no flush needed)",
               "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
@@ -509,9 +522,10 @@ def main():
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and "plain" in results:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and "plain" in results and not args.fixed_pressure_iterations:
         line["cpu_baseline"] = cpu_baseline(sf, scene, statistics.mean(results["plain"]["pressure_iterations"]))
-    net.close()
+    if net is not None:
+        net.close()
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -291,6 +291,136 @@ bool vec_ok(const StencilArgs& a) {
     return a.dims.nx % 4 == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
 }
 
+// Two Jacobi sweeps per pass (temporal blocking): a CTA owns a TX x TY
+// column of the grid over a z chunk and marches up it. Per plane step it
+// stages the input plane q + 1 (tile + 2-cell halo) and the right-hand side
+// (tile + 1-cell halo) in shared memory, computes the first sweep on plane q
+// over the tile + 1-cell halo into a 3-plane ring, and the second sweep on
+// plane q - 1 over the tile from that ring, writing only the result of both
+// sweeps to HBM: 12 bytes per cell per two sweeps. The halo ring of the first
+// sweep is recomputed by neighbouring CTAs. Face ghosts are applied inline
+// from the kind's GhostRule (periodic axes read wrapped coordinates), and
+// the per-cell arithmetic is k_jacobi_vec's, so two sweeps here are
+// bit-identical to two single sweeps. The next plane's loads are issued into
+// registers before the current plane is computed.
+constexpr int kTbX = 32, kTbY = 32, kTbThreads = 256;
+constexpr int kTb0W = kTbX + 4, kTb0H = kTbY + 4;  // sweep-1 input tile
+constexpr int kTb1W = kTbX + 2, kTb1H = kTbY + 2;  // sweep-1 output / rhs tile
+constexpr int kTbLoad0 = (kTb0W * kTb0H + kTbThreads - 1) / kTbThreads;
+constexpr int kTbLoad1 = (kTb1W * kTb1H + kTbThreads - 1) / kTbThreads;
+
+__device__ __forceinline__ int wrap_if(int c, int n, int periodic) { return periodic ? (c < 0 ? c + n : (c >= n ? c - n : c)) : c; }
+
+template <int KIND>
+__global__ void __launch_bounds__(kTbThreads) k_jacobi_tb2(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    __shared__ float s0[3][kTb0H][kTb0W];  // input planes, slot = plane mod 3
+    __shared__ float s1[3][kTb1H][kTb1W];  // first-sweep planes, slot = plane mod 3
+    __shared__ float sr[4][kTb1H][kTb1W];  // right-hand side planes, slot = plane mod 4
+    const int tid = static_cast<int>(threadIdx.x);
+    const int x0 = static_cast<int>(blockIdx.x) * kTbX, y0 = static_cast<int>(blockIdx.y) * kTbY;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    const int sy = d.nx, sz = d.nx * d.ny;
+    const int px = g.periodic[0], py = g.periodic[1], pz = g.periodic[2];
+    const auto mod3 = [](int q) { return ((q % 3) + 3) % 3; };
+    const auto mod4 = [](int q) { return q & 3; };  // two's complement: also right for q < 0
+
+    // in-plane offset of each element this thread stages (-1: outside the grid)
+    int off0[kTbLoad0], off1[kTbLoad1];
+#pragma unroll
+    for (int k = 0; k < kTbLoad0; ++k) {
+        const int i = tid + k * kTbThreads;
+        off0[k] = -1;
+        if (i < kTb0W * kTb0H) {
+            const int gx = wrap_if(x0 - 2 + i % kTb0W, d.nx, px), gy = wrap_if(y0 - 2 + i / kTb0W, d.ny, py);
+            if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny)) off0[k] = gx + sy * gy;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kTbLoad1; ++k) {
+        const int i = tid + k * kTbThreads;
+        off1[k] = -1;
+        if (i < kTb1W * kTb1H) {
+            const int gx = wrap_if(x0 - 1 + i % kTb1W, d.nx, px), gy = wrap_if(y0 - 1 + i / kTb1W, d.ny, py);
+            if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny)) off1[k] = gx + sy * gy;
+        }
+    }
+    // stored plane of plane index q (periodic wrap), -1 outside a non-periodic grid
+    const auto plane = [&](int q) { return pz ? (q < 0 ? q + d.nz : (q >= d.nz ? q - d.nz : q)) : (static_cast<unsigned>(q) < static_cast<unsigned>(d.nz) ? q : -1); };
+    float r0[kTbLoad0], r1[kTbLoad1];
+    const auto fetch = [&](int q) {  // input and rhs of plane q into registers
+        const int pq = plane(q);
+#pragma unroll
+        for (int k = 0; k < kTbLoad0; ++k) r0[k] = (pq >= 0 && off0[k] >= 0) ? src[off0[k] + sz * pq] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < kTbLoad1; ++k) r1[k] = (pq >= 0 && off1[k] >= 0) ? rhs[off1[k] + sz * pq] : 0.0f;
+    };
+    const auto stage = [&](int q) {  // registers -> the ring slots of plane q
+#pragma unroll
+        for (int k = 0; k < kTbLoad0; ++k) {
+            const int i = tid + k * kTbThreads;
+            if (i < kTb0W * kTb0H) (&s0[mod3(q)][0][0])[i] = r0[k];
+        }
+#pragma unroll
+        for (int k = 0; k < kTbLoad1; ++k) {
+            const int i = tid + k * kTbThreads;
+            if (i < kTb1W * kTb1H) (&sr[mod4(q)][0][0])[i] = r1[k];
+        }
+    };
+    // one cell update from a 3-plane ring (slot = plane mod 3); (hx, hy) are
+    // the cell's ring coordinates, q its plane, (gx, gy) its grid coordinates
+    const auto cell = [&](const float* ring, int W, int H, int hx, int hy, int q, int gx, int gy, float b) {
+        const int n = W * H, at = hy * W + hx;
+        const float* c = ring + mod3(q) * n + at;
+        const float self = *c;
+        const float xm = (!px && gx == 0) ? tb::ghost(g, XM, self) : c[-1];
+        const float xp = (!px && gx == d.nx - 1) ? tb::ghost(g, XP, self) : c[1];
+        const float ym = (!py && gy == 0) ? tb::ghost(g, YM, self) : c[-W];
+        const float yp = (!py && gy == d.ny - 1) ? tb::ghost(g, YP, self) : c[W];
+        const float zm = (!pz && q == 0) ? tb::ghost(g, ZM, self) : ring[mod3(q - 1) * n + at];
+        const float zp = (!pz && q == d.nz - 1) ? tb::ghost(g, ZP, self) : ring[mod3(q + 1) * n + at];
+        return tb::update_div<KIND>(tb::numerator<KIND>(xm + xp + ym + yp + zm + zp, b, coef), divisor, recip);
+    };
+
+    // Iteration q stages input plane q + 1, runs the first sweep on plane q
+    // and the second sweep on plane q - 1. Input planes zb - 2 and zb - 1 are
+    // staged before the loop.
+    fetch(zb - 2);
+    stage(zb - 2);
+    fetch(zb - 1);
+    stage(zb - 1);
+    fetch(zb);
+    for (int q = zb - 1; q <= ze; ++q) {
+        stage(q + 1);
+        if (q + 2 <= ze + 1) fetch(q + 2);
+        __syncthreads();  // input plane q + 1 staged; the second sweep of q - 2 done with s1 slot mod3(q)
+        if (plane(q) >= 0) {
+#pragma unroll
+            for (int k = 0; k < kTbLoad1; ++k) {
+                const int i = tid + k * kTbThreads;
+                if (i < kTb1W * kTb1H) {
+                    const int hx = i % kTb1W, hy = i / kTb1W;
+                    const int gx = wrap_if(x0 - 1 + hx, d.nx, px), gy = wrap_if(y0 - 1 + hy, d.ny, py);
+                    if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny))
+                        s1[mod3(q)][hy][hx] = cell(&s0[0][0][0], kTb0W, kTb0H, hx + 1, hy + 1, q, gx, gy, sr[mod4(q)][hy][hx]);
+                }
+            }
+        }
+        __syncthreads();  // first-sweep plane q complete
+        const int qo = q - 1;
+        if (qo >= zb && qo < ze) {
+#pragma unroll
+            for (int k = 0; k < (kTbX * kTbY) / kTbThreads; ++k) {
+                const int i = tid + k * kTbThreads;
+                const int tx = i % kTbX, ty = i / kTbX;
+                const int gx = x0 + tx, gy = y0 + ty;
+                if (gx < d.nx && gy < d.ny) dst[gx + sy * gy + sz * qo] = cell(&s1[0][0][0], kTb1W, kTb1H, tx + 1, ty + 1, qo, gx, gy, sr[mod4(qo)][ty + 1][tx + 1]);
+            }
+        }
+    }
+}
+
 // FP64 sums of the pressure residual e = h^2 div - (sum6(p) - 6 p) and of
 // b = h^2 div (the four sums of k_residual_sums, same per-cell arithmetic),
 // with the z-marching float4 layout above; one atomic per sum per CTA.
@@ -362,6 +492,30 @@ __global__ void k_scale_field(float* __restrict__ q, float factor, size_t n) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = q[i] * factor;
 }
 
+struct TbShape2 {
+    dim3 grid;
+    int z_chunk;
+};
+
+// Launch shape of k_jacobi_tb2: one wave of CTAs, z chunks of at least 8 planes.
+template <typename Kernel>
+TbShape2 tb2_shape(const Dims& d, Kernel kernel) {
+    static int per_sm = [&] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kTbThreads, 0) != cudaSuccess || n < 1) n = 2;
+        return n;
+    }();
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int bx = (d.nx + kTbX - 1) / kTbX, by = (d.ny + kTbY - 1) / kTbY;
+    long long chunks = static_cast<long long>(sms) * per_sm / (static_cast<long long>(bx) * by);
+    if (chunks < 1) chunks = 1;
+    int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
+    if (z_chunk < 8) z_chunk = d.nz < 8 ? d.nz : 8;
+    return {dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), static_cast<unsigned>((d.nz + z_chunk - 1) / z_chunk)), z_chunk};
+}
+
 GhostRule ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb);
 
 template <int KIND>
@@ -394,12 +548,19 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         const VecShape vs = vec ? vec_shape(d, k_jacobi_vec<KIND>) : VecShape{};
         const dim3 jblock(32, 8, 1);
         const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
-        // Choose the first source so that the last sweep lands in x.
+        // With blocking requested, sweeps go two per pass (k_jacobi_tb2) where
+        // the grid suits the vectorised kernels, an odd sweep first as a
+        // single sweep. (On B200 the single-sweep kernel is faster today.)
+        const int pairs = (vec && a.blocked) ? a.iterations / 2 : 0;
+        const int singles = a.iterations - 2 * pairs;
+        const int units = pairs + singles;
+        const TbShape2 tb = pairs > 0 ? tb2_shape(d, k_jacobi_tb2<KIND>) : TbShape2{};
+        // Choose the first source so that the last launch lands in x.
         const float* src = a.x;
         if (a.init == INIT_FROM_B) src = a.b;
         else if (a.init == INIT_ZERO) {
-            // Zero the buffer the first sweep does not write.
-            float* zero = (a.iterations & 1) ? a.scratch : a.x;
+            // Zero the buffer the first launch does not write.
+            float* zero = (units & 1) ? a.scratch : a.x;
             if ((e = cudaMemsetAsync(zero, 0, bytes, s)) != cudaSuccess) return e;
             src = zero;
         }
@@ -407,15 +568,16 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             if (src != a.x) e = cudaMemcpyAsync(a.x, src, bytes, cudaMemcpyDeviceToDevice, s);
             if (e != cudaSuccess) return e;
         }
-        for (int it = 0; it < a.iterations; ++it) {
-            const int left = a.iterations - it;  // sweeps still to run, this one included
+        for (int u = 0; u < units; ++u) {
+            const int left = units - u;  // launches still to run, this one included
             float* dst = (left & 1) ? a.x : a.scratch;
             if (dst == src) dst = (dst == a.x) ? a.scratch : a.x;
-            if (vec) k_jacobi_vec<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
+            if (u >= singles) k_jacobi_tb2<KIND><<<tb.grid, kTbThreads, 0, s>>>(dst, src, a.b, a.coef, tb.z_chunk, d, g);
+            else if (vec) k_jacobi_vec<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
             else k_jacobi<KIND><<<grid, jblock, 0, s>>>(dst, src, a.b, a.coef, d, a.flow, a.scalar);
             src = dst;
         }
-        if (a.launches) *a.launches += a.iterations;
+        if (a.launches) *a.launches += units;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (src != a.x && a.iterations > 0) {
             if ((e = cudaMemcpyAsync(a.x, src, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
