@@ -31,6 +31,9 @@ Solver variants, all timed the same way (W untimed steps, then K steps):
           convolutions are reported beside it against the bf16 peak.
   fixed_iterations : the reference's own configuration (80 red-black
           pressure iterations per step) for a like-for-like kernel comparison.
+  batched : 64 uneven simulations (sizes over {32..128}^3, config-0
+          coefficients) stepped by one batch graph launch per step; aggregate
+          cell-updates/s (the reference arm steps its contexts in turn).
   cpu_baseline : the FP32 C++/OpenMP transcription of the step (oracle/) on a
           bounded sample, scaled to the metric's unit.
 
@@ -86,6 +89,7 @@ def parse():
     p.add_argument("--learning-rate", type=float, default=3e-4)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--fixed-steps", type=int, default=20)
+    p.add_argument("--batch-steps", type=int, default=20, help="steps of the batched 64-simulation workload (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--fixed-pressure-iterations", type=int, default=0,
@@ -367,6 +371,38 @@ def fixed_iterations(sf, lib, scene, steps, warmup, device, world):
     return {"steps_per_s": world * steps / t, "ms_per_step": 1000.0 * t / steps, "steps": steps, "pressure_iterations": scene.config.pressure_iterations, "scheme": "rbgs"}
 
 
+def batched(sf, lib, steps, warmup, count=64, use_batch=True):
+    """Batched workload: `count` uneven plumes (sizes over {32..128}^3,
+    config-0 coefficients, 20 diffusion / 40 red-black pressure iterations).
+    use_batch: one batch graph launch per step (this library); otherwise each
+    context is stepped in turn on its own stream (how a caller drives the
+    reference library). Returns aggregate cell-updates/s."""
+    import torch
+
+    scenes = sf.scenes.batch_scenes(count=count)
+    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib) for sc in scenes]
+    for sim, sc in zip(sims, scenes):
+        sf.scenes.apply_inputs(sim, sc, 0)
+    cells = sum(sim.cells for sim in sims)
+    batch = sf.Batch(sims) if use_batch else None
+    step = batch.step if use_batch else (lambda: [sim.step(1) for sim in sims])
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    if batch is not None:
+        batch.close()
+    for sim in sims:
+        sim.close()
+    sizes = sorted({sc.config.nx for sc in scenes})
+    return {"cell_updates_per_s": cells * steps / t, "steps_per_s": steps / t, "sims": count, "cells": cells, "sizes": sizes, "steps": steps,
+            "timing": "host wall clock around the steps with a device synchronize on both sides (work spans many streams)", "mode": "one batch graph launch per step" if use_batch else "each context stepped on its own stream"}
+
+
 def cpu_baseline(sf, scene, plain_iterations):
     """The FP32 C++/OpenMP transcription of the step (oracle/) on all host
     cores: one step without pressure sweeps and one with 16 Jacobi sweeps,
@@ -438,6 +474,8 @@ def reference_arm(sf, args, scene, world, rank, local):
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": f"{args.steps} steps; the reference has no CPU implementation, so its own CUDA backend (backend-cuda.cu built unmodified for sm_100a) runs on the GPU"},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     line["fixed_iterations"] = fixed_iterations(sf, lib, scene, args.fixed_steps, args.warmup, local, 1)
+    if args.batch_steps > 0:
+        line["batched"] = batched(sf, lib, args.batch_steps, args.warmup, use_batch=False)
     c = clk.summary()
     if c:
         line["clocks"] = c
@@ -509,6 +547,7 @@ def main():
     for sim in sims.values():
         sim.close()
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
+    batch = batched(sf, None, args.batch_steps, args.warmup) if args.batch_steps > 0 else None
 
     config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
               "grid": [n, n, n], "solver": {"learned": "Jacobi sweeps from the learned warm start", "plain": "Jacobi sweeps from zero", "previous": "Jacobi sweeps from the previous pressure", "rbgs": "red-black Gauss-Seidel from zero"}[headline]
@@ -518,7 +557,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
             "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"],
             "speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
-            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed}
+            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch}
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c

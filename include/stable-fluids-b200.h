@@ -154,6 +154,21 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_train_step(void*
  * attachment and must not be used on another stream while the context steps. */
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network);
 
+/* ---- Batched stepping (no counterpart in the reference) ----
+ * A batch holds the step graphs of several contexts (each with its own grid
+ * size and fields) as children of one CUDA graph: one batch step launches
+ * every context's step once, and the simulations' kernels run concurrently
+ * on the GPU. The batch is ordered after the work queued on each context's
+ * stream and each context's stream after the batch, so update/view calls keep
+ * working as for a single context. The batch copies the step graphs when it
+ * is created: rebuild it after stable_fluids_b200_attach_network. Contexts
+ * with a residual-driven solve (conditional graph nodes) cannot be batched. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_create(void* const* contexts, uint32_t count, void** out_batch);
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_step(void* batch);
+/* Number of contexts, kernel launches per batch step, and the batch's stream. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_info(void* batch, uint32_t* out_count, int32_t* out_kernels_per_step, void** out_stream);
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_destroy(void* batch);
+
 /* No counterpart in the reference. The FP64 relative Poisson residual
  * ||b - A p|| / ||b|| (b = h^2 divergence, mean removed when no face is
  * OUTFLOW; A p = sum of the 6 neighbours - 6 p with the pressure ghost rules)

@@ -138,6 +138,10 @@ B200_SYMBOLS = (
     "stable_fluids_b200_network_gradients",
     "stable_fluids_b200_network_train_step",
     "stable_fluids_b200_attach_network",
+    "stable_fluids_b200_batch_create",
+    "stable_fluids_b200_batch_step",
+    "stable_fluids_b200_batch_info",
+    "stable_fluids_b200_batch_destroy",
 )
 
 (STAGE_FORCES, STAGE_VELOCITY_ADVECTION, STAGE_VELOCITY_DIFFUSION, STAGE_DIVERGENCE, STAGE_PRESSURE,
@@ -174,6 +178,10 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_network_gradients.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, POINTER(c_double), P, P]
         lib.stable_fluids_b200_network_train_step.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, c_float, POINTER(c_double), P]
         lib.stable_fluids_b200_attach_network.argtypes = [P, P]
+        lib.stable_fluids_b200_batch_create.argtypes = [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]
+        lib.stable_fluids_b200_batch_step.argtypes = [P]
+        lib.stable_fluids_b200_batch_info.argtypes = [P, POINTER(c_uint32), POINTER(c_int32), POINTER(c_void_p)]
+        lib.stable_fluids_b200_batch_destroy.argtypes = [P]
         for name in B200_SYMBOLS:
             getattr(lib, name).restype = c_int32
     return lib
@@ -200,12 +208,12 @@ def default_options(lib: ctypes.CDLL | None = None) -> B200Options:
     return o
 
 
-from .simulation import Simulation, StableFluidsError  # noqa: E402  (needs the structs above)
+from .simulation import Batch, Simulation, StableFluidsError  # noqa: E402  (needs the structs above)
 from . import scenes  # noqa: E402
 from .warmstart import WarmStartNetwork, LAYERS as NETWORK_LAYERS  # noqa: E402
 
 __all__ = [
-    "Simulation", "StableFluidsError", "load_library", "default_options", "scenes", "WarmStartNetwork", "NETWORK_LAYERS",
+    "Simulation", "Batch", "StableFluidsError", "load_library", "default_options", "scenes", "WarmStartNetwork", "NETWORK_LAYERS",
     "SimulationConfig", "ScalarFieldDesc", "VectorFieldDesc", "ContextCreateDesc", "FlowBoundary", "FlowFace",
     "ScalarBoundary", "ScalarFace", "ViewRequest", "View", "B200Options", "B200StepStats", "B200StepInfo",
 ]

@@ -782,6 +782,103 @@ StableFluidsResult stable_fluids_b200_attach_network(void* context, void* networ
     return STABLE_FLUIDS_RESULT_OK;
 }
 
+}  // extern "C"
+
+namespace sfb {
+namespace {
+
+// A batch: the step graphs of several contexts as child graphs of one graph,
+// launched once per batch step on the batch's stream. The children share no
+// data, so the GPU runs the simulations' kernels concurrently; small grids
+// that cannot fill the GPU alone fill it together, and the host pays one
+// launch per batch step instead of one per simulation.
+struct Batch {
+    std::vector<Context*> contexts;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+    int kernels = 0;
+
+    ~Batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (done) cudaEventDestroy(done);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace
+}  // namespace sfb
+
+extern "C" {
+
+StableFluidsResult stable_fluids_b200_batch_create(void* const* contexts, uint32_t count, void** out_batch) {
+    if (out_batch == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    *out_batch = nullptr;
+    if (contexts == nullptr || count == 0) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    std::unique_ptr<sfb::Batch> b{new (std::nothrow) sfb::Batch{}};
+    if (!b) return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaGraphCreate(&b->graph, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    for (uint32_t i = 0; i < count; ++i) {
+        auto* c = static_cast<Context*>(contexts[i]);
+        if (c == nullptr || c->graph == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        for (auto* other : b->contexts)
+            if (other == c) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;  // a context steps once per batch step
+        // all work queued on the context so far (updates) precedes the batch
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        cudaGraphNode_t node = nullptr;
+        if (cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, c->graph) != cudaSuccess) {
+            cudaGetLastError();
+            return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        }
+        b->contexts.push_back(c);
+        b->kernels += c->step_kernels;
+    }
+    if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
+        b->exec = nullptr;
+        cudaGetLastError();
+        return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    *out_batch = b.release();
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_batch_step(void* batch) {
+    sfb::Range range("stable.batch_step");
+    if (batch == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& b = *static_cast<sfb::Batch*>(batch);
+    // order the batch after each context's queued work and each context after the batch
+    for (auto* c : b.contexts) {
+        if (cudaEventRecord(c->ready, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaStreamWaitEvent(b.stream, c->ready, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    if (cudaGraphLaunch(b.exec, b.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaEventRecord(b.done, b.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    for (auto* c : b.contexts)
+        if (cudaStreamWaitEvent(c->stream, b.done, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_batch_info(void* batch, uint32_t* out_count, int32_t* out_kernels_per_step, void** out_stream) {
+    if (batch == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const auto& b = *static_cast<const sfb::Batch*>(batch);
+    if (out_count) *out_count = static_cast<uint32_t>(b.contexts.size());
+    if (out_kernels_per_step) *out_kernels_per_step = b.kernels;
+    if (out_stream) *out_stream = b.stream;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_batch_destroy(void* batch) {
+    if (batch == nullptr) return STABLE_FLUIDS_RESULT_OK;
+    auto* b = static_cast<sfb::Batch*>(batch);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    delete b;
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
 StableFluidsResult stable_fluids_b200_get_step_info(void* context, StableFluidsB200StepInfo* out_info) {
     if (context == nullptr || out_info == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     const auto& c = *static_cast<const Context*>(context);

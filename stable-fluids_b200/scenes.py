@@ -169,6 +169,23 @@ def training_scene(seed: int, n: int = 128, pressure_iterations: int = 1000) -> 
     return plume(f"train-{seed}-{n}^3", (n, n, n), dt=0.1, viscosity=1e-4, diffusion=1e-5, diffuse_iterations=20, pressure_iterations=pressure_iterations, sources=sources, steps=1)
 
 
+def batch_scenes(count: int = 64, seed: int = 4, steps: int = 100) -> list[Scene]:
+    """Batched workload: `count` plumes with sizes drawn from the seed over
+    {32, 48, 64, 96, 128}^3, each with its own seeded Gaussian source
+    (radius 2-6 cells, strength 10) and upward force U[1, 10], config-0
+    coefficients (dt 0.1, viscosity 1e-4, diffusion 1e-5, 20 diffusion and 40
+    pressure iterations, Stam walls), `steps` steps."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.choice([32, 48, 64, 96, 128]))
+        r = float(rng.uniform(2.0, 6.0))
+        cx, cz = rng.uniform(r + 2, n - r - 2, size=2)
+        src = [(float(cx), 2 + r, float(cz), r, 10.0, float(rng.uniform(1.0, 10.0)))]
+        out.append(plume(f"batch-{k}-{n}^3", (n, n, n), dt=0.1, viscosity=1e-4, diffusion=1e-5, diffuse_iterations=20, pressure_iterations=40, sources=src, steps=steps))
+    return out
+
+
 def apply_inputs(sim, scene: Scene, step_index: int):
     """Uploads the scene's source and force for step `step_index` (the
     impulse only on step 0). `sim` is anything with set_scalar_source and

@@ -187,3 +187,49 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Several Simulations stepped together: one graph launch per batch step
+    runs every simulation's step graph concurrently (stable_fluids_b200_batch_*)."""
+
+    def __init__(self, simulations):
+        import torch
+
+        self.sims = list(simulations)
+        if not self.sims:
+            raise ValueError("empty batch")
+        self.lib = self.sims[0].lib
+        ctxs = (c_void_p * len(self.sims))(*[s.ctx for s in self.sims])
+        h = c_void_p()
+        rc = self.lib.stable_fluids_b200_batch_create(ctxs, len(self.sims), byref(h))
+        if rc != RESULT_OK:
+            raise StableFluidsError("stable_fluids_b200_batch_create", rc)
+        self.handle = h
+        n, k, st = ctypes.c_uint32(0), ctypes.c_int32(0), c_void_p()
+        self.lib.stable_fluids_b200_batch_info(h, byref(n), byref(k), byref(st))
+        self.kernels_per_step = k.value
+        self.stream = torch.cuda.ExternalStream(st.value, device=self.sims[0].device)
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            rc = self.lib.stable_fluids_b200_batch_step(self.handle)
+            if rc != RESULT_OK:
+                raise StableFluidsError("stable_fluids_b200_batch_step", rc)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.stable_fluids_b200_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -346,3 +346,25 @@ def test_blocked_jacobi_matches_single_sweeps(kind, sf, lib, cuda):
         outs.append(C.collect_outputs(sim, sf, C.Case(kind, scene.config, scene.scalars, scene.vectors, scene.steps)))
         sim.close()
     assert_bit_equal(outs[1], outs[0])
+
+
+@pytest.mark.gpu
+def test_batch_step_matches_single_contexts(sf, lib, cuda):
+    """A batch of differently sized contexts stepped through one graph gives
+    the same bits as stepping each context on its own."""
+    scenes = sf.scenes.batch_scenes(count=4, seed=7, steps=3)
+    single = []
+    for sc in scenes:
+        sim = sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib)
+        sf.scenes.run(sim, sc)
+        single.append(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)))
+        sim.close()
+    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib) for sc in scenes]
+    for sim, sc in zip(sims, scenes):
+        sf.scenes.apply_inputs(sim, sc, 0)
+    with sf.Batch(sims) as batch:
+        assert batch.kernels_per_step == sum(s.info().kernels_per_step for s in sims)
+        batch.step(scenes[0].steps)
+    for sim, sc, ref in zip(sims, scenes, single):
+        assert_bit_equal(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), ref)
+        sim.close()
