@@ -34,6 +34,9 @@ Solver variants, all timed the same way (W untimed steps, then K steps):
   batched : 64 uneven simulations (sizes over {32..128}^3, config-0
           coefficients) stepped by one batch graph launch per step; aggregate
           cell-updates/s (the reference arm steps its contexts in turn).
+  bf16_storage : the 384^3 plume (20/80 red-black iterations) with FP32 and
+          with BF16 storage of velocity and density: steps/s and the fields'
+          relative difference.
   cpu_baseline : the FP32 C++/OpenMP transcription of the step (oracle/) on a
           bounded sample, scaled to the metric's unit.
 
@@ -90,6 +93,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--fixed-steps", type=int, default=20)
     p.add_argument("--batch-steps", type=int, default=20, help="steps of the batched 64-simulation workload (0: skip)")
+    p.add_argument("--bf16-size", type=int, default=384)
+    p.add_argument("--bf16-steps", type=int, default=5, help="timed steps of the FP32-vs-BF16-storage comparison (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--fixed-pressure-iterations", type=int, default=0,
@@ -403,6 +408,38 @@ def batched(sf, lib, steps, warmup, count=64, use_batch=True):
             "timing": "host wall clock around the steps with a device synchronize on both sides (work spans many streams)", "mode": "one batch graph launch per step" if use_batch else "each context stepped on its own stream"}
 
 
+def bf16_storage(sf, n, steps, warmup, device):
+    """Mixed precision at n^3 (the config-1 plume generator, 20 diffusion /
+    80 red-black pressure iterations): steps/s with FP32 and with BF16
+    storage of velocity and density, and the BF16 run's relative L2
+    difference from the FP32 run per field after warmup + steps steps."""
+    import numpy as np
+    import torch
+
+    scene = sf.scenes.config1(n=n)
+    out = {"grid": [n, n, n], "steps": steps, "warmup": warmup}
+    fields = {}
+    for name, storage in (("fp32", sf.STORAGE_FP32), ("bf16", sf.STORAGE_BF16)):
+        opts = sf.default_options()
+        opts.storage = storage
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=device)
+        sf.scenes.apply_inputs(sim, scene, 0)
+        sim.step(warmup)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(sim.stream)
+        sim.step(steps)
+        end.record(sim.stream)
+        torch.cuda.synchronize()
+        out[f"{name}_steps_per_s"] = steps / (start.elapsed_time(end) / 1000.0)
+        out[f"{name}_device_bytes"] = sim.info().device_bytes
+        fields[name] = {"density": sim.fetch(sf.VIEW_SCALAR_FIELD_DATA, sim.scalar_handles[0]), "velocity": np.stack(sim.fetch(sf.VIEW_FLOW_VELOCITY)), "pressure": sim.fetch(sf.VIEW_FLOW_PRESSURE)}
+        sim.close()
+    out["speedup"] = out["bf16_steps_per_s"] / out["fp32_steps_per_s"]
+    out["rel_l2_bf16_vs_fp32"] = {k: float(np.linalg.norm(fields["bf16"][k].astype(np.float64) - fields["fp32"][k]) / max(np.linalg.norm(fields["fp32"][k].astype(np.float64)), 1e-30)) for k in fields["fp32"]}
+    return out
+
+
 def cpu_baseline(sf, scene, plain_iterations):
     """The FP32 C++/OpenMP transcription of the step (oracle/) on all host
     cores: one step without pressure sweeps and one with 16 Jacobi sweeps,
@@ -548,6 +585,7 @@ def main():
         sim.close()
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
     batch = batched(sf, None, args.batch_steps, args.warmup) if args.batch_steps > 0 else None
+    mixed = bf16_storage(sf, args.bf16_size, args.bf16_steps, args.warmup, local) if args.bf16_steps > 0 else None
 
     config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
               "grid": [n, n, n], "solver": {"learned": "Jacobi sweeps from the learned warm start", "plain": "Jacobi sweeps from zero", "previous": "Jacobi sweeps from the previous pressure", "rbgs": "red-black Gauss-Seidel from zero"}[headline]
@@ -557,7 +595,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
             "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"],
             "speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
-            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch}
+            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch, "bf16_storage": mixed}
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c

@@ -41,6 +41,15 @@ typedef enum StableFluidsB200WarmStart {
     STABLE_FLUIDS_B200_WARM_START_LEARNED  = 2, /* p0 = network(divergence, previous pressure) */
 } StableFluidsB200WarmStart;
 
+typedef enum StableFluidsB200Storage {
+    STABLE_FLUIDS_B200_STORAGE_FP32 = 0, /* every field FP32 (the reference's layout) */
+    /* velocity and scalar fields stored as BF16 (half the bytes of the
+     * advection and diffusion passes), all arithmetic FP32; pressure,
+     * divergence, forces and sources stay FP32. Views of velocity and scalar
+     * data are FP32 copies converted at stable_fluids_get_view_cuda. */
+    STABLE_FLUIDS_B200_STORAGE_BF16 = 1,
+} StableFluidsB200Storage;
+
 typedef struct StableFluidsB200Options {
     uint32_t scheme;                  /* StableFluidsB200Scheme */
     uint32_t warm_start;              /* StableFluidsB200WarmStart */
@@ -52,7 +61,8 @@ typedef struct StableFluidsB200Options {
     int32_t warm_start_trial_iterations; /* learned warm start: sweeps run on the learned and on the
                                           * previous-pressure start before the one with the smaller
                                           * rel_res is kept (0 = compare the starts themselves) */
-    uint32_t reserved[8];
+    uint32_t storage;                 /* StableFluidsB200Storage */
+    uint32_t reserved[7];
 } StableFluidsB200Options;
 
 /* Statistics of the most recent step (device values copied to the host). */

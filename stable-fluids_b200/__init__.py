@@ -42,6 +42,7 @@ VIEW_LAYOUT_F32_3D, VIEW_LAYOUT_F32_3D_SOA3 = 0, 1
 
 SCHEME_RBGS, SCHEME_JACOBI = 0, 1
 WARM_START_ZERO, WARM_START_PREVIOUS, WARM_START_LEARNED = 0, 1, 2
+STORAGE_FP32, STORAGE_BF16 = 0, 1
 
 
 # -------------------------------------------------------------- structs --
@@ -103,7 +104,7 @@ class B200Options(ctypes.Structure):
         ("scheme", c_uint32), ("warm_start", c_uint32), ("iterations_per_pass", c_int32),
         ("residual_tolerance", c_float), ("max_pressure_iterations", c_int32),
         ("residual_check_interval", c_int32), ("compute_residual", c_uint32),
-        ("warm_start_trial_iterations", c_int32), ("reserved", c_uint32 * 8),
+        ("warm_start_trial_iterations", c_int32), ("storage", c_uint32), ("reserved", c_uint32 * 7),
     ]
 
 

@@ -42,9 +42,10 @@ struct Range {
 struct ScalarField {
     StableFluidsScalarFieldDesc desc{};
     ScalarBC bc{};
-    float* data = nullptr;
-    float* temp = nullptr;
+    float* data = nullptr;    // BF16 elements in a BF16-storage context
+    float* temp = nullptr;    // BF16 elements in a BF16-storage context
     float* source = nullptr;
+    float* view = nullptr;    // BF16 storage: FP32 copy for views and updates
 };
 
 struct VectorField {
@@ -65,9 +66,13 @@ struct Context {
 
     void* slab = nullptr;
     size_t slab_bytes = 0;
+    // Advected fields: FP32, or BF16 elements (bf16) behind the same
+    // pointers; views of a BF16 context are FP32 copies made at get_view.
+    bool bf16 = false;
     float* vel[3] = {nullptr, nullptr, nullptr};
     float* temp[3] = {nullptr, nullptr, nullptr};
-    void* packed = nullptr;  // float4 velocity
+    float* view_vel[3] = {nullptr, nullptr, nullptr};
+    void* packed = nullptr;  // packed velocity: float4, or 4 x BF16
     float* pressure = nullptr;
     float* divergence = nullptr;
     float* magnitude = nullptr;
@@ -173,6 +178,11 @@ void apply_env_overrides(StableFluidsB200Options& o) {
         else if (s == "learned" || s == "2") o.warm_start = STABLE_FLUIDS_B200_WARM_START_LEARNED;
     }
     if (env_flag("STABLE_FLUIDS_B200_COMPUTE_RESIDUAL")) o.compute_residual = 1;
+    if (const char* v = std::getenv("STABLE_FLUIDS_B200_STORAGE")) {
+        const std::string_view s(v);
+        if (s == "bf16" || s == "BF16" || s == "1") o.storage = STABLE_FLUIDS_B200_STORAGE_BF16;
+        else if (s == "fp32" || s == "FP32" || s == "0") o.storage = STABLE_FLUIDS_B200_STORAGE_FP32;
+    }
 }
 
 void default_options(StableFluidsB200Options& o) {
@@ -191,6 +201,7 @@ bool validate_options(const StableFluidsB200Options& o) {
     if (o.scheme > STABLE_FLUIDS_B200_SCHEME_JACOBI) return false;
     if (o.warm_start > STABLE_FLUIDS_B200_WARM_START_LEARNED) return false;
     if (o.warm_start_trial_iterations < 0) return false;
+    if (o.storage > STABLE_FLUIDS_B200_STORAGE_BF16) return false;
     if (o.iterations_per_pass < 0) return false;
     if (!(o.residual_tolerance >= 0.0f) || !std::isfinite(o.residual_tolerance)) return false;
     if (o.residual_tolerance > 0.0f && (o.max_pressure_iterations <= 0 || o.residual_check_interval <= 0)) return false;
@@ -253,6 +264,7 @@ struct Stages {
             ForceArgs fa{};
             for (int comp = 0; comp < 3; ++comp) fa.vel[comp] = c.vel[comp];
             fa.dt = c.config.dt;
+            fa.bf16 = c.bf16 ? 1 : 0;
             fa.n = c.cells;
             for (; k < list.size() && fa.force_count < kMaxForcesPerLaunch; ++k, ++fa.force_count)
                 for (int comp = 0; comp < 3; ++comp) fa.force[fa.force_count][comp] = list[k]->data[comp];
@@ -268,7 +280,7 @@ struct Stages {
     // 2. advection (:617-619); skipped when alpha <= 0 because the reference
     //    then never copies the advected velocity back (:623).
     void advect_velocity() {
-        if (alpha_v() > 0.0f) ok(launch_advect_velocity(c.packed, c.temp[0], c.temp[1], c.temp[2], c.config.dt, c.dims, h(), c.flow, c.stream));
+        if (alpha_v() > 0.0f) ok(launch_advect_velocity(c.packed, c.temp[0], c.temp[1], c.temp[2], c.config.dt, c.dims, h(), c.flow, c.bf16, c.stream));
     }
 
     StencilArgs stencil(int kind, int init, int iterations, float coef, float* x, const float* b) {
@@ -288,6 +300,7 @@ struct Stages {
         a.launches = &launches;
         a.blocked = c.blocked ? 1 : 0;
         a.error_flag = &c.stats->error;
+        a.bf16 = (c.bf16 && kind != KIND_PRESSURE) ? 1 : 0;
         return a;
     }
 
@@ -298,7 +311,7 @@ struct Stages {
     }
 
     // 4. divergence (:643).
-    void divergence() { ok(launch_divergence(c.divergence, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.stream)); }
+    void divergence() { ok(launch_divergence(c.divergence, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.bf16, c.stream)); }
 
     // 5. pressure from zero (:644-649), from the previous step's pressure, or
     //    from the learned warm start.
@@ -397,7 +410,7 @@ struct Stages {
     void project() {
         // the residual-driven solve has measured the residual already
         const bool measure = c.residual_enabled && !residual_measured;
-        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, nullptr, c.stream));
+        ok(launch_project(c.vel[0], c.vel[1], c.vel[2], any_scalar_advects() ? c.packed : nullptr, c.pressure, c.divergence, c.dims, h(), h() * h(), c.flow, nullptr, c.bf16, c.stream));
         if (measure) {
             // projection reads p and div without changing them: the residual
             // of the solve is measured after it, by one separate pass
@@ -414,20 +427,20 @@ struct Stages {
             const float a_s = alpha_s(f);
             const float factor = f.desc.dissipation > 0.0f ? 1.0f / (1.0f + c.config.dt * f.desc.dissipation) : 1.0f;  // :665
             if (a_s > 0.0f) {
-                ok(launch_scalar_source_advect(c.packed, f.data, f.source, f.temp, c.config.dt, c.dims, h(), c.flow, f.bc, c.stream));
+                ok(launch_scalar_source_advect(c.packed, f.data, f.source, f.temp, c.config.dt, c.dims, h(), c.flow, f.bc, c.bf16, c.stream));
                 auto a = stencil(KIND_SCALAR, INIT_FROM_B, c.config.diffuse_iterations, a_s, f.data, f.temp);
                 a.scalar = f.bc;
                 a.out_scale = factor;
                 ok(launch_stencil(a, c.stream), 0);
             } else {
-                ok(launch_scalar_source(f.data, f.source, c.config.dt, c.cells, c.stream));
-                if (f.desc.dissipation > 0.0f) ok(launch_scale(f.data, factor, c.cells, c.stream));
+                ok(launch_scalar_source(f.data, f.source, c.config.dt, c.cells, c.bf16, c.stream));
+                if (f.desc.dissipation > 0.0f) ok(launch_scale(f.data, factor, c.cells, c.bf16, c.stream));
             }
         }
     }
 
     // 8. post-projection divergence and |u| (:670-671).
-    void diagnostics() { ok(launch_post_diagnostics(c.divergence, c.magnitude, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.stream)); }
+    void diagnostics() { ok(launch_post_diagnostics(c.divergence, c.magnitude, c.vel[0], c.vel[1], c.vel[2], c.dims, h(), c.flow, c.bf16, c.stream)); }
 
     cudaError_t whole_step() {
         forces();
@@ -502,7 +515,8 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
     c->residual_enabled = options.compute_residual != 0 || options.residual_tolerance > 0.0f;
     // Temporally blocked passes when asked for (iterations_per_pass >= 1);
     // the default one-launch-per-colour kernels are faster on B200 today.
-    c->blocked = options.iterations_per_pass > 0 || env_flag("STABLE_FLUIDS_B200_BLOCKED_STENCIL");
+    c->bf16 = options.storage == STABLE_FLUIDS_B200_STORAGE_BF16;
+    c->blocked = !c->bf16 && (options.iterations_per_pass > 0 || env_flag("STABLE_FLUIDS_B200_BLOCKED_STENCIL"));
 
     // Handles are 1-based indices (:544, :551).
     for (uint32_t i = 0; i < desc->scalar_field_count; ++i) {
@@ -530,9 +544,12 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         Range alloc("stable.create_context.alloc");
         SlabPlan plan;
         const size_t fb = c->field_bytes;
-        for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->vel[k]), fb);
-        for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->temp[k]), fb);
-        plan.add(&c->packed, c->cells * 4 * sizeof(float));
+        const size_t sb = c->bf16 ? c->cells * 2 : fb;  // an advected field
+        for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->vel[k]), sb);
+        for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->temp[k]), sb);
+        if (c->bf16)
+            for (int k = 0; k < 3; ++k) plan.add(reinterpret_cast<void**>(&c->view_vel[k]), fb);
+        plan.add(&c->packed, c->cells * 4 * (c->bf16 ? 2 : sizeof(float)));
         plan.add(reinterpret_cast<void**>(&c->pressure), fb);
         plan.add(reinterpret_cast<void**>(&c->divergence), fb);
         plan.add(reinterpret_cast<void**>(&c->magnitude), fb);
@@ -544,8 +561,9 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
             plan.add(reinterpret_cast<void**>(&c->alt_stats), sizeof(DeviceStats));
         }
         for (auto& f : c->scalars) {
-            plan.add(reinterpret_cast<void**>(&f.data), fb);
-            plan.add(reinterpret_cast<void**>(&f.temp), fb);
+            plan.add(reinterpret_cast<void**>(&f.data), sb);
+            plan.add(reinterpret_cast<void**>(&f.temp), sb);
+            if (c->bf16) plan.add(reinterpret_cast<void**>(&f.view), fb);
             plan.add(reinterpret_cast<void**>(&f.source), fb);
         }
         for (auto& f : c->vectors)
@@ -575,13 +593,13 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         if (cudaMemsetAsync(c->slab, 0, c->slab_bytes, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         for (auto& f : c->scalars) {
             if (f.desc.initial_value == 0.0f) continue;
-            if (launch_fill(f.data, f.desc.initial_value, c->cells, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-            if (launch_fill(f.temp, f.desc.initial_value, c->cells, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+            if (launch_fill(f.data, f.desc.initial_value, c->cells, c->bf16, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+            if (launch_fill(f.temp, f.desc.initial_value, c->cells, c->bf16, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         }
         for (auto& f : c->vectors) {
             const float init[3] = {f.desc.initial_value_x, f.desc.initial_value_y, f.desc.initial_value_z};
             for (int k = 0; k < 3; ++k)
-                if (init[k] != 0.0f && launch_fill(f.data[k], init[k], c->cells, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+                if (init[k] != 0.0f && launch_fill(f.data[k], init[k], c->cells, 0, c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         }
     }
 
@@ -636,6 +654,11 @@ StableFluidsResult stable_fluids_update_scalar_field_cuda(void* context, StableF
     auto& c = *static_cast<Context*>(context);
     auto* f = sfb::scalar_field(c, field);
     if (f == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (c.bf16) {
+        // FP32 values through the view copy into BF16 storage
+        if (sfb::copy_or_zero(f->view, values, c.field_bytes, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        return sfb::launch_convert(f->data, f->view, c.cells, 1, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
     return sfb::copy_or_zero(f->data, values, c.field_bytes, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
 }
 
@@ -684,6 +707,10 @@ StableFluidsResult stable_fluids_get_view_cuda(void* context, const StableFluids
         auto* f = sfb::scalar_field(c, request->scalar_field);
         if (f == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         v.data0 = request->kind == STABLE_FLUIDS_VIEW_SCALAR_FIELD_DATA ? f->data : f->source;
+        if (c.bf16 && request->kind == STABLE_FLUIDS_VIEW_SCALAR_FIELD_DATA) {
+            if (sfb::launch_convert(f->view, f->data, c.cells, 0, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+            v.data0 = f->view;
+        }
         break;
     }
     case STABLE_FLUIDS_VIEW_VECTOR_FIELD: {
@@ -700,6 +727,13 @@ StableFluidsResult stable_fluids_get_view_cuda(void* context, const StableFluids
         v.data0 = c.vel[0];
         v.data1 = c.vel[1];
         v.data2 = c.vel[2];
+        if (c.bf16) {
+            for (int k = 0; k < 3; ++k)
+                if (sfb::launch_convert(c.view_vel[k], c.vel[k], c.cells, 0, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+            v.data0 = c.view_vel[0];
+            v.data1 = c.view_vel[1];
+            v.data2 = c.view_vel[2];
+        }
         break;
     case STABLE_FLUIDS_VIEW_FLOW_VELOCITY_MAGNITUDE: v.data0 = c.magnitude; break;
     case STABLE_FLUIDS_VIEW_FLOW_PRESSURE: v.data0 = c.pressure; break;

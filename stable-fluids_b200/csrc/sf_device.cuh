@@ -12,14 +12,50 @@
 //              about the prescribed wall velocity (2 v_wall - v).
 // Arithmetic that rounds is written in the same expression shapes as the
 // reference so the compiler forms the same fused multiply-adds.
+//
+// Field storage: the advected fields (velocity, scalars) are FP32 (the
+// reference's layout) or BF16 (half the bytes, FP32 arithmetic); the readers
+// below are templates over the element type T (float or __nv_bfloat16) and
+// the packed-velocity type P (float4, or Bf16x4 = four BF16 in 8 bytes).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "sf_types.h"
 #include "stable-fluids-3d.h"
 
 namespace sfb {
+
+struct __align__(8) Bf16x4 {
+    __nv_bfloat162 xy, zw;
+};
+
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename T>
+__device__ __forceinline__ T from_f(float v);
+template <>
+__device__ __forceinline__ float from_f<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+// read-only cached loads
+__device__ __forceinline__ float ldg_f(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ldg_f(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ float4 ldg4(const Bf16x4* p) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+template <typename P>
+__device__ __forceinline__ P pack4(float x, float y, float z);
+template <>
+__device__ __forceinline__ float4 pack4<float4>(float x, float y, float z) { return make_float4(x, y, z, 0.0f); }
+template <>
+__device__ __forceinline__ Bf16x4 pack4<Bf16x4>(float x, float y, float z) { return Bf16x4{__floats2bfloat162_rn(x, y), __floats2bfloat162_rn(z, 0.0f)}; }
 
 __device__ __forceinline__ size_t lin(int x, int y, int z, const Dims& d) {
     return static_cast<size_t>(x) + static_cast<size_t>(d.nx) * (static_cast<size_t>(y) + static_cast<size_t>(d.ny) * static_cast<size_t>(z));
@@ -61,11 +97,12 @@ __device__ __forceinline__ bool scalar_resolve(int& x, int& y, int& z, const Dim
     return true;
 }
 
-__device__ __forceinline__ float load_scalar(const float* __restrict__ f, int x, int y, int z, const Dims& d, const ScalarBC& b) {
-    if (inside(x, y, z, d)) return f[lin(x, y, z, d)];
+template <typename T>
+__device__ __forceinline__ float load_scalar(const T* __restrict__ f, int x, int y, int z, const Dims& d, const ScalarBC& b) {
+    if (inside(x, y, z, d)) return to_f(f[lin(x, y, z, d)]);
     float value;
     if (!scalar_resolve(x, y, z, d, b, value)) return value;
-    return f[lin(x, y, z, d)];
+    return to_f(f[lin(x, y, z, d)]);
 }
 
 // --------------------------------------------------------------- pressure --
@@ -103,8 +140,9 @@ __device__ __forceinline__ float velocity_ghost(float interior, int comp, int ax
 }
 
 // Component `comp` of a SoA velocity field at any integer position.
-__device__ __forceinline__ float load_velocity(const float* __restrict__ f, int comp, int x, int y, int z, const Dims& d, const FlowBC& b) {
-    if (inside(x, y, z, d)) return f[lin(x, y, z, d)];
+template <typename T>
+__device__ __forceinline__ float load_velocity(const T* __restrict__ f, int comp, int x, int y, int z, const Dims& d, const FlowBC& b) {
+    if (inside(x, y, z, d)) return to_f(f[lin(x, y, z, d)]);
     int c[3] = {x, y, z};
     const int n[3] = {d.nx, d.ny, d.nz};
 #pragma unroll
@@ -118,16 +156,17 @@ __device__ __forceinline__ float load_velocity(const float* __restrict__ f, int 
         int q[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) q[k] = clamp_index(c[k], n[k]);
-        const float interior = f[lin(q[0], q[1], q[2], d)];
+        const float interior = to_f(f[lin(q[0], q[1], q[2], d)]);
         return velocity_ghost(interior, comp, a, face, b);
     }
-    return f[lin(c[0], c[1], c[2], d)];
+    return to_f(f[lin(c[0], c[1], c[2], d)]);
 }
 
-// All three components from a packed (x, y, z, unused) float4 field.
-__device__ __forceinline__ float3 load_velocity3(const float4* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& b) {
+// All three components from a packed (x, y, z, unused) field.
+template <typename P>
+__device__ __forceinline__ float3 load_velocity3(const P* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& b) {
     if (inside(x, y, z, d)) {
-        const float4 v = __ldg(&f[lin(x, y, z, d)]);
+        const float4 v = ldg4(&f[lin(x, y, z, d)]);
         return make_float3(v.x, v.y, v.z);
     }
     int c[3] = {x, y, z};
@@ -143,10 +182,10 @@ __device__ __forceinline__ float3 load_velocity3(const float4* __restrict__ f, i
         int q[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) q[k] = clamp_index(c[k], n[k]);
-        const float4 v = __ldg(&f[lin(q[0], q[1], q[2], d)]);
+        const float4 v = ldg4(&f[lin(q[0], q[1], q[2], d)]);
         return make_float3(velocity_ghost(v.x, 0, a, face, b), velocity_ghost(v.y, 1, a, face, b), velocity_ghost(v.z, 2, a, face, b));
     }
-    const float4 v = __ldg(&f[lin(c[0], c[1], c[2], d)]);
+    const float4 v = ldg4(&f[lin(c[0], c[1], c[2], d)]);
     return make_float3(v.x, v.y, v.z);
 }
 
@@ -190,7 +229,8 @@ __device__ __forceinline__ float trilerp(float c000, float c100, float c010, flo
 }
 
 // Velocity (3 components) at a world position from the packed field.
-__device__ __forceinline__ float3 sample_velocity3(const float4* __restrict__ v, float x, float y, float z, const Dims& d, float h, const FlowBC& b) {
+template <typename P>
+__device__ __forceinline__ float3 sample_velocity3(const P* __restrict__ v, float x, float y, float z, const Dims& d, float h, const FlowBC& b) {
     if (b.periodic[0]) x = wrap_world(x, static_cast<float>(d.nx) * h);
     if (b.periodic[1]) y = wrap_world(y, static_cast<float>(d.ny) * h);
     if (b.periodic[2]) z = wrap_world(z, static_cast<float>(d.nz) * h);
@@ -202,7 +242,7 @@ __device__ __forceinline__ float3 sample_velocity3(const float4* __restrict__ v,
         const size_t off[8] = {0, 1, sy, sy + 1, sz, sz + 1, sz + sy, sz + sy + 1};
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const float4 q = __ldg(&v[i + off[k]]);
+            const float4 q = ldg4(&v[i + off[k]]);
             s[k] = make_float3(q.x, q.y, q.z);
         }
     } else {
@@ -215,7 +255,8 @@ __device__ __forceinline__ float3 sample_velocity3(const float4* __restrict__ v,
 }
 
 // Midpoint RK2 back-trace in world units (backend-cuda.cu:295-300).
-__device__ __forceinline__ float3 trace_rk2(float x, float y, float z, const float4* __restrict__ v, float dt, const Dims& d, float h, const FlowBC& b) {
+template <typename P>
+__device__ __forceinline__ float3 trace_rk2(float x, float y, float z, const P* __restrict__ v, float dt, const Dims& d, float h, const FlowBC& b) {
     const float3 v0 = sample_velocity3(v, x, y, z, d, h, b);
     const float mx = x - 0.5f * dt * v0.x;
     const float my = y - 0.5f * dt * v0.y;

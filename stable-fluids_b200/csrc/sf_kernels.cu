@@ -2,10 +2,13 @@
 // packing, fused RK2 advection, divergence, projection with the FP64
 // residual, scalar source/advection, diagnostics.
 //
-// Layout in HBM: every field is a dense x-fastest FP32 array (the layout the
-// ABI views expose); velocity additionally has a packed float4 copy
-// (x, y, z, 0) that the advection gathers read with one 16-byte load per
-// interpolation corner.
+// Layout in HBM: every field is a dense x-fastest array (the layout the ABI
+// views expose); velocity additionally has a packed copy (x, y, z, 0) that
+// the advection gathers read with one load per interpolation corner. The
+// advected fields (velocity, scalar data) are FP32 or, with BF16 storage,
+// BF16 (kernels are templates over the element type T and the packed type P;
+// arithmetic is FP32 either way). Forces, sources, pressure, divergence and
+// |u| are always FP32.
 
 #include <cuda_runtime.h>
 
@@ -36,27 +39,39 @@ __device__ __forceinline__ bool cell_coords(const Dims& d, int& x, int& y, int& 
 }
 
 // ------------------------------------------------------------------ fill --
-__global__ void k_fill(float* __restrict__ f, float value, size_t n) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) f[i] = value;
+template <typename T>
+__global__ void k_fill(T* __restrict__ f, float value, size_t n) {
+    const T v = from_f<T>(value);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) f[i] = v;
+}
+
+// Storage conversions for BF16 contexts (views, updates).
+__global__ void k_bf16_to_f32(float* __restrict__ dst, const __nv_bfloat16* __restrict__ src, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) dst[i] = __bfloat162float(src[i]);
+}
+__global__ void k_f32_to_bf16(__nv_bfloat16* __restrict__ dst, const float* __restrict__ src, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) dst[i] = __float2bfloat16_rn(src[i]);
 }
 
 // ------------------------------------------------------- force + packing --
 // v += dt * f for each force field in order (backend-cuda.cu:310-319 applied
 // field after field), then writes the packed float4 copy.
+template <typename T, typename P>
 __global__ void k_force_pack(ForceArgs a) {
+    T* vel[3] = {static_cast<T*>(a.vel[0]), static_cast<T*>(a.vel[1]), static_cast<T*>(a.vel[2])};
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < a.n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        float vx = a.vel[0][i], vy = a.vel[1][i], vz = a.vel[2][i];
+        float vx = to_f(vel[0][i]), vy = to_f(vel[1][i]), vz = to_f(vel[2][i]);
         for (int k = 0; k < a.force_count; ++k) {
             vx += a.dt * a.force[k][0][i];
             vy += a.dt * a.force[k][1][i];
             vz += a.dt * a.force[k][2][i];
         }
         if (a.write_soa) {
-            a.vel[0][i] = vx;
-            a.vel[1][i] = vy;
-            a.vel[2][i] = vz;
+            vel[0][i] = from_f<T>(vx);
+            vel[1][i] = from_f<T>(vy);
+            vel[2][i] = from_f<T>(vz);
         }
-        if (a.packed) static_cast<float4*>(a.packed)[i] = make_float4(vx, vy, vz, 0.0f);
+        if (a.packed) static_cast<P*>(a.packed)[i] = pack4<P>(vx, vy, vz);
     }
 }
 
@@ -64,7 +79,8 @@ __global__ void k_force_pack(ForceArgs a) {
 // One RK2 trace per cell for all three components (the reference re-traces
 // per component, backend-cuda.cu:330-340; the trace is deterministic so the
 // results are identical), then a trilinear sample of the packed velocity.
-__global__ void __launch_bounds__(256) k_advect_velocity(const float4* __restrict__ v, float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz, float dt, Dims d, float h, FlowBC b) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_advect_velocity(const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) {
     int x, y, z;
     if (!cell_coords(d, x, y, z)) return;
     const float px = (static_cast<float>(x) + 0.5f) * h;
@@ -73,26 +89,28 @@ __global__ void __launch_bounds__(256) k_advect_velocity(const float4* __restric
     const float3 t = trace_rk2(px, py, pz, v, dt, d, h, b);
     const float3 s = sample_velocity3(v, t.x, t.y, t.z, d, h, b);
     const size_t i = lin(x, y, z, d);
-    ox[i] = s.x;
-    oy[i] = s.y;
-    oz[i] = s.z;
+    ox[i] = from_f<T>(s.x);
+    oy[i] = from_f<T>(s.y);
+    oz[i] = from_f<T>(s.z);
 }
 
 // Scalar value after the source injection rho + dt * S at an interior cell,
 // or the fixed face value (the source never reaches a ghost).
-__device__ __forceinline__ float sourced_scalar(const float* __restrict__ q, const float* __restrict__ src, float dt, int x, int y, int z, const Dims& d, const ScalarBC& b) {
+template <typename T>
+__device__ __forceinline__ float sourced_scalar(const T* __restrict__ q, const float* __restrict__ src, float dt, int x, int y, int z, const Dims& d, const ScalarBC& b) {
     if (!inside(x, y, z, d)) {
         float value;
         if (!scalar_resolve(x, y, z, d, b, value)) return value;
     }
     const size_t i = lin(x, y, z, d);
-    return __ldg(&q[i]) + dt * __ldg(&src[i]);
+    return ldg_f(&q[i]) + dt * __ldg(&src[i]);
 }
 
 // Source injection fused into the advection gather (backend-cuda.cu:321-328
 // followed by :342-352): each gathered corner is rho + dt * S, exactly the
 // value the reference stores before it advects.
-__global__ void __launch_bounds__(256) k_scalar_source_advect(const float4* __restrict__ v, const float* __restrict__ q, const float* __restrict__ src, float* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_scalar_source_advect(const P* __restrict__ v, const T* __restrict__ q, const float* __restrict__ src, T* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) {
     int x, y, z;
     if (!cell_coords(d, x, y, z)) return;
     const float px = (static_cast<float>(x) + 0.5f) * h;
@@ -106,20 +124,23 @@ __global__ void __launch_bounds__(256) k_scalar_source_advect(const float4* __re
     float s[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, sb);
-    out[lin(x, y, z, d)] = trilerp(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], c);
+    out[lin(x, y, z, d)] = from_f<T>(trilerp(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], c));
 }
 
-__global__ void k_scalar_source(float* __restrict__ q, const float* __restrict__ src, float dt, size_t n) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] += dt * src[i];
+template <typename T>
+__global__ void k_scalar_source(T* __restrict__ q, const float* __restrict__ src, float dt, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(to_f(q[i]) + dt * src[i]);
 }
 
 // backend-cuda.cu:377-384
-__global__ void k_scale(float* __restrict__ q, float factor, size_t n) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = q[i] * factor;
+template <typename T>
+__global__ void k_scale(T* __restrict__ q, float factor, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(to_f(q[i]) * factor);
 }
 
 // ------------------------------------------------------------ divergence --
-__device__ __forceinline__ float divergence_at(const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, int x, int y, int z, const Dims& d, float h, const FlowBC& b) {
+template <typename T>
+__device__ __forceinline__ float divergence_at(const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, int x, int y, int z, const Dims& d, float h, const FlowBC& b) {
     const float inv_2h = 0.5f / h;
     const float ddx = (load_velocity(vx, 0, x + 1, y, z, d, b) - load_velocity(vx, 0, x - 1, y, z, d, b)) * inv_2h;
     const float ddy = (load_velocity(vy, 1, x, y + 1, z, d, b) - load_velocity(vy, 1, x, y - 1, z, d, b)) * inv_2h;
@@ -128,7 +149,8 @@ __device__ __forceinline__ float divergence_at(const float* __restrict__ vx, con
 }
 
 // backend-cuda.cu:386-396
-__global__ void __launch_bounds__(256) k_divergence(float* __restrict__ div, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, Dims d, float h, FlowBC b) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_divergence(float* __restrict__ div, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
     int x, y, z;
     if (!cell_coords(d, x, y, z)) return;
     div[lin(x, y, z, d)] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
@@ -181,7 +203,8 @@ __device__ __forceinline__ void block_accumulate4(double a, double b, double c, 
 // u -= central gradient of p (backend-cuda.cu:409-422, in place), repacks the
 // float4 velocity for the scalar advection, and (stats != nullptr) adds the
 // FP64 residual terms of A p = b: e = h^2 div - (sum6(p) - 6 p).
-__global__ void __launch_bounds__(256) k_project(float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz, float4* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_project(T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) {
     int x, y, z;
     const bool ok = cell_coords(d, x, y, z);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
@@ -194,13 +217,13 @@ __global__ void __launch_bounds__(256) k_project(float* __restrict__ vx, float* 
         const float grad_x = (pxp - pxm) * inv_2h;
         const float grad_y = (pyp - pym) * inv_2h;
         const float grad_z = (pzp - pzm) * inv_2h;
-        const float ux = vx[i] - grad_x;
-        const float uy = vy[i] - grad_y;
-        const float uz = vz[i] - grad_z;
-        vx[i] = ux;
-        vy[i] = uy;
-        vz[i] = uz;
-        if (packed) packed[i] = make_float4(ux, uy, uz, 0.0f);
+        const float ux = to_f(vx[i]) - grad_x;
+        const float uy = to_f(vy[i]) - grad_y;
+        const float uz = to_f(vz[i]) - grad_z;
+        vx[i] = from_f<T>(ux);
+        vy[i] = from_f<T>(uy);
+        vz[i] = from_f<T>(uz);
+        if (packed) packed[i] = pack4<P>(ux, uy, uz);
         if (stats) {
             const double nb = static_cast<double>(pxm) + static_cast<double>(pxp) + static_cast<double>(pym) + static_cast<double>(pyp) + static_cast<double>(pzm) + static_cast<double>(pzp);
             const double bb = static_cast<double>(h2) * static_cast<double>(div[i]);
@@ -298,55 +321,78 @@ __global__ void k_warm_start_commit(DeviceStats* learned, const DeviceStats* pla
 
 // ----------------------------------------------------------- diagnostics --
 // Post-projection divergence (backend-cuda.cu:670) and |u| (:424-434) in one pass.
-__global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, Dims d, float h, FlowBC b) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
     int x, y, z;
     if (!cell_coords(d, x, y, z)) return;
     const size_t i = lin(x, y, z, d);
     div[i] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
-    const float ux = vx[i], uy = vy[i], uz = vz[i];
+    const float ux = to_f(vx[i]), uy = to_f(vy[i]), uz = to_f(vz[i]);
     mag[i] = sqrtf(ux * ux + uy * uy + uz * uz);
 }
 
 }  // namespace
 
 // ------------------------------------------------------------- launchers --
-cudaError_t launch_fill(float* f, float value, size_t n, cudaStream_t s) {
-    k_fill<<<linear_grid(n, 256), 256, 0, s>>>(f, value, n);
+// Storage dispatch: bf16 selects the BF16 element type (and the 8-byte packed velocity).
+#define SFB_STORAGE(bf16, CALL_F32, CALL_BF16) \
+    do {                                       \
+        if (bf16) {                            \
+            CALL_BF16;                         \
+        } else {                               \
+            CALL_F32;                          \
+        }                                      \
+    } while (0)
+
+using bf16_t = __nv_bfloat16;
+
+cudaError_t launch_fill(void* f, float value, size_t n, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_fill<float><<<linear_grid(n, 256), 256, 0, s>>>(static_cast<float*>(f), value, n)), (k_fill<bf16_t><<<linear_grid(n, 256), 256, 0, s>>>(static_cast<bf16_t*>(f), value, n)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(void* dst, const void* src, size_t n, int to_bf16, cudaStream_t s) {
+    if (to_bf16) k_f32_to_bf16<<<linear_grid(n, 256), 256, 0, s>>>(static_cast<bf16_t*>(dst), static_cast<const float*>(src), n);
+    else k_bf16_to_f32<<<linear_grid(n, 256), 256, 0, s>>>(static_cast<float*>(dst), static_cast<const bf16_t*>(src), n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_force_pack(const ForceArgs& a, cudaStream_t s) {
-    k_force_pack<<<linear_grid(a.n, 256), 256, 0, s>>>(a);
+    SFB_STORAGE(a.bf16, (k_force_pack<float, float4><<<linear_grid(a.n, 256), 256, 0, s>>>(a)), (k_force_pack<bf16_t, Bf16x4><<<linear_grid(a.n, 256), 256, 0, s>>>(a)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_advect_velocity(const void* packed, float* ox, float* oy, float* oz, float dt, Dims d, float h, const FlowBC& b, cudaStream_t s) {
-    k_advect_velocity<<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const float4*>(packed), ox, oy, oz, dt, d, h, b);
+cudaError_t launch_advect_velocity(const void* packed, void* ox, void* oy, void* oz, float dt, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_advect_velocity<float, float4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const float4*>(packed), static_cast<float*>(ox), static_cast<float*>(oy), static_cast<float*>(oz), dt, d, h, b)),
+                (k_advect_velocity<bf16_t, Bf16x4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const Bf16x4*>(packed), static_cast<bf16_t*>(ox), static_cast<bf16_t*>(oy), static_cast<bf16_t*>(oz), dt, d, h, b)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_scalar_source_advect(const void* packed, const float* data, const float* source, float* out, float dt, Dims d, float h, const FlowBC& fb, const ScalarBC& sb, cudaStream_t s) {
-    k_scalar_source_advect<<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const float4*>(packed), data, source, out, dt, d, h, fb, sb);
+cudaError_t launch_scalar_source_advect(const void* packed, const void* data, const float* source, void* out, float dt, Dims d, float h, const FlowBC& fb, const ScalarBC& sb, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_scalar_source_advect<float, float4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const float4*>(packed), static_cast<const float*>(data), source, static_cast<float*>(out), dt, d, h, fb, sb)),
+                (k_scalar_source_advect<bf16_t, Bf16x4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<const Bf16x4*>(packed), static_cast<const bf16_t*>(data), source, static_cast<bf16_t*>(out), dt, d, h, fb, sb)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_scalar_source(float* data, const float* source, float dt, size_t n, cudaStream_t s) {
-    k_scalar_source<<<linear_grid(n, 256), 256, 0, s>>>(data, source, dt, n);
+cudaError_t launch_scalar_source(void* data, const float* source, float dt, size_t n, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_scalar_source<float><<<linear_grid(n, 256), 256, 0, s>>>(static_cast<float*>(data), source, dt, n)), (k_scalar_source<bf16_t><<<linear_grid(n, 256), 256, 0, s>>>(static_cast<bf16_t*>(data), source, dt, n)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_scale(float* data, float factor, size_t n, cudaStream_t s) {
-    k_scale<<<linear_grid(n, 256), 256, 0, s>>>(data, factor, n);
+cudaError_t launch_scale(void* data, float factor, size_t n, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_scale<float><<<linear_grid(n, 256), 256, 0, s>>>(static_cast<float*>(data), factor, n)), (k_scale<bf16_t><<<linear_grid(n, 256), 256, 0, s>>>(static_cast<bf16_t*>(data), factor, n)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_divergence(float* div, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s) {
-    k_divergence<<<cell_grid(d), cell_block(), 0, s>>>(div, vx, vy, vz, d, h, b);
+cudaError_t launch_divergence(float* div, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_divergence<float><<<cell_grid(d), cell_block(), 0, s>>>(div, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), d, h, b)),
+                (k_divergence<bf16_t><<<cell_grid(d), cell_block(), 0, s>>>(div, static_cast<const bf16_t*>(vx), static_cast<const bf16_t*>(vy), static_cast<const bf16_t*>(vz), d, h, b)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_project(float* vx, float* vy, float* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
-    k_project<<<cell_grid(d), cell_block(), 0, s>>>(vx, vy, vz, static_cast<float4*>(packed), p, div, d, h, h2, b, stats);
+cudaError_t launch_project(void* vx, void* vy, void* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_project<float, float4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<float*>(vx), static_cast<float*>(vy), static_cast<float*>(vz), static_cast<float4*>(packed), p, div, d, h, h2, b, stats)),
+                (k_project<bf16_t, Bf16x4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<bf16_t*>(vx), static_cast<bf16_t*>(vy), static_cast<bf16_t*>(vz), static_cast<Bf16x4*>(packed), p, div, d, h, h2, b, stats)));
     return cudaGetLastError();
 }
 
@@ -376,8 +422,9 @@ cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* pl
     return cudaGetLastError();
 }
 
-cudaError_t launch_post_diagnostics(float* div, float* mag, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s) {
-    k_post_diagnostics<<<cell_grid(d), cell_block(), 0, s>>>(div, mag, vx, vy, vz, d, h, b);
+cudaError_t launch_post_diagnostics(float* div, float* mag, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s) {
+    SFB_STORAGE(bf16, (k_post_diagnostics<float><<<cell_grid(d), cell_block(), 0, s>>>(div, mag, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), d, h, b)),
+                (k_post_diagnostics<bf16_t><<<cell_grid(d), cell_block(), 0, s>>>(div, mag, static_cast<const bf16_t*>(vx), static_cast<const bf16_t*>(vy), static_cast<const bf16_t*>(vz), d, h, b)));
     return cudaGetLastError();
 }
 

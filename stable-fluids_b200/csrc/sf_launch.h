@@ -12,13 +12,14 @@ namespace sfb {
 constexpr int kMaxForcesPerLaunch = 8;
 
 struct ForceArgs {
-    float* vel[3];                          // SoA velocity (read; written when write_soa)
+    void* vel[3];                           // SoA velocity, FP32 or BF16 (read; written when write_soa)
     const float* force[kMaxForcesPerLaunch][3];
     int force_count;
     float dt;
     size_t n;
-    void* packed;                           // float4 velocity (written when non-null)
+    void* packed;                           // packed velocity, float4 or 4 x BF16 (written when non-null)
     int write_soa;
+    int bf16;                               // advected fields stored in BF16
 };
 
 // How a stencil solve obtains its initial iterate.
@@ -34,8 +35,8 @@ struct StencilArgs {
     int per_pass;        // iterations fused per HBM pass (temporal blocking); 0 = automatic
     float coef;          // alpha (diffusion) or h^2 (pressure)
     float out_scale;     // multiply the final iterate by this (1 = none)
-    float* x;            // the iterate (result lands here)
-    const float* b;      // right-hand side (diffusion: advected field; pressure: divergence)
+    float* x;            // the iterate (result lands here); BF16 elements when bf16
+    const float* b;      // right-hand side (diffusion: advected field; pressure: divergence); BF16 when bf16
     float* scratch;      // a field-sized buffer for out-of-place sweeps
     Dims dims;
     FlowBC flow;
@@ -43,19 +44,23 @@ struct StencilArgs {
     int* launches;       // incremented by the number of kernels enqueued (may be null)
     int blocked;         // 1: temporally blocked passes where supported; 0: one launch per sweep
     unsigned* error_flag;  // device word a kernel sets when a bounded wait gives up
+    int bf16;            // x, b, scratch hold BF16 (diffusion kinds of a BF16-storage context)
 };
 
-cudaError_t launch_fill(float* f, float value, size_t n, cudaStream_t s);
+// `bf16` arguments: the advected field arrays passed are BF16 (else FP32).
+cudaError_t launch_fill(void* f, float value, size_t n, int bf16, cudaStream_t s);
+// FP32 -> BF16 (to_bf16) or BF16 -> FP32 element conversion.
+cudaError_t launch_convert(void* dst, const void* src, size_t n, int to_bf16, cudaStream_t s);
 cudaError_t launch_force_pack(const ForceArgs& a, cudaStream_t s);
-cudaError_t launch_advect_velocity(const void* packed, float* out_x, float* out_y, float* out_z, float dt, Dims d, float h, const FlowBC& b, cudaStream_t s);
-cudaError_t launch_scalar_source_advect(const void* packed, const float* data, const float* source, float* out, float dt, Dims d, float h, const FlowBC& fb, const ScalarBC& sb, cudaStream_t s);
-cudaError_t launch_scalar_source(float* data, const float* source, float dt, size_t n, cudaStream_t s);
-cudaError_t launch_scale(float* data, float factor, size_t n, cudaStream_t s);
+cudaError_t launch_advect_velocity(const void* packed, void* out_x, void* out_y, void* out_z, float dt, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s);
+cudaError_t launch_scalar_source_advect(const void* packed, const void* data, const float* source, void* out, float dt, Dims d, float h, const FlowBC& fb, const ScalarBC& sb, int bf16, cudaStream_t s);
+cudaError_t launch_scalar_source(void* data, const float* source, float dt, size_t n, int bf16, cudaStream_t s);
+cudaError_t launch_scale(void* data, float factor, size_t n, int bf16, cudaStream_t s);
 cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s);
-cudaError_t launch_divergence(float* div, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s);
+cudaError_t launch_divergence(float* div, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s);
 // u -= grad p (in place) and repack; with stats != nullptr also accumulates
 // the FP64 residual sums of the pressure system into stats.
-cudaError_t launch_project(float* vx, float* vy, float* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
+cudaError_t launch_project(void* vx, void* vy, void* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, int bf16, cudaStream_t s);
 cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
 // The same sums with the vectorised z-marching layout; false (nothing
 // launched) when the grid or the pointers do not suit it (nx % 4, 16-byte
@@ -67,6 +72,6 @@ cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int 
 // Learned warm start: keeps the candidate in p or replaces it by alt,
 // whichever has the smaller relative residual (two kernels).
 cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* plain, Dims d, int singular, float* p, const float* alt, cudaStream_t s);
-cudaError_t launch_post_diagnostics(float* div, float* mag, const float* vx, const float* vy, const float* vz, Dims d, float h, const FlowBC& b, cudaStream_t s);
+cudaError_t launch_post_diagnostics(float* div, float* mag, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s);
 
 }  // namespace sfb

@@ -23,9 +23,9 @@ namespace sfb {
 
 namespace {
 
-template <int KIND>
-__device__ __forceinline__ float neighbour(const float* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& fb, const ScalarBC& sb) {
-    if constexpr (KIND == KIND_PRESSURE) return load_pressure(f, x, y, z, d, fb);
+template <int KIND, typename T>
+__device__ __forceinline__ float neighbour(const T* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& fb, const ScalarBC& sb) {
+    if constexpr (KIND == KIND_PRESSURE) return load_pressure(reinterpret_cast<const float*>(f), x, y, z, d, fb);
     else if constexpr (KIND == KIND_SCALAR) return load_scalar(f, x, y, z, d, sb);
     else return load_velocity(f, KIND, x, y, z, d, fb);
 }
@@ -36,8 +36,8 @@ __device__ __forceinline__ float update(float nb, float rhs, float coef) {
     else return (rhs + coef * nb) / (1.0f + 6.0f * coef);
 }
 
-template <int KIND>
-__device__ __forceinline__ float neighbour_sum(const float* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& fb, const ScalarBC& sb) {
+template <int KIND, typename T>
+__device__ __forceinline__ float neighbour_sum(const T* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& fb, const ScalarBC& sb) {
     return neighbour<KIND>(f, x - 1, y, z, d, fb, sb) + neighbour<KIND>(f, x + 1, y, z, d, fb, sb) + neighbour<KIND>(f, x, y - 1, z, d, fb, sb) + neighbour<KIND>(f, x, y + 1, z, d, fb, sb) + neighbour<KIND>(f, x, y, z - 1, d, fb, sb)
          + neighbour<KIND>(f, x, y, z + 1, d, fb, sb);
 }
@@ -51,8 +51,8 @@ __device__ __forceinline__ float neighbour_sum(const float* __restrict__ f, int 
 // reference's ghost rules.
 constexpr int kColourPlanes = 4;
 
-template <int KIND>
-__global__ void __launch_bounds__(256) k_rbgs_colour(float* x, const float* __restrict__ rhs, float coef, int parity, Dims d, FlowBC fb, ScalarBC sb) {
+template <int KIND, typename T = float>
+__global__ void __launch_bounds__(256) k_rbgs_colour(T* x, const T* __restrict__ rhs, float coef, int parity, Dims d, FlowBC fb, ScalarBC sb) {
     const int hx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
     const int z0 = static_cast<int>(blockIdx.z) * kColourPlanes;
@@ -73,26 +73,26 @@ __global__ void __launch_bounds__(256) k_rbgs_colour(float* x, const float* __re
         if (ok[k]) {
             const bool interior = cx >= 1 && cx <= d.nx - 2 && y >= 1 && y <= d.ny - 2 && z >= 1 && z <= d.nz - 2;
             if (interior) {
-                const float* c = x + idx[k];
-                nb = c[-1] + c[1] + c[-static_cast<ptrdiff_t>(sy)] + c[sy] + c[-static_cast<ptrdiff_t>(sz)] + c[sz];
+                const T* c = x + idx[k];
+                nb = to_f(c[-1]) + to_f(c[1]) + to_f(c[-static_cast<ptrdiff_t>(sy)]) + to_f(c[sy]) + to_f(c[-static_cast<ptrdiff_t>(sz)]) + to_f(c[sz]);
             } else {
                 nb = neighbour_sum<KIND>(x, cx, y, z, d, fb, sb);
             }
         }
-        num[k] = tb::numerator<KIND>(nb, ok[k] ? rhs[idx[k]] : 0.0f, coef);
+        num[k] = tb::numerator<KIND>(nb, ok[k] ? to_f(rhs[idx[k]]) : 0.0f, coef);
     }
 #pragma unroll
     for (int k = 0; k < kColourPlanes; ++k) {
         if (!ok[k]) continue;
-        x[idx[k]] = tb::update_div<KIND>(num[k], divisor, recip);
+        x[idx[k]] = from_f<T>(tb::update_div<KIND>(num[k], divisor, recip));
     }
 }
 
 // One Jacobi sweep, dst = update(src): thread (x, y) owns the cells of
 // kColourPlanes consecutive planes; interior cells read their neighbours
 // directly, boundary cells use the ghost rules.
-template <int KIND>
-__global__ void __launch_bounds__(256) k_jacobi(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, Dims d, FlowBC fb, ScalarBC sb) {
+template <int KIND, typename T = float>
+__global__ void __launch_bounds__(256) k_jacobi(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ rhs, float coef, Dims d, FlowBC fb, ScalarBC sb) {
     const int cx = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
     const int z0 = static_cast<int>(blockIdx.z) * kColourPlanes;
@@ -108,13 +108,13 @@ __global__ void __launch_bounds__(256) k_jacobi(float* __restrict__ dst, const f
         const size_t i = lin(cx, y, z, d);
         float nb;
         if (xy_interior && z >= 1 && z <= d.nz - 2) {
-            const float* c = src + i;
-            nb = c[-1] + c[1] + c[-static_cast<ptrdiff_t>(sy)] + c[sy] + c[-static_cast<ptrdiff_t>(sz)] + c[sz];
+            const T* c = src + i;
+            nb = to_f(c[-1]) + to_f(c[1]) + to_f(c[-static_cast<ptrdiff_t>(sy)]) + to_f(c[sy]) + to_f(c[-static_cast<ptrdiff_t>(sz)]) + to_f(c[sz]);
         } else {
             nb = neighbour_sum<KIND>(src, cx, y, z, d, fb, sb);
         }
-        const float num = tb::numerator<KIND>(nb, rhs[i], coef);
-        dst[i] = tb::update_div<KIND>(num, divisor, recip);
+        const float num = tb::numerator<KIND>(nb, to_f(rhs[i]), coef);
+        dst[i] = from_f<T>(tb::update_div<KIND>(num, divisor, recip));
     }
 }
 
@@ -129,15 +129,215 @@ __global__ void __launch_bounds__(256) k_jacobi(float* __restrict__ dst, const f
 // with selects, so boundary threads take the same path as interior ones.
 // Arithmetic, neighbour order and division are those of k_rbgs_colour /
 // k_jacobi, so results are bit-identical.
+// A thread owns W consecutive cells of a row held in one 16-byte vector:
+// W = 4 for FP32 fields (the float4 kernels further down), W = 8 for BF16
+// fields (the generic W-cell kernels here, 8 BF16 per vector).
+template <typename T>
+struct VecWidth {
+    static constexpr int W = sizeof(T) == 2 ? 8 : 4;
+};
+template <int W>
+struct Row {
+    float v[W];
+};
+
+__device__ __forceinline__ void loadv(const __nv_bfloat16* p, Row<8>& r) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[k]));
+        r.v[2 * k] = f.x;
+        r.v[2 * k + 1] = f.y;
+    }
+}
+__device__ __forceinline__ void storev(__nv_bfloat16* p, const Row<8>& r) {
+    uint32_t w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(r.v[2 * k], r.v[2 * k + 1]);
+        w[k] = *reinterpret_cast<uint32_t*>(&h);
+    }
+    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+__device__ __forceinline__ float ld1(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+
+template <int W>
+__device__ __forceinline__ Row<W> ghostv(const GhostRule& g, int face, const Row<W>& self) {
+    Row<W> r;
+#pragma unroll
+    for (int k = 0; k < W; ++k) r.v[k] = tb::ghost(g, face, self.v[k]);
+    return r;
+}
+
 struct VecGhost {
+    int ox_lo, ox_hi;  // offsets of the row's x- / x+ neighbours from x0 (wrap or self on a face)
+    int oy_lo, oy_hi;  // y offsets of the y- / y+ rows
+    bool gx_lo, gx_hi, gy_lo, gy_hi;  // apply the face ghost
+};
+
+template <int W>
+__device__ __forceinline__ VecGhost vec_ghost(int x0, int y, const Dims& d, const GhostRule& g) {
+    const int sy = d.nx;
+    VecGhost v{-1, W, -sy, sy, false, false, false, false};
+    if (x0 == 0) {
+        v.ox_lo = g.periodic[0] ? d.nx - 1 : 0;
+        v.gx_lo = !g.periodic[0];
+    }
+    if (x0 + W == d.nx) {
+        v.ox_hi = g.periodic[0] ? -x0 : W - 1;
+        v.gx_hi = !g.periodic[0];
+    }
+    if (y == 0) {
+        v.oy_lo = g.periodic[1] ? (d.ny - 1) * sy : 0;
+        v.gy_lo = !g.periodic[1];
+    }
+    if (y == d.ny - 1) {
+        v.oy_hi = g.periodic[1] ? -(d.ny - 1) * sy : 0;
+        v.gy_hi = !g.periodic[1];
+    }
+    return v;
+}
+
+template <int KIND>
+__device__ __forceinline__ float vec_update(float nb, float rhs, float coef, float divisor, float recip) {
+    return tb::update_div<KIND>(tb::numerator<KIND>(nb, rhs, coef), divisor, recip);
+}
+
+// The plane below the chunk's first plane (or its ghost at z = 0).
+template <typename T, int W>
+__device__ __forceinline__ Row<W> vec_below(const T* x, int i, int z, const Dims& d, const GhostRule& g, const Row<W>& cur) {
+    const int sz = d.nx * d.ny;
+    Row<W> r;
+    if (z > 0) loadv(x + i - sz, r);
+    else if (g.periodic[2]) loadv(x + i + (d.nz - 1) * sz, r);
+    else r = ghostv<W>(g, ZM, cur);
+    return r;
+}
+
+template <typename T, int W>
+__device__ __forceinline__ Row<W> vec_above(const T* x, int i, int z, const Dims& d, const GhostRule& g, const Row<W>& cur) {
+    const int sz = d.nx * d.ny;
+    Row<W> r;
+    if (z + 1 < d.nz) loadv(x + i + sz, r);
+    else if (g.periodic[2]) loadv(x + i - (d.nz - 1) * sz, r);
+    else r = ghostv<W>(g, ZP, cur);
+    return r;
+}
+
+// Neighbours of the W cells of a row: x- / x+ (from the row itself and the
+// two single loads at its ends), y- / y+ rows, with face ghosts applied.
+template <typename T, int W>
+struct RowNeighbours {
+    float a, b;     // x- neighbour of cell 0, x+ neighbour of cell W - 1
+    Row<W> c, e;    // y- and y+ rows
+};
+
+template <typename T, int W>
+__device__ __forceinline__ RowNeighbours<T, W> row_neighbours(const T* x, int i, const VecGhost& v, const GhostRule& g) {
+    RowNeighbours<T, W> n;
+    n.a = ld1(x + i + v.ox_lo);
+    n.b = ld1(x + i + v.ox_hi);
+    loadv(x + i + v.oy_lo, n.c);
+    loadv(x + i + v.oy_hi, n.e);
+    if (v.gx_lo) n.a = tb::ghost(g, XM, n.a);
+    if (v.gx_hi) n.b = tb::ghost(g, XP, n.b);
+    if (v.gy_lo) n.c = ghostv<W>(g, YM, n.c);
+    if (v.gy_hi) n.e = ghostv<W>(g, YP, n.e);
+    return n;
+}
+
+constexpr int kVecRows = 4;  // rows per CTA; 32 x kVecRows threads
+
+// One Jacobi sweep dst = update(src).
+template <int KIND, typename T = float>
+__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vecw(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    constexpr int W = VecWidth<T>::W;
+    const int x0 = W * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    if (x0 >= d.nx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    const VecGhost v = vec_ghost<W>(x0, y, d, g);
+    const int sz = d.nx * d.ny;
+    int i = x0 + d.nx * (y + d.ny * zb);
+    Row<W> cur;
+    loadv(src + i, cur);
+    Row<W> below = vec_below<T, W>(src, i, zb, d, g, cur);
+#pragma unroll 2
+    for (int z = zb; z < ze; ++z, i += sz) {
+        const Row<W> above = vec_above<T, W>(src, i, z, d, g, cur);
+        const RowNeighbours<T, W> n = row_neighbours<T, W>(src, i, v, g);
+        Row<W> r;
+        loadv(rhs + i, r);
+        Row<W> o;
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const float xm = k == 0 ? n.a : cur.v[k - 1];
+            const float xp = k == W - 1 ? n.b : cur.v[k + 1];
+            o.v[k] = vec_update<KIND>(xm + xp + n.c.v[k] + n.e.v[k] + below.v[k] + above.v[k], r.v[k], coef, divisor, recip);
+        }
+        storev(dst + i, o);
+        below = cur;
+        cur = above;
+    }
+}
+
+// One colour of an RBGS iteration, in place: in each row of W cells the W/2
+// cells with (x + y + z + parity) even are updated; the others are stored
+// back unchanged (no thread of this launch changes them, so rewriting the
+// value just read is harmless and keeps every store a full 16 bytes).
+template <int KIND, typename T = float>
+__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vecw(T* x, const T* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+    constexpr int W = VecWidth<T>::W;
+    const int x0 = W * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    if (x0 >= d.nx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const float recip = 1.0f / divisor;
+    const VecGhost v = vec_ghost<W>(x0, y, d, g);
+    const int sz = d.nx * d.ny;
+    int i = x0 + d.nx * (y + d.ny * zb);
+    Row<W> cur;
+    loadv(x + i, cur);
+    Row<W> below = vec_below<T, W>(x, i, zb, d, g, cur);
+#pragma unroll 2
+    for (int z = zb; z < ze; ++z, i += sz) {
+        const Row<W> above = vec_above<T, W>(x, i, z, d, g, cur);
+        const RowNeighbours<T, W> n = row_neighbours<T, W>(x, i, v, g);
+        Row<W> r;
+        loadv(rhs + i, r);
+        const int first = (y + z + parity) & 1;  // cells first, first + 2, ... are updated
+        Row<W> o = cur;
+#pragma unroll
+        for (int m = 0; m < W / 2; ++m) {
+            // selects keep the loop free of divergence: cell k = 2 m + first
+            const float xm = first ? cur.v[2 * m] : (m == 0 ? n.a : cur.v[2 * m - 1]);
+            const float xp = first ? (m == W / 2 - 1 ? n.b : cur.v[2 * m + 2]) : cur.v[2 * m + 1];
+            const float ym = first ? n.c.v[2 * m + 1] : n.c.v[2 * m], yp = first ? n.e.v[2 * m + 1] : n.e.v[2 * m];
+            const float zm = first ? below.v[2 * m + 1] : below.v[2 * m], zp = first ? above.v[2 * m + 1] : above.v[2 * m];
+            const float q = vec_update<KIND>(xm + xp + ym + yp + zm + zp, first ? r.v[2 * m + 1] : r.v[2 * m], coef, divisor, recip);
+            if (first) o.v[2 * m + 1] = q;
+            else o.v[2 * m] = q;
+        }
+        storev(x + i, o);
+        below = cur;
+        cur = above;
+    }
+}
+
+// ---- FP32 fields: float4 rows (4 cells per thread) ----------------------
+// The FP32 kernels keep a hand-specialised float4 form; the generic W-cell
+// kernels above serve the BF16 storage.
+struct VecGhost4 {
     int ox_lo, ox_hi;  // x offsets of the row's x- / x+ neighbours from x0 (wrap or self on a face)
     int oy_lo, oy_hi;  // y offsets of the y- / y+ rows
     bool gx_lo, gx_hi, gy_lo, gy_hi;  // apply the face ghost
 };
 
-__device__ __forceinline__ VecGhost vec_ghost(int x0, int y, const Dims& d, const GhostRule& g) {
+__device__ __forceinline__ VecGhost4 vec_ghost4(int x0, int y, const Dims& d, const GhostRule& g) {
     const int sy = d.nx;
-    VecGhost v{-1, 4, -sy, sy, false, false, false, false};
+    VecGhost4 v{-1, 4, -sy, sy, false, false, false, false};
     if (x0 == 0) {
         v.ox_lo = g.periodic[0] ? d.nx - 1 : 0;
         v.gx_lo = !g.periodic[0];
@@ -163,44 +363,39 @@ __device__ __forceinline__ float4 ghost4(const GhostRule& g, int face, float4 se
     return make_float4(tb::ghost(g, face, self.x), tb::ghost(g, face, self.y), tb::ghost(g, face, self.z), tb::ghost(g, face, self.w));
 }
 
-template <int KIND>
-__device__ __forceinline__ float vec_update(float nb, float rhs, float coef, float divisor, float recip) {
-    return tb::update_div<KIND>(tb::numerator<KIND>(nb, rhs, coef), divisor, recip);
-}
 
 // The plane below the chunk's first plane (or its ghost at z = 0).
-__device__ __forceinline__ float4 vec_below(const float* x, int i, int z, const Dims& d, const GhostRule& g, float4 cur) {
+__device__ __forceinline__ float4 vec_below4(const float* x, int i, int z, const Dims& d, const GhostRule& g, float4 cur) {
     const int sz = d.nx * d.ny;
     if (z > 0) return ld4(x + i - sz);
     if (g.periodic[2]) return ld4(x + i + (d.nz - 1) * sz);
     return ghost4(g, ZM, cur);
 }
 
-__device__ __forceinline__ float4 vec_above(const float* x, int i, int z, const Dims& d, const GhostRule& g, float4 cur) {
+__device__ __forceinline__ float4 vec_above4(const float* x, int i, int z, const Dims& d, const GhostRule& g, float4 cur) {
     const int sz = d.nx * d.ny;
     if (z + 1 < d.nz) return ld4(x + i + sz);
     if (g.periodic[2]) return ld4(x + i - (d.nz - 1) * sz);
     return ghost4(g, ZP, cur);
 }
 
-constexpr int kVecRows = 4;  // rows per CTA; 32 x kVecRows threads
 
 // One Jacobi sweep dst = update(src).
 template <int KIND>
-__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
     const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const float recip = 1.0f / divisor;
-    const VecGhost v = vec_ghost(x0, y, d, g);
+    const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
     int i = x0 + d.nx * (y + d.ny * zb);
     float4 cur = ld4(src + i);
-    float4 below = vec_below(src, i, zb, d, g, cur);
+    float4 below = vec_below4(src, i, zb, d, g, cur);
 #pragma unroll 2
     for (int z = zb; z < ze; ++z, i += sz) {
-        const float4 above = vec_above(src, i, z, d, g, cur);
+        const float4 above = vec_above4(src, i, z, d, g, cur);
         float a = src[i + v.ox_lo], b = src[i + v.ox_hi];
         float4 c = ld4(src + i + v.oy_lo), e = ld4(src + i + v.oy_hi);
         const float4 r = ld4(rhs + i);
@@ -224,20 +419,20 @@ __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec(float* __restrict_
 // unchanged (no thread of this launch changes them, so rewriting the value
 // just read is harmless and keeps every store a full 16 bytes).
 template <int KIND>
-__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec(float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
     const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const float recip = 1.0f / divisor;
-    const VecGhost v = vec_ghost(x0, y, d, g);
+    const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
     int i = x0 + d.nx * (y + d.ny * zb);
     float4 cur = ld4(x + i);
-    float4 below = vec_below(x, i, zb, d, g, cur);
+    float4 below = vec_below4(x, i, zb, d, g, cur);
 #pragma unroll 2
     for (int z = zb; z < ze; ++z, i += sz) {
-        const float4 above = vec_above(x, i, z, d, g, cur);
+        const float4 above = vec_above4(x, i, z, d, g, cur);
         float a = x[i + v.ox_lo], b = x[i + v.ox_hi];
         float4 c = ld4(x + i + v.oy_lo), e = ld4(x + i + v.oy_hi);
         const float4 r = ld4(rhs + i);
@@ -266,7 +461,7 @@ struct VecShape {
 };
 
 template <typename Kernel>
-VecShape vec_shape(const Dims& d, Kernel kernel) {
+VecShape vec_shape(const Dims& d, Kernel kernel, int width = 4) {
     static int per_sm = [&] {
         int n = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 32 * kVecRows, 0) != cudaSuccess || n < 1) n = 4;
@@ -275,7 +470,7 @@ VecShape vec_shape(const Dims& d, Kernel kernel) {
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int bx = (d.nx / 4 + 31) / 32, by = (d.ny + kVecRows - 1) / kVecRows;
+    const int bx = (d.nx / width + 31) / 32, by = (d.ny + kVecRows - 1) / kVecRows;
     const long long slots = static_cast<long long>(sms) * per_sm;
     long long chunks = slots / (static_cast<long long>(bx) * by);  // one wave: every CTA resident at once
     if (chunks < 1) chunks = 1;
@@ -285,10 +480,10 @@ VecShape vec_shape(const Dims& d, Kernel kernel) {
     return {dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), static_cast<unsigned>(bz)), z_chunk};
 }
 
-bool vec_ok(const StencilArgs& a) {
+bool vec_ok(const StencilArgs& a, int width = 4) {
     const auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
     const size_t cells = static_cast<size_t>(a.dims.nx) * a.dims.ny * a.dims.nz;
-    return a.dims.nx % 4 == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
+    return a.dims.nx % width == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
 }
 
 // Two Jacobi sweeps per pass (temporal blocking): a CTA owns a TX x TY
@@ -435,13 +630,13 @@ __global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __r
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
     if (x0 < d.nx && y < d.ny) {
         const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
-        const VecGhost v = vec_ghost(x0, y, d, g);
+        const VecGhost4 v = vec_ghost4(x0, y, d, g);
         const int sz = d.nx * d.ny;
         int i = x0 + d.nx * (y + d.ny * zb);
         float4 cur = ld4(p + i);
-        float4 below = vec_below(p, i, zb, d, g, cur);
+        float4 below = vec_below4(p, i, zb, d, g, cur);
         for (int z = zb; z < ze; ++z, i += sz) {
-            const float4 above = vec_above(p, i, z, d, g, cur);
+            const float4 above = vec_above4(p, i, z, d, g, cur);
             float a = p[i + v.ox_lo], b = p[i + v.ox_hi];
             float4 c = ld4(p + i + v.oy_lo), e = ld4(p + i + v.oy_hi);
             const float4 r = ld4(div + i);
@@ -488,8 +683,9 @@ __global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __r
     }
 }
 
-__global__ void k_scale_field(float* __restrict__ q, float factor, size_t n) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = q[i] * factor;
+template <typename T = float>
+__global__ void k_scale_field(T* __restrict__ q, float factor, size_t n) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(to_f(q[i]) * factor);
 }
 
 struct TbShape2 {
@@ -518,75 +714,102 @@ TbShape2 tb2_shape(const Dims& d, Kernel kernel) {
 
 GhostRule ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb);
 
-template <int KIND>
+// Vectorised sweep kernels per element type: the float4 kernels for FP32
+// fields, the 8-cell kernels for BF16 fields.
+template <int KIND, typename T>
+auto jacobi_vec_kernel() {
+    if constexpr (sizeof(T) == sizeof(float)) return k_jacobi_vec4<KIND>;
+    else return k_jacobi_vecw<KIND, T>;
+}
+
+template <int KIND, typename T>
+auto rbgs_vec_kernel() {
+    if constexpr (sizeof(T) == sizeof(float)) return k_rbgs_vec4<KIND>;
+    else return k_rbgs_vecw<KIND, T>;
+}
+
+// T: element type of x, b and scratch (BF16 only for the diffusion kinds of a
+// BF16-storage context; the pressure is always FP32).
+template <int KIND, typename T>
 cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
     const Dims& d = a.dims;
     const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
-    const size_t bytes = n * sizeof(float);
-    const dim3 block(32, 4, 2);
+    const size_t bytes = n * sizeof(T);
+    T* const ax = reinterpret_cast<T*>(a.x);
+    T* const ascr = reinterpret_cast<T*>(a.scratch);
+    const T* const ab = reinterpret_cast<const T*>(a.b);
     cudaError_t e = cudaSuccess;
     if (a.scheme == SCHEME_RBGS) {
-        if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(a.x, a.b, bytes, cudaMemcpyDeviceToDevice, s);
-        else if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
+        if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(ax, ab, bytes, cudaMemcpyDeviceToDevice, s);
+        else if (a.init == INIT_ZERO) e = cudaMemsetAsync(ax, 0, bytes, s);
         if (e != cudaSuccess) return e;
-        if (vec_ok(a)) {
+        if (vec_ok(a, VecWidth<T>::W)) {
             const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
-            const VecShape vs = vec_shape(d, k_rbgs_vec<KIND>);
+            const auto kernel = rbgs_vec_kernel<KIND, T>();
+            const VecShape vs = vec_shape(d, kernel, VecWidth<T>::W);
             for (int it = 0; it < a.iterations; ++it)
-                for (int parity = 0; parity < 2; ++parity) k_rbgs_vec<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(a.x, a.b, a.coef, parity, vs.z_chunk, d, g);
+                for (int parity = 0; parity < 2; ++parity) kernel<<<vs.grid, dim3(32, kVecRows), 0, s>>>(ax, ab, a.coef, parity, vs.z_chunk, d, g);
         } else {
             const dim3 cblock(32, 8, 1);
             const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
             for (int it = 0; it < a.iterations; ++it)
-                for (int parity = 0; parity < 2; ++parity) k_rbgs_colour<KIND><<<grid, cblock, 0, s>>>(a.x, a.b, a.coef, parity, d, a.flow, a.scalar);
+                for (int parity = 0; parity < 2; ++parity) k_rbgs_colour<KIND, T><<<grid, cblock, 0, s>>>(ax, ab, a.coef, parity, d, a.flow, a.scalar);
         }
         if (a.launches) *a.launches += 2 * a.iterations;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
-        const bool vec = vec_ok(a);
+        const bool vec = vec_ok(a, VecWidth<T>::W);
         const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
-        const VecShape vs = vec ? vec_shape(d, k_jacobi_vec<KIND>) : VecShape{};
+        const auto jacobi_vec = jacobi_vec_kernel<KIND, T>();
+        const VecShape vs = vec ? vec_shape(d, jacobi_vec, VecWidth<T>::W) : VecShape{};
         const dim3 jblock(32, 8, 1);
         const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
-        // With blocking requested, sweeps go two per pass (k_jacobi_tb2) where
-        // the grid suits the vectorised kernels, an odd sweep first as a
-        // single sweep. (On B200 the single-sweep kernel is faster today.)
-        const int pairs = (vec && a.blocked) ? a.iterations / 2 : 0;
+        // With blocking requested, sweeps go two per pass (k_jacobi_tb2, FP32)
+        // where the grid suits the vectorised kernels, an odd sweep first as
+        // a single sweep. (On B200 the single-sweep kernel is faster today.)
+        constexpr bool kFp32 = sizeof(T) == sizeof(float);
+        const int pairs = (kFp32 && vec && a.blocked) ? a.iterations / 2 : 0;
         const int singles = a.iterations - 2 * pairs;
         const int units = pairs + singles;
-        const TbShape2 tb = pairs > 0 ? tb2_shape(d, k_jacobi_tb2<KIND>) : TbShape2{};
+        TbShape2 tb{};
+        if constexpr (kFp32)
+            if (pairs > 0) tb = tb2_shape(d, k_jacobi_tb2<KIND>);
         // Choose the first source so that the last launch lands in x.
-        const float* src = a.x;
-        if (a.init == INIT_FROM_B) src = a.b;
+        const T* src = ax;
+        if (a.init == INIT_FROM_B) src = ab;
         else if (a.init == INIT_ZERO) {
             // Zero the buffer the first launch does not write.
-            float* zero = (units & 1) ? a.scratch : a.x;
+            T* zero = (units & 1) ? ascr : ax;
             if ((e = cudaMemsetAsync(zero, 0, bytes, s)) != cudaSuccess) return e;
             src = zero;
         }
         if (a.iterations == 0) {
-            if (src != a.x) e = cudaMemcpyAsync(a.x, src, bytes, cudaMemcpyDeviceToDevice, s);
+            if (src != ax) e = cudaMemcpyAsync(ax, src, bytes, cudaMemcpyDeviceToDevice, s);
             if (e != cudaSuccess) return e;
         }
         for (int u = 0; u < units; ++u) {
             const int left = units - u;  // launches still to run, this one included
-            float* dst = (left & 1) ? a.x : a.scratch;
-            if (dst == src) dst = (dst == a.x) ? a.scratch : a.x;
-            if (u >= singles) k_jacobi_tb2<KIND><<<tb.grid, kTbThreads, 0, s>>>(dst, src, a.b, a.coef, tb.z_chunk, d, g);
-            else if (vec) k_jacobi_vec<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
-            else k_jacobi<KIND><<<grid, jblock, 0, s>>>(dst, src, a.b, a.coef, d, a.flow, a.scalar);
+            T* dst = (left & 1) ? ax : ascr;
+            if (dst == src) dst = (dst == ax) ? ascr : ax;
+            if (u >= singles) {
+                if constexpr (kFp32) k_jacobi_tb2<KIND><<<tb.grid, kTbThreads, 0, s>>>(dst, src, ab, a.coef, tb.z_chunk, d, g);
+            } else if (vec) {
+                jacobi_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, ab, a.coef, vs.z_chunk, d, g);
+            } else {
+                k_jacobi<KIND, T><<<grid, jblock, 0, s>>>(dst, src, ab, a.coef, d, a.flow, a.scalar);
+            }
             src = dst;
         }
         if (a.launches) *a.launches += units;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (src != a.x && a.iterations > 0) {
-            if ((e = cudaMemcpyAsync(a.x, src, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+        if (src != ax && a.iterations > 0) {
+            if ((e = cudaMemcpyAsync(ax, src, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
         }
     }
     if (a.out_scale != 1.0f) {
         size_t g = (n + 255) / 256;
         if (g > 148u * 32u) g = 148u * 32u;
-        k_scale_field<<<static_cast<unsigned>(g), 256, 0, s>>>(a.x, a.out_scale, n);
+        k_scale_field<T><<<static_cast<unsigned>(g), 256, 0, s>>>(ax, a.out_scale, n);
         e = cudaGetLastError();
         if (a.launches) *a.launches += 1;
     }
@@ -754,7 +977,7 @@ bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2
 }
 
 cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
-    if (a.blocked && tb_supported(a)) {
+    if (a.blocked && !a.bf16 && tb_supported(a)) {
         switch (a.kind) {
         case KIND_VEL_X: return run_tb<KIND_VEL_X>(a, s, a.error_flag);
         case KIND_VEL_Y: return run_tb<KIND_VEL_Y>(a, s, a.error_flag);
@@ -764,12 +987,21 @@ cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
         default: return cudaErrorInvalidValue;
         }
     }
+    if (a.bf16) {
+        switch (a.kind) {
+        case KIND_VEL_X: return run_simple<KIND_VEL_X, __nv_bfloat16>(a, s);
+        case KIND_VEL_Y: return run_simple<KIND_VEL_Y, __nv_bfloat16>(a, s);
+        case KIND_VEL_Z: return run_simple<KIND_VEL_Z, __nv_bfloat16>(a, s);
+        case KIND_SCALAR: return run_simple<KIND_SCALAR, __nv_bfloat16>(a, s);
+        default: return cudaErrorInvalidValue;  // the pressure is FP32
+        }
+    }
     switch (a.kind) {
-    case KIND_VEL_X: return run_simple<KIND_VEL_X>(a, s);
-    case KIND_VEL_Y: return run_simple<KIND_VEL_Y>(a, s);
-    case KIND_VEL_Z: return run_simple<KIND_VEL_Z>(a, s);
-    case KIND_SCALAR: return run_simple<KIND_SCALAR>(a, s);
-    case KIND_PRESSURE: return run_simple<KIND_PRESSURE>(a, s);
+    case KIND_VEL_X: return run_simple<KIND_VEL_X, float>(a, s);
+    case KIND_VEL_Y: return run_simple<KIND_VEL_Y, float>(a, s);
+    case KIND_VEL_Z: return run_simple<KIND_VEL_Z, float>(a, s);
+    case KIND_SCALAR: return run_simple<KIND_SCALAR, float>(a, s);
+    case KIND_PRESSURE: return run_simple<KIND_PRESSURE, float>(a, s);
     default: return cudaErrorInvalidValue;
     }
 }

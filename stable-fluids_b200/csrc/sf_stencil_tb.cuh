@@ -146,8 +146,8 @@ __device__ __forceinline__ float ghost(const GhostRule& g, int face, float self)
 // (exact with an FMA), q' = RN(q + r y). It equals IEEE division for every
 // numerator checked with |n| >= 1e-30 (all 2^32 numerators for d = 6,
 // sampled ones for the diffusion divisors 1 + 6 alpha). Zeros keep their
-// sign here; the caller sends the few numerators with 0 < |n| < 2^-99 to the
-// IEEE division (needs_ieee_div).
+// sign here; the caller sends the numerators with 0 < |n| < 2^-99 to the
+// exact tiny-numerator paths below (needs_ieee_div).
 __device__ __forceinline__ float markstein_div(float n, float d, float y) {
     const float q = __fmul_rn(n, y);
     const float r = __fmaf_rn(-q, d, n);
@@ -156,14 +156,33 @@ __device__ __forceinline__ float markstein_div(float n, float d, float y) {
 }
 __device__ __forceinline__ bool needs_ieee_div(float n) { return !(fabsf(n) >= 0x1p-99f) && n != 0.0f; }
 
-// n / d for those numerators: the quotient of the FP64 operands rounded once
-// to FP64 and then to FP32. Double rounding through a format with at least
-// 2p + 2 bits (53 >= 2 * 24 + 2) is innocuous for division (S. Figueroa,
-// "When is double rounding innocuous?", SIGNUM Newsl. 30(3), 1995), so this
-// is the correctly rounded FP32 quotient -- checked against IEEE FP32
-// division for all 2^32 numerators with d = 6 -- and, unlike FP32 division
-// of a tiny numerator, it has no scaling slow path.
-__device__ __forceinline__ float tiny_div(float n, float d) { return static_cast<float>(__ddiv_rn(static_cast<double>(n), static_cast<double>(d))); }
+// n / d for those numerators (0 < |n| < 2^-99, d >= 1) in FP32 arithmetic.
+// Markstein's correction is exact under scaling by powers of two, so
+// q' = markstein(n 2^64, d) is RN(n 2^64 / d) and, while the quotient is
+// normal (|q'| >= 2^-62), q' 2^-64 is the correctly rounded quotient. A
+// quotient in the subnormal range is a multiple of 2^-149: with
+// t = |n| / 2^-149 (an integer, exact in FP32) it is k 2^-149, k the integer
+// nearest t / d (ties to even). y = markstein(t, d) = RN(t / d) with
+// t / d < 2^23, where half-integers are representable, so rint(y) is k unless
+// y itself is a half-integer; that case is settled by the sign of t - y d
+// (one FMA, exact in sign). Checked against IEEE division for every tiny
+// numerator of both signs with 11 divisors between 1 and 601 (1, 6, the
+// all-ones significand, diffusion divisors 1 + 6 alpha), and on the GPU
+// against __fdiv_rn.
+__device__ __forceinline__ float tiny_div(float n, float d, float recip) {
+    const float q = markstein_div(__fmul_rn(n, 0x1p64f), d, recip);
+    if (fabsf(q) >= 0x1p-62f) return __fmul_rn(q, 0x1p-64f);
+    const float t = __fmul_rn(__fmul_rn(fabsf(n), 0x1p100f), 0x1p49f);
+    const float y = markstein_div(t, d, recip);
+    float k = rintf(y);
+    const float f = y - k;
+    if (f == 0.5f || f == -0.5f) {
+        const float c = __fmaf_rn(-y, d, t);
+        if (c > 0.0f) k = y + 0.5f;
+        else if (c < 0.0f) k = y - 0.5f;
+    }
+    return copysignf(__fmul_rn(__fmul_rn(k, 0x1p-100f), 0x1p-49f), n);
+}
 
 // n / 6 for the pressure update, correctly rounded for every FP32 n (checked
 // against IEEE division for all 2^32 numerators). Markstein's correction for
@@ -182,14 +201,15 @@ __device__ __forceinline__ float div6_tiny(float n) {
     return copysignf(static_cast<float>(k) * 0x1p-100f * 0x1p-49f, n);
 }
 
-// The division of a stencil update by its divisor: exact n / 6 for the
-// pressure, Markstein with the FP64 fallback for the diffusion divisors.
+// The division of a stencil update by its divisor, correctly rounded:
+// Markstein's correction, with the exact tiny-numerator paths (div6_tiny for
+// the pressure, tiny_div for the diffusion divisors).
 template <int KIND>
 __device__ __forceinline__ float update_div(float n, float divisor, float recip) {
     float q = markstein_div(n, divisor, recip);
     if (needs_ieee_div(n)) {
         if constexpr (KIND == KIND_PRESSURE) q = div6_tiny(n);
-        else q = tiny_div(n, divisor);
+        else q = tiny_div(n, divisor, recip);
     }
     return q;
 }
@@ -270,7 +290,7 @@ __device__ __forceinline__ void stage_all(const Combo* combo, float* xs, const f
             bool ok = lane_ok[k] && pair < npairs;
             if (mask_y) ok = ok && static_cast<unsigned>(gy_base + s + 2 * PG * m) < static_cast<unsigned>(ny);
             float q = tb::markstein_div(num[k][m], divisor, recip);
-            if (any_rare && tb::needs_ieee_div(num[k][m])) q = KIND == KIND_PRESSURE ? tb::div6_tiny(num[k][m]) : tb::tiny_div(num[k][m], divisor);
+            if (any_rare && tb::needs_ieee_div(num[k][m])) q = KIND == KIND_PRESSURE ? tb::div6_tiny(num[k][m]) : tb::tiny_div(num[k][m], divisor, recip);
             if (ok) cell[k][m * STEP] = q;
         }
 }

@@ -368,3 +368,35 @@ def test_batch_step_matches_single_contexts(sf, lib, cuda):
     for sim, sc, ref in zip(sims, scenes, single):
         assert_bit_equal(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), ref)
         sim.close()
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_bf16_storage_against_fp64_oracle(scheme, sf, lib, orc, cuda):
+    """BF16 storage of velocity and density (FP32 arithmetic, FP32 pressure):
+    the error against the FP64 oracle stays within a few BF16 roundings
+    (2^-8 relative) per field, close to the FP32 library's own error."""
+    scene = sf.scenes.config0(steps=20)
+    outs = {}
+    for storage in (sf.STORAGE_FP32, sf.STORAGE_BF16):
+        opts = sf.default_options(lib)
+        opts.scheme = scheme
+        opts.storage = storage
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=opts)
+        sf.scenes.run(sim, scene)
+        outs[storage] = {"density": sim.fetch(sf.VIEW_SCALAR_FIELD_DATA, sim.scalar_handles[0]), "velocity": np.stack(sim.fetch(sf.VIEW_FLOW_VELOCITY)), "pressure": sim.fetch(sf.VIEW_FLOW_PRESSURE)}
+        sim.close()
+    o = orc.Oracle(scene.config, scene.scalars, scene.vectors, precision=64, scheme=scheme)
+    sf.scenes.run(o, scene)
+    ref = {"density": o.get(orc.SCALAR, 1), "velocity": np.stack(o.velocity()), "pressure": o.get(orc.PRESSURE)}
+    errs = {k: (rel_l2(outs[sf.STORAGE_FP32][k], ref[k]), rel_l2(outs[sf.STORAGE_BF16][k], ref[k])) for k in ref}
+    print("relative L2 error vs FP64 (FP32 storage, BF16 storage):", errs)
+    for k, (e32, e16) in errs.items():
+        assert e16 <= 2e-2, (k, errs)
+        assert e32 <= 1e-4, (k, errs)
