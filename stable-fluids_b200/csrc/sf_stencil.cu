@@ -30,12 +30,6 @@ __device__ __forceinline__ float neighbour(const T* __restrict__ f, int x, int y
     else return load_velocity(f, KIND, x, y, z, d, fb);
 }
 
-template <int KIND>
-__device__ __forceinline__ float update(float nb, float rhs, float coef) {
-    if constexpr (KIND == KIND_PRESSURE) return (nb - coef * rhs) / 6.0f;
-    else return (rhs + coef * nb) / (1.0f + 6.0f * coef);
-}
-
 template <int KIND, typename T>
 __device__ __forceinline__ float neighbour_sum(const T* __restrict__ f, int x, int y, int z, const Dims& d, const FlowBC& fb, const ScalarBC& sb) {
     return neighbour<KIND>(f, x - 1, y, z, d, fb, sb) + neighbour<KIND>(f, x + 1, y, z, d, fb, sb) + neighbour<KIND>(f, x, y - 1, z, d, fb, sb) + neighbour<KIND>(f, x, y + 1, z, d, fb, sb) + neighbour<KIND>(f, x, y, z - 1, d, fb, sb)
@@ -59,7 +53,7 @@ __global__ void __launch_bounds__(256) k_rbgs_colour(T* x, const T* __restrict__
     if (y >= d.ny) return;
     const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
     float num[kColourPlanes];
     size_t idx[kColourPlanes];
     bool ok[kColourPlanes];
@@ -84,7 +78,7 @@ __global__ void __launch_bounds__(256) k_rbgs_colour(T* x, const T* __restrict__
 #pragma unroll
     for (int k = 0; k < kColourPlanes; ++k) {
         if (!ok[k]) continue;
-        x[idx[k]] = from_f<T>(tb::update_div<KIND>(num[k], divisor, recip));
+        x[idx[k]] = from_f<T>(tb::divide(num[k], divisor, recip));
     }
 }
 
@@ -99,7 +93,7 @@ __global__ void __launch_bounds__(256) k_jacobi(T* __restrict__ dst, const T* __
     if (cx >= d.nx || y >= d.ny) return;
     const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
     const bool xy_interior = cx >= 1 && cx <= d.nx - 2 && y >= 1 && y <= d.ny - 2;
 #pragma unroll
     for (int k = 0; k < kColourPlanes; ++k) {
@@ -114,7 +108,7 @@ __global__ void __launch_bounds__(256) k_jacobi(T* __restrict__ dst, const T* __
             nb = neighbour_sum<KIND>(src, cx, y, z, d, fb, sb);
         }
         const float num = tb::numerator<KIND>(nb, to_f(rhs[i]), coef);
-        dst[i] = from_f<T>(tb::update_div<KIND>(num, divisor, recip));
+        dst[i] = from_f<T>(tb::divide(num, divisor, recip));
     }
 }
 
@@ -129,206 +123,14 @@ __global__ void __launch_bounds__(256) k_jacobi(T* __restrict__ dst, const T* __
 // with selects, so boundary threads take the same path as interior ones.
 // Arithmetic, neighbour order and division are those of k_rbgs_colour /
 // k_jacobi, so results are bit-identical.
-// A thread owns W consecutive cells of a row held in one 16-byte vector:
-// W = 4 for FP32 fields (the float4 kernels further down), W = 8 for BF16
-// fields (the generic W-cell kernels here, 8 BF16 per vector).
-template <typename T>
-struct VecWidth {
-    static constexpr int W = sizeof(T) == 2 ? 8 : 4;
-};
-template <int W>
-struct Row {
-    float v[W];
-};
-
-__device__ __forceinline__ void loadv(const __nv_bfloat16* p, Row<8>& r) {
-    const uint4 u = *reinterpret_cast<const uint4*>(p);
-    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[k]));
-        r.v[2 * k] = f.x;
-        r.v[2 * k + 1] = f.y;
-    }
-}
-__device__ __forceinline__ void storev(__nv_bfloat16* p, const Row<8>& r) {
-    uint32_t w[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        __nv_bfloat162 h = __floats2bfloat162_rn(r.v[2 * k], r.v[2 * k + 1]);
-        w[k] = *reinterpret_cast<uint32_t*>(&h);
-    }
-    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
-}
-__device__ __forceinline__ float ld1(const __nv_bfloat16* p) { return __bfloat162float(*p); }
-
-template <int W>
-__device__ __forceinline__ Row<W> ghostv(const GhostRule& g, int face, const Row<W>& self) {
-    Row<W> r;
-#pragma unroll
-    for (int k = 0; k < W; ++k) r.v[k] = tb::ghost(g, face, self.v[k]);
-    return r;
-}
-
-struct VecGhost {
-    int ox_lo, ox_hi;  // offsets of the row's x- / x+ neighbours from x0 (wrap or self on a face)
-    int oy_lo, oy_hi;  // y offsets of the y- / y+ rows
-    bool gx_lo, gx_hi, gy_lo, gy_hi;  // apply the face ghost
-};
-
-template <int W>
-__device__ __forceinline__ VecGhost vec_ghost(int x0, int y, const Dims& d, const GhostRule& g) {
-    const int sy = d.nx;
-    VecGhost v{-1, W, -sy, sy, false, false, false, false};
-    if (x0 == 0) {
-        v.ox_lo = g.periodic[0] ? d.nx - 1 : 0;
-        v.gx_lo = !g.periodic[0];
-    }
-    if (x0 + W == d.nx) {
-        v.ox_hi = g.periodic[0] ? -x0 : W - 1;
-        v.gx_hi = !g.periodic[0];
-    }
-    if (y == 0) {
-        v.oy_lo = g.periodic[1] ? (d.ny - 1) * sy : 0;
-        v.gy_lo = !g.periodic[1];
-    }
-    if (y == d.ny - 1) {
-        v.oy_hi = g.periodic[1] ? -(d.ny - 1) * sy : 0;
-        v.gy_hi = !g.periodic[1];
-    }
-    return v;
-}
-
 template <int KIND>
-__device__ __forceinline__ float vec_update(float nb, float rhs, float coef, float divisor, float recip) {
-    return tb::update_div<KIND>(tb::numerator<KIND>(nb, rhs, coef), divisor, recip);
-}
-
-// The plane below the chunk's first plane (or its ghost at z = 0).
-template <typename T, int W>
-__device__ __forceinline__ Row<W> vec_below(const T* x, int i, int z, const Dims& d, const GhostRule& g, const Row<W>& cur) {
-    const int sz = d.nx * d.ny;
-    Row<W> r;
-    if (z > 0) loadv(x + i - sz, r);
-    else if (g.periodic[2]) loadv(x + i + (d.nz - 1) * sz, r);
-    else r = ghostv<W>(g, ZM, cur);
-    return r;
-}
-
-template <typename T, int W>
-__device__ __forceinline__ Row<W> vec_above(const T* x, int i, int z, const Dims& d, const GhostRule& g, const Row<W>& cur) {
-    const int sz = d.nx * d.ny;
-    Row<W> r;
-    if (z + 1 < d.nz) loadv(x + i + sz, r);
-    else if (g.periodic[2]) loadv(x + i - (d.nz - 1) * sz, r);
-    else r = ghostv<W>(g, ZP, cur);
-    return r;
-}
-
-// Neighbours of the W cells of a row: x- / x+ (from the row itself and the
-// two single loads at its ends), y- / y+ rows, with face ghosts applied.
-template <typename T, int W>
-struct RowNeighbours {
-    float a, b;     // x- neighbour of cell 0, x+ neighbour of cell W - 1
-    Row<W> c, e;    // y- and y+ rows
-};
-
-template <typename T, int W>
-__device__ __forceinline__ RowNeighbours<T, W> row_neighbours(const T* x, int i, const VecGhost& v, const GhostRule& g) {
-    RowNeighbours<T, W> n;
-    n.a = ld1(x + i + v.ox_lo);
-    n.b = ld1(x + i + v.ox_hi);
-    loadv(x + i + v.oy_lo, n.c);
-    loadv(x + i + v.oy_hi, n.e);
-    if (v.gx_lo) n.a = tb::ghost(g, XM, n.a);
-    if (v.gx_hi) n.b = tb::ghost(g, XP, n.b);
-    if (v.gy_lo) n.c = ghostv<W>(g, YM, n.c);
-    if (v.gy_hi) n.e = ghostv<W>(g, YP, n.e);
-    return n;
+__device__ __forceinline__ float vec_update(float nb, float rhs, float coef, float divisor, double recip) {
+    return tb::divide(tb::numerator<KIND>(nb, rhs, coef), divisor, recip);
 }
 
 constexpr int kVecRows = 4;  // rows per CTA; 32 x kVecRows threads
 
-// One Jacobi sweep dst = update(src).
-template <int KIND, typename T = float>
-__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vecw(T* __restrict__ dst, const T* __restrict__ src, const T* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
-    constexpr int W = VecWidth<T>::W;
-    const int x0 = W * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
-    if (x0 >= d.nx || y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
-    const VecGhost v = vec_ghost<W>(x0, y, d, g);
-    const int sz = d.nx * d.ny;
-    int i = x0 + d.nx * (y + d.ny * zb);
-    Row<W> cur;
-    loadv(src + i, cur);
-    Row<W> below = vec_below<T, W>(src, i, zb, d, g, cur);
-#pragma unroll 2
-    for (int z = zb; z < ze; ++z, i += sz) {
-        const Row<W> above = vec_above<T, W>(src, i, z, d, g, cur);
-        const RowNeighbours<T, W> n = row_neighbours<T, W>(src, i, v, g);
-        Row<W> r;
-        loadv(rhs + i, r);
-        Row<W> o;
-#pragma unroll
-        for (int k = 0; k < W; ++k) {
-            const float xm = k == 0 ? n.a : cur.v[k - 1];
-            const float xp = k == W - 1 ? n.b : cur.v[k + 1];
-            o.v[k] = vec_update<KIND>(xm + xp + n.c.v[k] + n.e.v[k] + below.v[k] + above.v[k], r.v[k], coef, divisor, recip);
-        }
-        storev(dst + i, o);
-        below = cur;
-        cur = above;
-    }
-}
-
-// One colour of an RBGS iteration, in place: in each row of W cells the W/2
-// cells with (x + y + z + parity) even are updated; the others are stored
-// back unchanged (no thread of this launch changes them, so rewriting the
-// value just read is harmless and keeps every store a full 16 bytes).
-template <int KIND, typename T = float>
-__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vecw(T* x, const T* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
-    constexpr int W = VecWidth<T>::W;
-    const int x0 = W * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
-    if (x0 >= d.nx || y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
-    const VecGhost v = vec_ghost<W>(x0, y, d, g);
-    const int sz = d.nx * d.ny;
-    int i = x0 + d.nx * (y + d.ny * zb);
-    Row<W> cur;
-    loadv(x + i, cur);
-    Row<W> below = vec_below<T, W>(x, i, zb, d, g, cur);
-#pragma unroll 2
-    for (int z = zb; z < ze; ++z, i += sz) {
-        const Row<W> above = vec_above<T, W>(x, i, z, d, g, cur);
-        const RowNeighbours<T, W> n = row_neighbours<T, W>(x, i, v, g);
-        Row<W> r;
-        loadv(rhs + i, r);
-        const int first = (y + z + parity) & 1;  // cells first, first + 2, ... are updated
-        Row<W> o = cur;
-#pragma unroll
-        for (int m = 0; m < W / 2; ++m) {
-            // selects keep the loop free of divergence: cell k = 2 m + first
-            const float xm = first ? cur.v[2 * m] : (m == 0 ? n.a : cur.v[2 * m - 1]);
-            const float xp = first ? (m == W / 2 - 1 ? n.b : cur.v[2 * m + 2]) : cur.v[2 * m + 1];
-            const float ym = first ? n.c.v[2 * m + 1] : n.c.v[2 * m], yp = first ? n.e.v[2 * m + 1] : n.e.v[2 * m];
-            const float zm = first ? below.v[2 * m + 1] : below.v[2 * m], zp = first ? above.v[2 * m + 1] : above.v[2 * m];
-            const float q = vec_update<KIND>(xm + xp + ym + yp + zm + zp, first ? r.v[2 * m + 1] : r.v[2 * m], coef, divisor, recip);
-            if (first) o.v[2 * m + 1] = q;
-            else o.v[2 * m] = q;
-        }
-        storev(x + i, o);
-        below = cur;
-        cur = above;
-    }
-}
-
 // ---- FP32 fields: float4 rows (4 cells per thread) ----------------------
-// The FP32 kernels keep a hand-specialised float4 form; the generic W-cell
-// kernels above serve the BF16 storage.
 struct VecGhost4 {
     int ox_lo, ox_hi;  // x offsets of the row's x- / x+ neighbours from x0 (wrap or self on a face)
     int oy_lo, oy_hi;  // y offsets of the y- / y+ rows
@@ -387,7 +189,7 @@ __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
     int i = x0 + d.nx * (y + d.ny * zb);
@@ -424,7 +226,7 @@ __global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const flo
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
     int i = x0 + d.nx * (y + d.ny * zb);
@@ -450,6 +252,129 @@ __global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const flo
         below = cur;
         cur = above;
     }
+}
+
+
+// ---- BF16 fields: 4 cells per thread (one 8-byte vector) ------------------
+// The diffusion fields of a BF16-storage context. Same march, ghosts, sum
+// order and division as the float4 kernels, in FP32 arithmetic on the
+// unpacked values, rounded once to BF16 on the store. Half the bytes per cell
+// means half the loads in flight per warp, so each thread issues the loads
+// of the next plane (the row above it, the y- / y+ rows, the right-hand side
+// and the two x-end cells) before it computes the current one. For RBGS that
+// is safe in place: a colour launch reads only cells of the other colour
+// (unchanged by the launch) or its own row before storing it.
+__device__ __forceinline__ uint2 ld_bf4(const __nv_bfloat16* p) { return *reinterpret_cast<const uint2*>(p); }
+__device__ __forceinline__ float4 unpack_bf4(uint2 u) {
+    return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u), __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
+}
+__device__ __forceinline__ unsigned pack_bf2(float lo, float hi) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const unsigned*>(&h);
+}
+__device__ __forceinline__ float ld_bf1(const __nv_bfloat16* p) { return __uint_as_float(static_cast<unsigned>(*reinterpret_cast<const unsigned short*>(p)) << 16); }
+
+// Raw loads of one plane for one thread.
+struct Bf16Plane {
+    uint2 up;        // the row above (plane z + 1, or the periodic wrap)
+    uint2 ym, yp;    // the y- / y+ rows
+    uint2 rhs;       // the right-hand side row
+    float xm, xp;    // x- neighbour of cell 0, x+ neighbour of cell 3
+};
+
+__device__ __forceinline__ void fetch_bf16(Bf16Plane& q, const __nv_bfloat16* src, const __nv_bfloat16* rhs, int i, int z, const Dims& d, const GhostRule& g, const VecGhost4& v) {
+    const int sz = d.nx * d.ny;
+    if (z + 1 < d.nz) q.up = ld_bf4(src + i + sz);
+    else if (g.periodic[2]) q.up = ld_bf4(src + i - (d.nz - 1) * sz);
+    q.ym = ld_bf4(src + i + v.oy_lo);
+    q.yp = ld_bf4(src + i + v.oy_hi);
+    q.rhs = ld_bf4(rhs + i);
+    q.xm = ld_bf1(src + i + v.ox_lo);
+    q.xp = ld_bf1(src + i + v.ox_hi);
+}
+
+// RB: one colour of an RBGS iteration in place (dst == src); else one Jacobi
+// sweep. DEPTH: planes of loads in flight ahead of the one computed.
+template <int KIND, bool RB, int DEPTH>
+__device__ __forceinline__ void march_bf16(__nv_bfloat16* dst, const __nv_bfloat16* src, const __nv_bfloat16* rhs, float coef, int parity, int z_chunk, const Dims& d, const GhostRule& g) {
+    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    if (x0 >= d.nx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const double recip = tb::recip64(divisor);
+    const VecGhost4 v = vec_ghost4(x0, y, d, g);
+    const int sz = d.nx * d.ny;
+    int i = x0 + d.nx * (y + d.ny * zb);
+    float4 cur = unpack_bf4(ld_bf4(src + i));
+    float4 below;
+    if (zb > 0) below = unpack_bf4(ld_bf4(src + i - sz));
+    else if (g.periodic[2]) below = unpack_bf4(ld_bf4(src + i + (d.nz - 1) * sz));
+    else below = ghost4(g, ZM, cur);
+    // one plane: q holds its raw loads; advances below / cur
+    const auto plane = [&](const Bf16Plane& q, int z, int at) {
+        const float4 above = (z + 1 < d.nz || g.periodic[2]) ? unpack_bf4(q.up) : ghost4(g, ZP, cur);
+        float a = q.xm, b = q.xp;
+        float4 c = unpack_bf4(q.ym), e = unpack_bf4(q.yp);
+        const float4 r = unpack_bf4(q.rhs);
+        if (v.gx_lo) a = tb::ghost(g, XM, a);
+        if (v.gx_hi) b = tb::ghost(g, XP, b);
+        if (v.gy_lo) c = ghost4(g, YM, c);
+        if (v.gy_hi) e = ghost4(g, YP, e);
+        uint2 o;
+        if constexpr (RB) {
+            if (((y + z + parity) & 1) == 0) {  // cells 0 and 2 (warp-uniform branch)
+                o.x = pack_bf2(vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip), cur.y);
+                o.y = pack_bf2(vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip), cur.w);
+            } else {  // cells 1 and 3
+                o.x = pack_bf2(cur.x, vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip));
+                o.y = pack_bf2(cur.z, vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip));
+            }
+        } else {
+            o.x = pack_bf2(vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip), vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip));
+            o.y = pack_bf2(vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip), vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip));
+        }
+        *reinterpret_cast<uint2*>(dst + at) = o;
+        below = cur;
+        cur = above;
+    };
+    if constexpr (DEPTH == 1) {
+        Bf16Plane nxt;
+        fetch_bf16(nxt, src, rhs, i, zb, d, g, v);
+        for (int z = zb; z < ze; ++z, i += sz) {
+            const Bf16Plane q = nxt;  // waits for the loads issued one plane ago
+            if (z + 1 < ze) fetch_bf16(nxt, src, rhs, i + sz, z + 1, d, g, v);
+            plane(q, z, i);
+        }
+    } else {
+        // two buffers, planes alternating: the copy out of one waits only for
+        // loads issued two planes ago while the other's stay in flight
+        static_assert(DEPTH == 2, "prefetch depth 1 or 2");
+        Bf16Plane pa, pb;
+        fetch_bf16(pa, src, rhs, i, zb, d, g, v);
+        if (zb + 1 < ze) fetch_bf16(pb, src, rhs, i + sz, zb + 1, d, g, v);
+        for (int z = zb; z < ze; z += 2, i += 2 * sz) {
+            const Bf16Plane qa = pa;
+            if (z + 2 < ze) fetch_bf16(pa, src, rhs, i + 2 * sz, z + 2, d, g, v);
+            plane(qa, z, i);
+            if (z + 1 < ze) {
+                const Bf16Plane qb = pb;
+                if (z + 3 < ze) fetch_bf16(pb, src, rhs, i + 3 * sz, z + 3, d, g, v);
+                plane(qb, z + 1, i + sz);
+            }
+        }
+    }
+}
+
+constexpr int kBf16Depth = 2;
+
+template <int KIND, int DEPTH = kBf16Depth>
+__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_bf16(__nv_bfloat16* __restrict__ dst, const __nv_bfloat16* __restrict__ src, const __nv_bfloat16* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    march_bf16<KIND, false, DEPTH>(dst, src, rhs, coef, 0, z_chunk, d, g);
+}
+
+template <int KIND, int DEPTH = kBf16Depth>
+__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_bf16(__nv_bfloat16* x, const __nv_bfloat16* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+    march_bf16<KIND, true, DEPTH>(x, x, rhs, coef, parity, z_chunk, d, g);
 }
 
 // Launch shape of the vectorised kernels: as many z chunks as fit the
@@ -515,7 +440,7 @@ __global__ void __launch_bounds__(kTbThreads) k_jacobi_tb2(float* __restrict__ d
     const int x0 = static_cast<int>(blockIdx.x) * kTbX, y0 = static_cast<int>(blockIdx.y) * kTbY;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
     const int sy = d.nx, sz = d.nx * d.ny;
     const int px = g.periodic[0], py = g.periodic[1], pz = g.periodic[2];
     const auto mod3 = [](int q) { return ((q % 3) + 3) % 3; };
@@ -575,7 +500,7 @@ __global__ void __launch_bounds__(kTbThreads) k_jacobi_tb2(float* __restrict__ d
         const float yp = (!py && gy == d.ny - 1) ? tb::ghost(g, YP, self) : c[W];
         const float zm = (!pz && q == 0) ? tb::ghost(g, ZM, self) : ring[mod3(q - 1) * n + at];
         const float zp = (!pz && q == d.nz - 1) ? tb::ghost(g, ZP, self) : ring[mod3(q + 1) * n + at];
-        return tb::update_div<KIND>(tb::numerator<KIND>(xm + xp + ym + yp + zm + zp, b, coef), divisor, recip);
+        return tb::divide(tb::numerator<KIND>(xm + xp + ym + yp + zm + zp, b, coef), divisor, recip);
     };
 
     // Iteration q stages input plane q + 1, runs the first sweep on plane q
@@ -714,18 +639,17 @@ TbShape2 tb2_shape(const Dims& d, Kernel kernel) {
 
 GhostRule ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb);
 
-// Vectorised sweep kernels per element type: the float4 kernels for FP32
-// fields, the 8-cell kernels for BF16 fields.
+// Vectorised sweep kernels per element type (4 cells per thread for both).
 template <int KIND, typename T>
 auto jacobi_vec_kernel() {
     if constexpr (sizeof(T) == sizeof(float)) return k_jacobi_vec4<KIND>;
-    else return k_jacobi_vecw<KIND, T>;
+    else return k_jacobi_bf16<KIND>;
 }
 
 template <int KIND, typename T>
 auto rbgs_vec_kernel() {
     if constexpr (sizeof(T) == sizeof(float)) return k_rbgs_vec4<KIND>;
-    else return k_rbgs_vecw<KIND, T>;
+    else return k_rbgs_bf16<KIND>;
 }
 
 // T: element type of x, b and scratch (BF16 only for the diffusion kinds of a
@@ -743,10 +667,10 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(ax, ab, bytes, cudaMemcpyDeviceToDevice, s);
         else if (a.init == INIT_ZERO) e = cudaMemsetAsync(ax, 0, bytes, s);
         if (e != cudaSuccess) return e;
-        if (vec_ok(a, VecWidth<T>::W)) {
+        if (vec_ok(a)) {
             const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
             const auto kernel = rbgs_vec_kernel<KIND, T>();
-            const VecShape vs = vec_shape(d, kernel, VecWidth<T>::W);
+            const VecShape vs = vec_shape(d, kernel);
             for (int it = 0; it < a.iterations; ++it)
                 for (int parity = 0; parity < 2; ++parity) kernel<<<vs.grid, dim3(32, kVecRows), 0, s>>>(ax, ab, a.coef, parity, vs.z_chunk, d, g);
         } else {
@@ -758,10 +682,10 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         if (a.launches) *a.launches += 2 * a.iterations;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
-        const bool vec = vec_ok(a, VecWidth<T>::W);
+        const bool vec = vec_ok(a);
         const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
         const auto jacobi_vec = jacobi_vec_kernel<KIND, T>();
-        const VecShape vs = vec ? vec_shape(d, jacobi_vec, VecWidth<T>::W) : VecShape{};
+        const VecShape vs = vec ? vec_shape(d, jacobi_vec) : VecShape{};
         const dim3 jblock(32, 8, 1);
         const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
         // With blocking requested, sweeps go two per pass (k_jacobi_tb2, FP32)

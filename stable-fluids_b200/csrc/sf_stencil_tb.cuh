@@ -141,77 +141,29 @@ __device__ __forceinline__ float ghost(const GhostRule& g, int face, float self)
     return g.k[face] - self;
 }
 
-// Correctly rounded n / d from y = RN(1 / d) by Markstein's correction
-// (P. Markstein, IBM J. Res. Dev. 34(1), 1990): q = RN(n y), r = n - q d
-// (exact with an FMA), q' = RN(q + r y). It equals IEEE division for every
-// numerator checked with |n| >= 1e-30 (all 2^32 numerators for d = 6,
-// sampled ones for the diffusion divisors 1 + 6 alpha). Zeros keep their
-// sign here; the caller sends the numerators with 0 < |n| < 2^-99 to the
-// exact tiny-numerator paths below (needs_ieee_div).
-__device__ __forceinline__ float markstein_div(float n, float d, float y) {
-    const float q = __fmul_rn(n, y);
-    const float r = __fmaf_rn(-q, d, n);
-    const float out = __fmaf_rn(r, y, q);
-    return n == 0.0f ? n : out;
-}
-__device__ __forceinline__ bool needs_ieee_div(float n) { return !(fabsf(n) >= 0x1p-99f) && n != 0.0f; }
+// Correctly rounded FP32 n / d for every FP32 n and the stencil divisors:
+// the quotient is formed in FP64 by Markstein's correction (P. Markstein,
+// IBM J. Res. Dev. 34(1), 1990) from y = RN64(1 / d) -- q = RN(n y),
+// r = n - q d (exact with an FMA), q' = RN(q + r y) = RN64(n / d) -- and
+// rounded once to FP32. For a normal FP32 quotient that double rounding is
+// innocuous (53 >= 2 * 24 + 2; S. Figueroa, "When is double rounding
+// innocuous?", SIGNUM Newsl. 30(3), 1995). For a quotient in the subnormal
+// range, an exact FP32 midpoint n / d is representable in FP64 and every
+// other quotient lies at least 2^-175 from a midpoint, farther than the FP64
+// error (<= 2^-179), so the FP32 rounding is right there too. Checked against
+// IEEE FP32 division for all finite FP32 numerators with d = 6 and with
+// diffusion divisors 1 + 6 alpha. There is no data-dependent branch: tiny and
+// subnormal numerators (common where a field decays to zero) cost the same as
+// any other, and B200 issues FP64 FMAs at half its FP32 rate. Zeros keep
+// their sign.
+__device__ __forceinline__ double recip64(float d) { return __drcp_rn(static_cast<double>(d)); }
 
-// n / d for those numerators (0 < |n| < 2^-99, d >= 1) in FP32 arithmetic.
-// Markstein's correction is exact under scaling by powers of two, so
-// q' = markstein(n 2^64, d) is RN(n 2^64 / d) and, while the quotient is
-// normal (|q'| >= 2^-62), q' 2^-64 is the correctly rounded quotient. A
-// quotient in the subnormal range is a multiple of 2^-149: with
-// t = |n| / 2^-149 (an integer, exact in FP32) it is k 2^-149, k the integer
-// nearest t / d (ties to even). y = markstein(t, d) = RN(t / d) with
-// t / d < 2^23, where half-integers are representable, so rint(y) is k unless
-// y itself is a half-integer; that case is settled by the sign of t - y d
-// (one FMA, exact in sign). Checked against IEEE division for every tiny
-// numerator of both signs with 11 divisors between 1 and 601 (1, 6, the
-// all-ones significand, diffusion divisors 1 + 6 alpha), and on the GPU
-// against __fdiv_rn.
-__device__ __forceinline__ float tiny_div(float n, float d, float recip) {
-    const float q = markstein_div(__fmul_rn(n, 0x1p64f), d, recip);
-    if (fabsf(q) >= 0x1p-62f) return __fmul_rn(q, 0x1p-64f);
-    const float t = __fmul_rn(__fmul_rn(fabsf(n), 0x1p100f), 0x1p49f);
-    const float y = markstein_div(t, d, recip);
-    float k = rintf(y);
-    const float f = y - k;
-    if (f == 0.5f || f == -0.5f) {
-        const float c = __fmaf_rn(-y, d, t);
-        if (c > 0.0f) k = y + 0.5f;
-        else if (c < 0.0f) k = y - 0.5f;
-    }
-    return copysignf(__fmul_rn(__fmul_rn(k, 0x1p-100f), 0x1p-49f), n);
-}
-
-// n / 6 for the pressure update, correctly rounded for every FP32 n (checked
-// against IEEE division for all 2^32 numerators). Markstein's correction for
-// |n| >= 2^-99; below that, n scaled by 2^64 (exact) while the quotient is
-// normal, and for quotients in the subnormal range (|n| < 6 * 2^-126) the
-// exact integer rounding of N / 6 with N = |n| / 2^-149 (round half to even),
-// since every such quotient is a multiple of 2^-149.
-__device__ __forceinline__ float div6_tiny(float n) {
-    if (n == 0.0f) return n;
-    const float a = fabsf(n);
-    if (a >= 0x1.8p-124f) return markstein_div(__fmul_rn(n, 0x1p64f), 6.0f, 1.0f / 6.0f) * 0x1p-64f;
-    const uint32_t big = static_cast<uint32_t>(a * 0x1p100f * 0x1p49f);
-    uint32_t k = big / 6u;
-    const uint32_t r = big - 6u * k;
-    if (r > 3u || (r == 3u && (k & 1u))) ++k;
-    return copysignf(static_cast<float>(k) * 0x1p-100f * 0x1p-49f, n);
-}
-
-// The division of a stencil update by its divisor, correctly rounded:
-// Markstein's correction, with the exact tiny-numerator paths (div6_tiny for
-// the pressure, tiny_div for the diffusion divisors).
-template <int KIND>
-__device__ __forceinline__ float update_div(float n, float divisor, float recip) {
-    float q = markstein_div(n, divisor, recip);
-    if (needs_ieee_div(n)) {
-        if constexpr (KIND == KIND_PRESSURE) q = div6_tiny(n);
-        else q = tiny_div(n, divisor, recip);
-    }
-    return q;
+__device__ __forceinline__ float divide(float n, float d, double y) {
+    const double a = static_cast<double>(n);
+    const double q = __dmul_rn(a, y);
+    const double r = __fma_rn(-q, static_cast<double>(d), a);
+    const double q1 = __fma_rn(r, y, q);
+    return n == 0.0f ? n : __double2float_rn(q1);
 }
 
 // Numerator of the update in the reference's expression shape
@@ -236,7 +188,7 @@ struct Combo {
 // then the updates, then predicated stores.
 template <int KIND, int W, int MP, int PG, int NPL>
 __device__ __forceinline__ void stage_all(const Combo* combo, float* xs, const float* bs, int s, int npairs, int pg, int hi, int lane_off, int lx_lane, int lo_x, bool mask_x, int gx_base, int nx, bool mask_y, int gy_base, int ny, const TbArgs& a,
-                                          float divisor, float recip) {
+                                          float divisor, double recip) {
     constexpr int STEP = 2 * PG * W;  // floats between this lane's row pairs
     float num[NPL][MP];
     float* cell[NPL];
@@ -276,12 +228,6 @@ __device__ __forceinline__ void stage_all(const Combo* combo, float* xs, const f
             }
         }
     }
-    bool rare = false;
-#pragma unroll
-    for (int k = 0; k < NPL; ++k)
-#pragma unroll
-        for (int m = 0; m < MP; ++m) rare = rare || tb::needs_ieee_div(num[k][m]);
-    const bool any_rare = __any_sync(0xffffffffu, rare);
 #pragma unroll
     for (int k = 0; k < NPL; ++k)
 #pragma unroll
@@ -289,8 +235,7 @@ __device__ __forceinline__ void stage_all(const Combo* combo, float* xs, const f
             const int pair = pg + PG * m;
             bool ok = lane_ok[k] && pair < npairs;
             if (mask_y) ok = ok && static_cast<unsigned>(gy_base + s + 2 * PG * m) < static_cast<unsigned>(ny);
-            float q = tb::markstein_div(num[k][m], divisor, recip);
-            if (any_rare && tb::needs_ieee_div(num[k][m])) q = KIND == KIND_PRESSURE ? tb::div6_tiny(num[k][m]) : tb::tiny_div(num[k][m], divisor, recip);
+            const float q = tb::divide(num[k][m], divisor, recip);
             if (ok) cell[k][m * STEP] = q;
         }
 }
@@ -393,7 +338,7 @@ __global__ void __launch_bounds__(NT, 1) k_rbgs_tb(const __grid_constant__ CUten
     const int tid = static_cast<int>(threadIdx.x);
     const int warp = tid >> 5, lane = tid & 31;
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * a.coef;
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
 
     if (tid == 0) {
         for (int i = 0; i < NB; ++i) tb::mbar_init(&bars[i], 1);

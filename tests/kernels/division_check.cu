@@ -1,8 +1,8 @@
-// Exhaustive check, on the GPU, of the correctly rounded divisions the
-// stencil kernels use (tb::update_div in sf_stencil_tb.cuh) against IEEE
+// Exhaustive check, on the GPU, of the correctly rounded division the
+// stencil kernels use (tb::divide in sf_stencil_tb.cuh) against IEEE
 // FP32 division (__fdiv_rn): every finite FP32 numerator for the pressure
 // divisor 6; for a few diffusion divisors 1 + 6a every 61st numerator plus
-// every tiny one (0 < |n| < 2^-99, the exact FP32 fallback).
+// every tiny one (0 < |n| < 2^-99, including the subnormal quotients).
 // Prints "<divisor> <checked> <mismatches>" per divisor; exit status 1 on a
 // mismatch.
 #include <cstdio>
@@ -13,9 +13,8 @@ using namespace sfb;
 
 // Numerators u * stride for u < 2^32 / stride, then (tiny != 0) every
 // numerator with 0 < |n| < 2^-99 of both signs.
-template <int KIND>
 __global__ void k_check(float divisor, unsigned long long stride, int tiny, unsigned long long* counts) {
-    const float recip = 1.0f / divisor;
+    const double recip = tb::recip64(divisor);
     unsigned long long checked = 0, bad = 0;
     const unsigned long long tiny_bits = 0x0E000000ull;  // bit pattern of 2^-99
     const unsigned long long total = 0x100000000ull / stride + (tiny ? 2 * tiny_bits : 0);
@@ -28,7 +27,7 @@ __global__ void k_check(float divisor, unsigned long long stride, int tiny, unsi
         const float n = __uint_as_float(static_cast<unsigned>(u));
         if (!isfinite(n)) continue;
         const float want = __fdiv_rn(n, divisor);
-        const float got = tb::update_div<KIND>(n, divisor, recip);
+        const float got = tb::divide(n, divisor, recip);
         bad += __float_as_uint(want) != __float_as_uint(got);
         ++checked;
     }
@@ -44,8 +43,8 @@ int main() {
     for (int k = 0; k < 5; ++k) {
         counts[0] = counts[1] = 0;
         const float d = k == 0 ? 6.0f : diffusion[k - 1];
-        if (k == 0) k_check<KIND_PRESSURE><<<148 * 8, 256>>>(d, 1, 0, counts);
-        else k_check<KIND_SCALAR><<<148 * 8, 256>>>(d, 61, 1, counts);
+        if (k == 0) k_check<<<148 * 8, 256>>>(d, 1, 0, counts);
+        else k_check<<<148 * 8, 256>>>(d, 61, 1, counts);
         if (cudaDeviceSynchronize() != cudaSuccess) return 2;
         std::printf("%.9g %llu %llu\n", d, counts[0], counts[1]);
         failed |= counts[1] != 0;

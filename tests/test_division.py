@@ -1,10 +1,10 @@
 """The stencil kernels replace IEEE FP32 division by the update divisor with
-a multiply-based correctly rounded division (Markstein's correction, exact
-fallbacks for tiny numerators). This test compiles a small CUDA program
+a multiply-based correctly rounded division (Markstein's correction in FP64,
+rounded once to FP32). This test compiles a small CUDA program
 around the library's device function and checks it against IEEE division on
 the GPU for all 2^32 numerators with the pressure divisor 6 and, for
 diffusion divisors, for a sample of numerators plus every tiny one
-(0 < |n| < 2^-99, the FP32 fallback); bit equality is required."""
+(0 < |n| < 2^-99); bit equality is required."""
 
 import pathlib
 import shutil
