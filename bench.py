@@ -376,12 +376,16 @@ def fixed_iterations(sf, lib, scene, steps, warmup, device, world):
     return {"steps_per_s": world * steps / t, "ms_per_step": 1000.0 * t / steps, "steps": steps, "pressure_iterations": scene.config.pressure_iterations, "scheme": "rbgs"}
 
 
-def batched(sf, lib, steps, warmup, count=64, use_batch=True):
+def batched(sf, lib, steps, warmup, count=64, mode=None):
     """Batched workload: `count` uneven plumes (sizes over {32..128}^3,
     config-0 coefficients, 20 diffusion / 40 red-black pressure iterations).
-    use_batch: one batch graph launch per step (this library); otherwise each
-    context is stepped in turn on its own stream (how a caller drives the
-    reference library). Returns aggregate cell-updates/s."""
+    mode: "work_table" (one persistent launch per stage over all
+    simulations, z chunks from the tile autotuner), "graphs" (the step graphs
+    as children of one graph), or None (each context stepped in turn on its
+    own stream: how a caller drives the reference library). Timed with CUDA
+    events on the batch stream (work table, graphs) or by the host clock
+    around device synchronizations (contexts in turn). Returns aggregate
+    cell-updates/s."""
     import torch
 
     scenes = sf.scenes.batch_scenes(count=count)
@@ -389,23 +393,41 @@ def batched(sf, lib, steps, warmup, count=64, use_batch=True):
     for sim, sc in zip(sims, scenes):
         sf.scenes.apply_inputs(sim, sc, 0)
     cells = sum(sim.cells for sim in sims)
-    batch = sf.Batch(sims) if use_batch else None
-    step = batch.step if use_batch else (lambda: [sim.step(1) for sim in sims])
+    batch, extra = None, {}
+    if mode is not None:
+        t0 = time.perf_counter()
+        with tempfile.TemporaryDirectory() as tmp:
+            batch = sf.Batch(sims, mode=sf.BATCH_WORK_TABLE if mode == "work_table" else sf.BATCH_GRAPHS, autotune=mode == "work_table", tile_cache=os.path.join(tmp, "tiles.json") if mode == "work_table" else None)
+        extra = {"kernels_per_step": batch.kernels_per_step, "layout_create_s": time.perf_counter() - t0, "l2_groups": batch.groups}
+        if mode == "work_table":
+            extra["z_chunks_by_size"] = {f"{sc.config.nx}^3": z for sc, z in sorted(zip(scenes, batch.z_chunks), key=lambda p: p[0].config.nx)}
+    step = batch.step if batch is not None else (lambda: [sim.step(1) for sim in sims])
     for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    torch.cuda.synchronize()
-    t = time.perf_counter() - t0
+    if batch is not None:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(batch.stream)
+        for _ in range(steps):
+            step()
+        end.record(batch.stream)
+        torch.cuda.synchronize()
+        t = start.elapsed_time(end) / 1000.0
+        timing = "CUDA events on the batch stream"
+    else:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        timing = "host clock around the steps with a device synchronize on both sides (work spans many streams)"
     if batch is not None:
         batch.close()
     for sim in sims:
         sim.close()
     sizes = sorted({sc.config.nx for sc in scenes})
-    return {"cell_updates_per_s": cells * steps / t, "steps_per_s": steps / t, "sims": count, "cells": cells, "sizes": sizes, "steps": steps,
-            "timing": "host wall clock around the steps with a device synchronize on both sides (work spans many streams)", "mode": "one batch graph launch per step" if use_batch else "each context stepped on its own stream"}
+    label = {"work_table": "one persistent launch per stage over a work table of all simulations (autotuned z chunks)", "graphs": "one graph of the simulations' step graphs per batch step", None: "each context stepped on its own stream"}[mode]
+    return {"cell_updates_per_s": cells * steps / t, "steps_per_s": steps / t, "sims": count, "cells": cells, "sizes": sizes, "steps": steps, "timing": timing, "mode": label, **extra}
 
 
 def bf16_storage(sf, n, steps, warmup, device):
@@ -512,7 +534,7 @@ def reference_arm(sf, args, scene, world, rank, local):
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     line["fixed_iterations"] = fixed_iterations(sf, lib, scene, args.fixed_steps, args.warmup, local, 1)
     if args.batch_steps > 0:
-        line["batched"] = batched(sf, lib, args.batch_steps, args.warmup, use_batch=False)
+        line["batched"] = batched(sf, lib, args.batch_steps, args.warmup, mode=None)
     c = clk.summary()
     if c:
         line["clocks"] = c
@@ -584,7 +606,10 @@ def main():
     for sim in sims.values():
         sim.close()
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
-    batch = batched(sf, None, args.batch_steps, args.warmup) if args.batch_steps > 0 else None
+    batch = None
+    if args.batch_steps > 0:
+        batch = batched(sf, None, args.batch_steps, args.warmup, mode="graphs")
+        batch["work_table_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="work_table").items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "z_chunks_by_size", "layout_create_s", "l2_groups")}
     mixed = bf16_storage(sf, args.bf16_size, args.bf16_steps, args.warmup, local) if args.bf16_steps > 0 else None
 
     config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",

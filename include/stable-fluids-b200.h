@@ -165,15 +165,50 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_train_step(void*
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network);
 
 /* ---- Batched stepping (no counterpart in the reference) ----
- * A batch holds the step graphs of several contexts (each with its own grid
- * size and fields) as children of one CUDA graph: one batch step launches
- * every context's step once, and the simulations' kernels run concurrently
- * on the GPU. The batch is ordered after the work queued on each context's
- * stream and each context's stream after the batch, so update/view calls keep
- * working as for a single context. The batch copies the step graphs when it
- * is created: rebuild it after stable_fluids_b200_attach_network. Contexts
- * with a residual-driven solve (conditional graph nodes) cannot be batched. */
+ * A batch steps several contexts (each with its own grid size and fields)
+ * together; one batch step advances every context by one step. Two layouts:
+ *
+ *  - WORK_TABLE: one persistent kernel launch per stage of the step covers
+ *    every simulation, walking a table of (simulation, thread block) work
+ *    items; the stencil sweeps' z chunk per grid size comes from an
+ *    autotuner. Needs contexts with the same stage structure: FP32 storage,
+ *    the same scheme, iteration counts and warm start (zero or previous, no
+ *    residual-driven solve, no temporal blocking), one scalar field with
+ *    diffusion > 0, viscosity > 0, at most 4 force fields, nx % 4 == 0.
+ *  - GRAPHS: the contexts' own step graphs as children of one CUDA graph; the
+ *    simulations' kernels run concurrently. Any contexts except ones with a
+ *    residual-driven solve (conditional graph nodes).
+ *
+ * Both give the same bits as stepping each context alone. On B200 with 64
+ * uneven simulations (32^3..128^3) GRAPHS is the faster layout (its 64
+ * independent chains hide each kernel's ramp and tail); WORK_TABLE issues
+ * ~250 launches per L2-sized group of simulations instead of ~250 per
+ * simulation. The batch is
+ * ordered after the work queued on each context's stream and each context's
+ * stream after the batch, so update/view calls keep working as for a single
+ * context. The batch reads the contexts' configuration when it is created:
+ * rebuild it after stable_fluids_b200_attach_network. */
+typedef enum StableFluidsB200BatchMode {
+    STABLE_FLUIDS_B200_BATCH_GRAPHS = 0,     /* the default; any batchable contexts */
+    STABLE_FLUIDS_B200_BATCH_WORK_TABLE = 1, /* BACKEND_FAILURE when the contexts do not allow it */
+} StableFluidsB200BatchMode;
+
+typedef struct StableFluidsB200BatchOptions {
+    uint32_t mode;           /* StableFluidsB200BatchMode */
+    uint32_t autotune;       /* WORK_TABLE: 1 = time the sweep tile options per grid size at create */
+    const char* tile_cache;  /* JSON file of tuned tiles, read and updated when autotuning; may be NULL */
+    uint32_t reserved[4];
+} StableFluidsB200BatchOptions;
+
+/* stable_fluids_b200_batch_create_ex with mode GRAPHS and no autotuning. */
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_create(void* const* contexts, uint32_t count, void** out_batch);
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_create_ex(void* const* contexts, uint32_t count, const StableFluidsB200BatchOptions* options, void** out_batch);
+/* The layout in use (StableFluidsB200BatchMode); for WORK_TABLE the
+ * number of L2-sized groups the contexts were partitioned into (each group's
+ * whole step runs before the next group's, so its sweeps reread their fields
+ * from L2) and the z chunk (planes per thread block) of each context's
+ * sweeps, in batch order (up to `capacity` entries; 0 for GRAPHS). */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_layout(void* batch, uint32_t* out_mode, uint32_t* out_groups, int32_t* out_z_chunks, uint32_t capacity);
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_step(void* batch);
 /* Number of contexts, kernel launches per batch step, and the batch's stream. */
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_info(void* batch, uint32_t* out_count, int32_t* out_kernels_per_step, void** out_stream);

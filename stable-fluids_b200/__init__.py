@@ -140,6 +140,8 @@ B200_SYMBOLS = (
     "stable_fluids_b200_network_train_step",
     "stable_fluids_b200_attach_network",
     "stable_fluids_b200_batch_create",
+    "stable_fluids_b200_batch_create_ex",
+    "stable_fluids_b200_batch_layout",
     "stable_fluids_b200_batch_step",
     "stable_fluids_b200_batch_info",
     "stable_fluids_b200_batch_destroy",
@@ -147,6 +149,13 @@ B200_SYMBOLS = (
 
 (STAGE_FORCES, STAGE_VELOCITY_ADVECTION, STAGE_VELOCITY_DIFFUSION, STAGE_DIVERGENCE, STAGE_PRESSURE,
  STAGE_PROJECTION, STAGE_SCALARS, STAGE_DIAGNOSTICS, STAGE_STEP) = range(9)
+
+
+BATCH_GRAPHS, BATCH_WORK_TABLE = 0, 1
+
+
+class B200BatchOptions(ctypes.Structure):
+    _fields_ = [("mode", c_uint32), ("autotune", c_uint32), ("tile_cache", ctypes.c_char_p), ("reserved", c_uint32 * 4)]
 
 
 class B200StepInfo(ctypes.Structure):
@@ -180,6 +189,8 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_network_train_step.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, c_float, POINTER(c_double), P]
         lib.stable_fluids_b200_attach_network.argtypes = [P, P]
         lib.stable_fluids_b200_batch_create.argtypes = [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]
+        lib.stable_fluids_b200_batch_create_ex.argtypes = [POINTER(c_void_p), c_uint32, POINTER(B200BatchOptions), POINTER(c_void_p)]
+        lib.stable_fluids_b200_batch_layout.argtypes = [P, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_int32), c_uint32]
         lib.stable_fluids_b200_batch_step.argtypes = [P]
         lib.stable_fluids_b200_batch_info.argtypes = [P, POINTER(c_uint32), POINTER(c_int32), POINTER(c_void_p)]
         lib.stable_fluids_b200_batch_destroy.argtypes = [P]

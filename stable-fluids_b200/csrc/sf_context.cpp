@@ -20,9 +20,13 @@
 #include <cstring>
 #include <memory>
 #include <new>
+#include <cstdio>
+#include <string>
 #include <string_view>
+#include <utility>
 #include <vector>
 
+#include "sf_batch.h"
 #include "sf_launch.h"
 #include "sf_types.h"
 #include "sf_unet.h"
@@ -821,11 +825,12 @@ StableFluidsResult stable_fluids_b200_attach_network(void* context, void* networ
 namespace sfb {
 namespace {
 
-// A batch: the step graphs of several contexts as child graphs of one graph,
-// launched once per batch step on the batch's stream. The children share no
-// data, so the GPU runs the simulations' kernels concurrently; small grids
-// that cannot fill the GPU alone fill it together, and the host pays one
-// launch per batch step instead of one per simulation.
+// A batch of contexts stepped together (stable-fluids-b200.h).
+//  GRAPHS: the contexts' step graphs as child graphs of one graph, launched
+//    once per batch step; the children share no data, so the GPU runs the
+//    simulations' kernels concurrently.
+//  WORK_TABLE: one graph of persistent launches, one per stage of the step,
+//    each covering every simulation through the work table (sf_batch.h).
 struct Batch {
     std::vector<Context*> contexts;
     cudaStream_t stream = nullptr;
@@ -833,14 +838,394 @@ struct Batch {
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;
     int kernels = 0;
+    uint32_t mode = STABLE_FLUIDS_B200_BATCH_GRAPHS;
+    // work table: host entries (grouped: the simulations of a group are
+    // contiguous), their device copy, the per-group per-shape prefix offsets,
+    // and one table per group
+    std::vector<BatchSim> sims;
+    std::vector<int> order;                      // sims[i] belongs to context order[i]
+    std::vector<std::pair<int, int>> groups;     // [begin, end) ranges of sims
+    BatchSim* d_sims = nullptr;
+    uint32_t* d_first = nullptr;
+    std::vector<BatchTable> tables;              // one per group
 
     ~Batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (done) cudaEventDestroy(done);
         if (stream) cudaStreamDestroy(stream);
+        if (d_sims) cudaFree(d_sims);
+        if (d_first) cudaFree(d_first);
     }
 };
+
+float alpha_velocity(const Context& c) {
+    const float h = c.config.cell_size;
+    return c.config.dt * c.config.viscosity / (h * h);  // same expression as Stages::alpha_v
+}
+float alpha_scalar(const Context& c, const ScalarField& f) {
+    const float h = c.config.cell_size;
+    return c.config.dt * f.desc.diffusion / (h * h);  // same expression as Stages::alpha_s
+}
+int force_fields(const Context& c) {
+    int n = 0;
+    for (const auto& v : c.vectors) n += v.desc.usage == STABLE_FLUIDS_VECTOR_FIELD_FORCE ? 1 : 0;
+    return n;
+}
+
+// Whether the contexts share the stage structure the work-table kernels
+// implement (one step = the same sequence of stages and sweep counts).
+bool work_table_compatible(const std::vector<Context*>& cs) {
+    const Context& r = *cs.front();
+    for (const Context* c : cs) {
+        const auto& o = c->options;
+        if (c->bf16 || c->blocked || c->network != nullptr) return false;
+        if (o.scheme != r.options.scheme || o.warm_start != r.options.warm_start || o.warm_start == STABLE_FLUIDS_B200_WARM_START_LEARNED) return false;
+        if (o.residual_tolerance > 0.0f || c->residual_enabled != r.residual_enabled) return false;
+        if (c->config.diffuse_iterations != r.config.diffuse_iterations || c->config.pressure_iterations != r.config.pressure_iterations) return false;
+        if (!(alpha_velocity(*c) > 0.0f) || c->scalars.size() != 1 || !(alpha_scalar(*c, c->scalars[0]) > 0.0f)) return false;
+        if ((c->scalars[0].desc.dissipation > 0.0f) != (r.scalars[0].desc.dissipation > 0.0f)) return false;
+        if (force_fields(*c) > kBatchForces) return false;
+        if (c->dims.nx % 4 != 0 || c->cells >= (1ull << 31)) return false;
+    }
+    return true;
+}
+
+BatchSim make_batch_sim(const Context& c, int z_chunk) {
+    BatchSim m{};
+    const ScalarField& f = c.scalars[0];
+    m.d = c.dims;
+    m.h = c.config.cell_size;
+    m.dt = c.config.dt;
+    m.alpha_v = alpha_velocity(c);
+    m.alpha_s = alpha_scalar(c, f);
+    m.scale_s = f.desc.dissipation > 0.0f ? 1.0f / (1.0f + c.config.dt * f.desc.dissipation) : 1.0f;
+    m.z_chunk = z_chunk;
+    m.flow = c.flow;
+    m.sbc = f.bc;
+    for (int k = 0; k < 5; ++k) m.ghost[k] = make_ghost_rule(k, c.flow, k == KIND_SCALAR ? f.bc : ScalarBC{});
+    for (int k = 0; k < 3; ++k) {
+        m.vel[k] = c.vel[k];
+        m.temp[k] = c.temp[k];
+    }
+    m.packed = static_cast<float*>(c.packed);
+    m.pressure = c.pressure;
+    m.divergence = c.divergence;
+    m.magnitude = c.magnitude;
+    m.scratch = c.scratch;
+    m.sdata = f.data;
+    m.stemp = f.temp;
+    m.source = f.source;
+    for (const auto& v : c.vectors) {
+        if (v.desc.usage != STABLE_FLUIDS_VECTOR_FIELD_FORCE) continue;
+        for (int k = 0; k < 3; ++k) m.force[m.force_count][k] = v.data[k];
+        ++m.force_count;
+    }
+    m.stats = c.stats;
+    return m;
+}
+
+// Uploads the entries and, per group, the prefix offsets per launch shape.
+cudaError_t upload_table(Batch& b) {
+    const int n = static_cast<int>(b.sims.size());
+    const int ng = static_cast<int>(b.groups.size());
+    std::vector<uint32_t> first(3 * static_cast<size_t>(n + ng));
+    b.tables.assign(ng, BatchTable{});
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t at = 0;
+    std::vector<size_t> offset(3 * static_cast<size_t>(ng));
+    for (int g = 0; g < ng; ++g) {
+        const auto [lo, hi] = b.groups[g];
+        for (int shape = 0; shape < 3; ++shape) {
+            offset[3 * g + shape] = at;
+            uint32_t acc = 0;
+            for (int i = lo; i < hi; ++i) {
+                first[at++] = acc;
+                acc += batch_blocks(b.sims[i].d, shape, b.sims[i].z_chunk);
+            }
+            first[at++] = acc;
+            b.tables[g].total[shape] = acc;
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (b.d_sims == nullptr && (e = cudaMalloc(&b.d_sims, sizeof(BatchSim) * n)) != cudaSuccess) return e;
+    if (b.d_first == nullptr && (e = cudaMalloc(&b.d_first, sizeof(uint32_t) * first.size())) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.d_sims, b.sims.data(), sizeof(BatchSim) * n, cudaMemcpyHostToDevice, b.stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.d_first, first.data(), sizeof(uint32_t) * first.size(), cudaMemcpyHostToDevice, b.stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(b.stream)) != cudaSuccess) return e;
+    for (int g = 0; g < ng; ++g) {
+        auto& t = b.tables[g];
+        t.sims = b.d_sims + b.groups[g].first;
+        for (int shape = 0; shape < 3; ++shape) t.first[shape] = b.d_first + offset[3 * g + shape];
+        t.nsims = b.groups[g].second - b.groups[g].first;
+        t.sms = sms;
+    }
+    return cudaSuccess;
+}
+
+// Groups of simulations whose sweep working set (iterate, right-hand side
+// and scratch: 12 bytes per cell) fits in half the L2 cache: the batched step
+// runs group after group, so a group's hundreds of sweeps reread its fields
+// from L2 instead of HBM. Largest simulations first, first fit. Fills
+// b.sims / b.order / b.groups; `make` builds one entry from a context index.
+template <typename Make>
+void group_by_l2(Batch& b, Make make) {
+    int dev = 0, l2 = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0) l2 = 50 << 20;
+    const size_t budget = static_cast<size_t>(l2) / 2 / 12;  // cells per group
+    std::vector<int> idx(b.contexts.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = static_cast<int>(i);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return b.contexts[x]->cells > b.contexts[y]->cells; });
+    std::vector<std::vector<int>> bins;
+    std::vector<size_t> fill;
+    for (int i : idx) {
+        const size_t c = b.contexts[i]->cells;
+        size_t k = 0;
+        while (k < bins.size() && fill[k] + c > budget) ++k;
+        if (k == bins.size()) {
+            bins.emplace_back();
+            fill.push_back(0);
+        }
+        bins[k].push_back(i);
+        fill[k] += c;
+    }
+    b.sims.clear();
+    b.order.clear();
+    b.groups.clear();
+    for (const auto& bin : bins) {
+        const int lo = static_cast<int>(b.sims.size());
+        for (int i : bin) {
+            b.sims.push_back(make(i));
+            b.order.push_back(i);
+        }
+        b.groups.emplace_back(lo, static_cast<int>(b.sims.size()));
+    }
+}
+
+// ---- tile autotuner ------------------------------------------------------
+// The z chunk (planes per thread block) of the vectorised sweeps, per grid
+// size: each candidate is timed on the whole batch with CUDA events (a Jacobi
+// pressure sweep from the pressure into the scratch buffer, so no simulation
+// state changes), one size class at a time with the others fixed. Results
+// are kept in a flat JSON object {"<gpu>|<nx>x<ny>x<nz>": z_chunk, ...}.
+constexpr int kDefaultZChunk = 16;
+
+std::string tile_key(const std::string& gpu, const Dims& d) { return gpu + "|" + std::to_string(d.nx) + "x" + std::to_string(d.ny) + "x" + std::to_string(d.nz); }
+
+std::vector<std::pair<std::string, int>> read_tile_cache(const char* path) {
+    std::vector<std::pair<std::string, int>> out;
+    if (path == nullptr) return out;
+    std::FILE* f = std::fopen(path, "rb");
+    if (f == nullptr) return out;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, got);
+    std::fclose(f);
+    // "key": value pairs of a flat object; anything else is ignored
+    size_t i = 0;
+    while ((i = text.find('"', i)) != std::string::npos) {
+        const size_t j = text.find('"', i + 1);
+        if (j == std::string::npos) break;
+        const std::string key = text.substr(i + 1, j - i - 1);
+        size_t k = text.find_first_not_of(" \t\r\n", j + 1);
+        if (k == std::string::npos || text[k] != ':') {
+            i = j + 1;
+            continue;
+        }
+        k = text.find_first_not_of(" \t\r\n", k + 1);
+        if (k == std::string::npos) break;
+        char* end = nullptr;
+        const long v = std::strtol(text.c_str() + k, &end, 10);
+        if (end != text.c_str() + k && v > 0 && v < (1 << 20)) out.emplace_back(key, static_cast<int>(v));
+        i = static_cast<size_t>(end - text.c_str());
+        if (i <= j) i = j + 1;
+    }
+    return out;
+}
+
+void write_tile_cache(const char* path, const std::vector<std::pair<std::string, int>>& entries) {
+    if (path == nullptr) return;
+    std::FILE* f = std::fopen(path, "wb");
+    if (f == nullptr) return;
+    std::fputs("{\n", f);
+    for (size_t i = 0; i < entries.size(); ++i) std::fprintf(f, "  \"%s\": %d%s\n", entries[i].first.c_str(), entries[i].second, i + 1 < entries.size() ? "," : "");
+    std::fputs("}\n", f);
+    std::fclose(f);
+}
+
+// Average duration of `repeats` batched Jacobi pressure sweeps (scratch <-
+// update(p)) per group, summed over the groups, as the step runs them.
+float time_batch_sweep(Batch& b, int repeats) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -1.0f;
+    float ms = -1.0f;
+    if (cudaEventRecord(e0, b.stream) == cudaSuccess) {
+        bool ok = true;
+        for (const auto& t : b.tables)
+            for (int r = 0; r < repeats; ++r) ok = ok && launch_batch_sweep(t, KIND_PRESSURE, SCHEME_JACOBI, 0, BF_SCRATCH, BF_X, b.stream) == cudaSuccess;
+        if (ok && cudaEventRecord(e1, b.stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ms < 0.0f ? -1.0f : ms / static_cast<float>(repeats);
+}
+
+cudaError_t tune_tiles(Batch& b, const char* cache_path) {
+    int dev = 0;
+    cudaDeviceProp prop{};
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return e;
+    const std::string gpu = prop.name;
+    auto cache = read_tile_cache(cache_path);
+    const auto lookup = [&](const std::string& k) -> int {
+        for (const auto& [key, v] : cache)
+            if (key == k) return v;
+        return 0;
+    };
+    // size classes in first-seen order
+    std::vector<Dims> classes;
+    for (const auto& m : b.sims) {
+        bool seen = false;
+        for (const auto& d : classes) seen = seen || (d.nx == m.d.nx && d.ny == m.d.ny && d.nz == m.d.nz);
+        if (!seen) classes.push_back(m.d);
+    }
+    const auto set_class = [&](const Dims& d, int zc) {
+        for (auto& m : b.sims)
+            if (m.d.nx == d.nx && m.d.ny == d.ny && m.d.nz == d.nz) m.z_chunk = std::min(zc, d.nz);
+    };
+    std::vector<Dims> todo;
+    for (const auto& d : classes) {
+        const int cached = lookup(tile_key(gpu, d));
+        if (cached > 0) set_class(d, cached);
+        else todo.push_back(d);
+    }
+    if (!todo.empty()) {
+        if ((e = upload_table(b)) != cudaSuccess) return e;
+        time_batch_sweep(b, 2);  // warm-up
+        for (const Dims& d : todo) {
+            int best = std::min(kDefaultZChunk, d.nz);
+            float best_ms = -1.0f;
+            for (int zc : {2, 4, 8, 16, 32, 64, 128, 256}) {
+                if (zc > d.nz) break;
+                set_class(d, zc);
+                if ((e = upload_table(b)) != cudaSuccess) return e;
+                const float ms = time_batch_sweep(b, 5);
+                if (ms > 0.0f && (best_ms < 0.0f || ms < best_ms)) {
+                    best_ms = ms;
+                    best = zc;
+                }
+            }
+            set_class(d, best);
+            cache.emplace_back(tile_key(gpu, d), best);
+        }
+        write_tile_cache(cache_path, cache);
+    }
+    return upload_table(b);
+}
+
+// ---- the batched step -------------------------------------------------------
+// The stages of Stages::whole_step in the same order with the same sweep
+// counts and buffer sequence, each as one work-table launch.
+struct BatchStages {
+    Batch& b;
+    const BatchTable& t;  // the group's work table
+    const Context& r;     // every context has r's stage structure
+    cudaError_t e = cudaSuccess;
+    int launches = 0;
+
+    void ok(cudaError_t x) {
+        if (x == cudaSuccess) ++launches;
+        else if (e == cudaSuccess) e = x;
+    }
+
+    // One solve: the buffer sequence of run_simple (no temporal blocking).
+    void solve(int kind, int init, int iterations) {
+        if (r.options.scheme == STABLE_FLUIDS_B200_SCHEME_RBGS) {
+            if (init == INIT_FROM_B) ok(launch_batch_copy(t, kind, BF_X, BF_B, b.stream));
+            else if (init == INIT_ZERO) ok(launch_batch_copy(t, kind, BF_X, -1, b.stream));
+            for (int it = 0; it < iterations; ++it)
+                for (int parity = 0; parity < 2; ++parity) ok(launch_batch_sweep(t, kind, SCHEME_RBGS, parity, BF_X, BF_X, b.stream));
+            return;
+        }
+        int src = BF_X;
+        if (init == INIT_FROM_B) src = BF_B;
+        else if (init == INIT_ZERO) {
+            const int zero = (iterations & 1) ? BF_SCRATCH : BF_X;
+            ok(launch_batch_copy(t, kind, zero, -1, b.stream));
+            src = zero;
+        }
+        if (iterations == 0) {
+            if (src != BF_X) ok(launch_batch_copy(t, kind, BF_X, src, b.stream));
+            return;
+        }
+        for (int u = 0; u < iterations; ++u) {
+            const int left = iterations - u;
+            int dst = (left & 1) ? BF_X : BF_SCRATCH;
+            if (dst == src) dst = dst == BF_X ? BF_SCRATCH : BF_X;
+            ok(launch_batch_sweep(t, kind, SCHEME_JACOBI, 0, dst, src, b.stream));
+            src = dst;
+        }
+        if (src != BF_X) ok(launch_batch_copy(t, kind, BF_X, src, b.stream));
+    }
+
+    cudaError_t whole_step() {
+        const int diffuse = r.config.diffuse_iterations, pressure = r.config.pressure_iterations;
+        ok(launch_batch_force_pack(t, b.stream));
+        ok(launch_batch_advect_velocity(t, b.stream));
+        for (int comp = 0; comp < 3; ++comp) solve(KIND_VEL_X + comp, INIT_FROM_B, diffuse);
+        ok(launch_batch_divergence(t, b.stream));
+        solve(KIND_PRESSURE, r.options.warm_start == STABLE_FLUIDS_B200_WARM_START_ZERO ? INIT_ZERO : INIT_FROM_X, pressure);
+        ok(launch_batch_project(t, 1, b.stream));
+        if (r.residual_enabled) {
+            ok(launch_batch_stats(t, 0, 0, b.stream));
+            ok(launch_batch_residual_sums(t, b.stream));
+            ok(launch_batch_stats(t, 1, pressure, b.stream));
+        }
+        ok(launch_batch_scalar_source_advect(t, b.stream));
+        solve(KIND_SCALAR, INIT_FROM_B, diffuse);
+        if (r.scalars[0].desc.dissipation > 0.0f) ok(launch_batch_scale_scalar(t, b.stream));
+        ok(launch_batch_post_diagnostics(t, b.stream));
+        return e;
+    }
+};
+
+cudaError_t build_work_table(Batch& b, bool autotune, const char* cache_path) {
+    group_by_l2(b, [&](int i) { return make_batch_sim(*b.contexts[i], std::min(kDefaultZChunk, b.contexts[i]->dims.nz)); });
+    cudaError_t e = autotune ? tune_tiles(b, cache_path) : upload_table(b);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+    cudaError_t rec = cudaSuccess;
+    b.kernels = 0;
+    for (const auto& t : b.tables) {  // group after group: each group's step reuses L2
+        BatchStages st{b, t, *b.contexts.front()};
+        if (rec == cudaSuccess) rec = st.whole_step();
+        b.kernels += st.launches;
+    }
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b.stream, &g);
+    if (rec != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rec != cudaSuccess ? rec : e;
+    }
+    b.graph = g;
+    return cudaSuccess;
+}
+
+cudaError_t build_child_graphs(Batch& b) {
+    cudaError_t e = cudaGraphCreate(&b.graph, 0);
+    if (e != cudaSuccess) return e;
+    for (Context* c : b.contexts) {
+        if (c->graph == nullptr) return cudaErrorInvalidValue;
+        cudaGraphNode_t node = nullptr;
+        if ((e = cudaGraphAddChildGraphNode(&node, b.graph, nullptr, 0, c->graph)) != cudaSuccess) return e;
+        b.kernels += c->step_kernels;
+    }
+    return cudaSuccess;
+}
 
 }  // namespace
 }  // namespace sfb
@@ -848,14 +1233,19 @@ struct Batch {
 extern "C" {
 
 StableFluidsResult stable_fluids_b200_batch_create(void* const* contexts, uint32_t count, void** out_batch) {
+    StableFluidsB200BatchOptions o{};  // GRAPHS, no autotuning
+    return stable_fluids_b200_batch_create_ex(contexts, count, &o, out_batch);
+}
+
+StableFluidsResult stable_fluids_b200_batch_create_ex(void* const* contexts, uint32_t count, const StableFluidsB200BatchOptions* options, void** out_batch) {
+    sfb::Range range("stable.batch_create");
     if (out_batch == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     *out_batch = nullptr;
-    if (contexts == nullptr || count == 0) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (contexts == nullptr || count == 0 || options == nullptr || options->mode > STABLE_FLUIDS_B200_BATCH_WORK_TABLE) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     std::unique_ptr<sfb::Batch> b{new (std::nothrow) sfb::Batch{}};
     if (!b) return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-    if (cudaGraphCreate(&b->graph, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     for (uint32_t i = 0; i < count; ++i) {
         auto* c = static_cast<Context*>(contexts[i]);
         if (c == nullptr || c->graph == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
@@ -863,13 +1253,20 @@ StableFluidsResult stable_fluids_b200_batch_create(void* const* contexts, uint32
             if (other == c) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;  // a context steps once per batch step
         // all work queued on the context so far (updates) precedes the batch
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        cudaGraphNode_t node = nullptr;
-        if (cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, c->graph) != cudaSuccess) {
-            cudaGetLastError();
-            return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        }
         b->contexts.push_back(c);
-        b->kernels += c->step_kernels;
+    }
+    cudaError_t e;
+    if (options->mode == STABLE_FLUIDS_B200_BATCH_WORK_TABLE) {
+        if (!sfb::work_table_compatible(b->contexts)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        b->mode = STABLE_FLUIDS_B200_BATCH_WORK_TABLE;
+        e = sfb::build_work_table(*b, options->autotune != 0, options->tile_cache);
+    } else {
+        b->mode = STABLE_FLUIDS_B200_BATCH_GRAPHS;
+        e = sfb::build_child_graphs(*b);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? STABLE_FLUIDS_RESULT_OUT_OF_MEMORY : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     }
     if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
         b->exec = nullptr;
@@ -877,6 +1274,19 @@ StableFluidsResult stable_fluids_b200_batch_create(void* const* contexts, uint32
         return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     }
     *out_batch = b.release();
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_batch_layout(void* batch, uint32_t* out_mode, uint32_t* out_groups, int32_t* out_z_chunks, uint32_t capacity) {
+    if (batch == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const auto& b = *static_cast<const sfb::Batch*>(batch);
+    if (out_mode) *out_mode = b.mode;
+    if (out_groups) *out_groups = static_cast<uint32_t>(b.groups.size());
+    if (out_z_chunks) {
+        for (uint32_t i = 0; i < capacity && i < b.contexts.size(); ++i) out_z_chunks[i] = 0;
+        for (size_t k = 0; k < b.sims.size(); ++k)
+            if (static_cast<uint32_t>(b.order[k]) < capacity) out_z_chunks[b.order[k]] = b.sims[k].z_chunk;
+    }
     return STABLE_FLUIDS_RESULT_OK;
 }
 

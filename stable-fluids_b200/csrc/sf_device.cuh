@@ -217,15 +217,18 @@ __device__ __forceinline__ Cell locate(float x, float y, float z, float h) {
     return c;
 }
 
-// Interpolation in x, then y, then z, each as a + (b - a) * t.
+// Interpolation in x, then y, then z, each as a + (b - a) * t with the
+// product and the sum rounded once (one FMA): the contraction the compiler
+// applies to the reference's expression (backend-cuda.cu:231-237), written
+// out so that it does not depend on the code the function is inlined into.
 __device__ __forceinline__ float trilerp(float c000, float c100, float c010, float c110, float c001, float c101, float c011, float c111, const Cell& c) {
-    const float c00 = c000 + (c100 - c000) * c.tx;
-    const float c10 = c010 + (c110 - c010) * c.tx;
-    const float c01 = c001 + (c101 - c001) * c.tx;
-    const float c11 = c011 + (c111 - c011) * c.tx;
-    const float c0 = c00 + (c10 - c00) * c.ty;
-    const float c1 = c01 + (c11 - c01) * c.ty;
-    return c0 + (c1 - c0) * c.tz;
+    const float c00 = __fmaf_rn(c100 - c000, c.tx, c000);
+    const float c10 = __fmaf_rn(c110 - c010, c.tx, c010);
+    const float c01 = __fmaf_rn(c101 - c001, c.tx, c001);
+    const float c11 = __fmaf_rn(c111 - c011, c.tx, c011);
+    const float c0 = __fmaf_rn(c10 - c00, c.ty, c00);
+    const float c1 = __fmaf_rn(c11 - c01, c.ty, c01);
+    return __fmaf_rn(c1 - c0, c.tz, c0);
 }
 
 // Velocity (3 components) at a world position from the packed field.
@@ -257,12 +260,14 @@ __device__ __forceinline__ float3 sample_velocity3(const P* __restrict__ v, floa
 // Midpoint RK2 back-trace in world units (backend-cuda.cu:295-300).
 template <typename P>
 __device__ __forceinline__ float3 trace_rk2(float x, float y, float z, const P* __restrict__ v, float dt, const Dims& d, float h, const FlowBC& b) {
+    // x - (0.5 dt) v and x - dt v, each product and difference rounded once
     const float3 v0 = sample_velocity3(v, x, y, z, d, h, b);
-    const float mx = x - 0.5f * dt * v0.x;
-    const float my = y - 0.5f * dt * v0.y;
-    const float mz = z - 0.5f * dt * v0.z;
+    const float half_dt = __fmul_rn(0.5f, dt);
+    const float mx = __fmaf_rn(-half_dt, v0.x, x);
+    const float my = __fmaf_rn(-half_dt, v0.y, y);
+    const float mz = __fmaf_rn(-half_dt, v0.z, z);
     const float3 v1 = sample_velocity3(v, mx, my, mz, d, h, b);
-    return make_float3(x - dt * v1.x, y - dt * v1.y, z - dt * v1.z);
+    return make_float3(__fmaf_rn(-dt, v1.x, x), __fmaf_rn(-dt, v1.y, y), __fmaf_rn(-dt, v1.z, z));
 }
 
 }  // namespace sfb

@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 
+#include "sf_batch.cuh"
 #include "sf_device.cuh"
 #include "sf_launch.h"
 
@@ -31,10 +32,12 @@ unsigned linear_grid(size_t n, int threads) {
     return static_cast<unsigned>(g < cap ? (g == 0 ? 1 : g) : cap);
 }
 
-__device__ __forceinline__ bool cell_coords(const Dims& d, int& x, int& y, int& z) {
-    x = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
-    y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
-    z = static_cast<int>(blockIdx.z * blockDim.z + threadIdx.z);
+// Cell of this thread in block `blk` of a (kBX, kBY, kBZ) launch over the grid
+// (blockIdx for a single simulation, the work item's block in a batch).
+__device__ __forceinline__ bool cell_coords(const Dims& d, uint3 blk, int& x, int& y, int& z) {
+    x = static_cast<int>(blk.x * kBX + threadIdx.x);
+    y = static_cast<int>(blk.y * kBY + threadIdx.y);
+    z = static_cast<int>(blk.z * kBZ + threadIdx.z);
     return x < d.nx && y < d.ny && z < d.nz;
 }
 
@@ -80,12 +83,12 @@ __global__ void k_force_pack(ForceArgs a) {
 // per component, backend-cuda.cu:330-340; the trace is deterministic so the
 // results are identical), then a trilinear sample of the packed velocity.
 template <typename T, typename P>
-__global__ void __launch_bounds__(256) k_advect_velocity(const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) {
+__device__ __forceinline__ void advect_velocity_block(uint3 blk, const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) {
     int x, y, z;
-    if (!cell_coords(d, x, y, z)) return;
-    const float px = (static_cast<float>(x) + 0.5f) * h;
-    const float py = (static_cast<float>(y) + 0.5f) * h;
-    const float pz = (static_cast<float>(z) + 0.5f) * h;
+    if (!cell_coords(d, blk, x, y, z)) return;
+    const float px = __fmul_rn(static_cast<float>(x) + 0.5f, h);
+    const float py = __fmul_rn(static_cast<float>(y) + 0.5f, h);
+    const float pz = __fmul_rn(static_cast<float>(z) + 0.5f, h);
     const float3 t = trace_rk2(px, py, pz, v, dt, d, h, b);
     const float3 s = sample_velocity3(v, t.x, t.y, t.z, d, h, b);
     const size_t i = lin(x, y, z, d);
@@ -93,6 +96,9 @@ __global__ void __launch_bounds__(256) k_advect_velocity(const P* __restrict__ v
     oy[i] = from_f<T>(s.y);
     oz[i] = from_f<T>(s.z);
 }
+
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_advect_velocity(const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) { advect_velocity_block<T, P>(blockIdx, v, ox, oy, oz, dt, d, h, b); }
 
 // Scalar value after the source injection rho + dt * S at an interior cell,
 // or the fixed face value (the source never reaches a ghost).
@@ -110,12 +116,12 @@ __device__ __forceinline__ float sourced_scalar(const T* __restrict__ q, const f
 // followed by :342-352): each gathered corner is rho + dt * S, exactly the
 // value the reference stores before it advects.
 template <typename T, typename P>
-__global__ void __launch_bounds__(256) k_scalar_source_advect(const P* __restrict__ v, const T* __restrict__ q, const float* __restrict__ src, T* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) {
+__device__ __forceinline__ void scalar_source_advect_block(uint3 blk, const P* __restrict__ v, const T* __restrict__ q, const float* __restrict__ src, T* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) {
     int x, y, z;
-    if (!cell_coords(d, x, y, z)) return;
-    const float px = (static_cast<float>(x) + 0.5f) * h;
-    const float py = (static_cast<float>(y) + 0.5f) * h;
-    const float pz = (static_cast<float>(z) + 0.5f) * h;
+    if (!cell_coords(d, blk, x, y, z)) return;
+    const float px = __fmul_rn(static_cast<float>(x) + 0.5f, h);
+    const float py = __fmul_rn(static_cast<float>(y) + 0.5f, h);
+    const float pz = __fmul_rn(static_cast<float>(z) + 0.5f, h);
     float3 t = trace_rk2(px, py, pz, v, dt, d, h, fb);
     if (sb.periodic[0]) t.x = wrap_world(t.x, static_cast<float>(d.nx) * h);
     if (sb.periodic[1]) t.y = wrap_world(t.y, static_cast<float>(d.ny) * h);
@@ -126,6 +132,9 @@ __global__ void __launch_bounds__(256) k_scalar_source_advect(const P* __restric
     for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, sb);
     out[lin(x, y, z, d)] = from_f<T>(trilerp(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], c));
 }
+
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_scalar_source_advect(const P* __restrict__ v, const T* __restrict__ q, const float* __restrict__ src, T* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) { scalar_source_advect_block<T, P>(blockIdx, v, q, src, out, dt, d, h, fb, sb); }
 
 template <typename T>
 __global__ void k_scalar_source(T* __restrict__ q, const float* __restrict__ src, float dt, size_t n) {
@@ -150,11 +159,14 @@ __device__ __forceinline__ float divergence_at(const T* __restrict__ vx, const T
 
 // backend-cuda.cu:386-396
 template <typename T>
-__global__ void __launch_bounds__(256) k_divergence(float* __restrict__ div, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
+__device__ __forceinline__ void divergence_block(uint3 blk, float* __restrict__ div, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
     int x, y, z;
-    if (!cell_coords(d, x, y, z)) return;
+    if (!cell_coords(d, blk, x, y, z)) return;
     div[lin(x, y, z, d)] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
 }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_divergence(float* __restrict__ div, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) { divergence_block<T>(blockIdx, div, vx, vy, vz, d, h, b); }
 
 // --------------------------------------------------- residual reductions --
 __device__ __forceinline__ double warp_sum(double v) {
@@ -204,9 +216,9 @@ __device__ __forceinline__ void block_accumulate4(double a, double b, double c, 
 // float4 velocity for the scalar advection, and (stats != nullptr) adds the
 // FP64 residual terms of A p = b: e = h^2 div - (sum6(p) - 6 p).
 template <typename T, typename P>
-__global__ void __launch_bounds__(256) k_project(T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) {
+__device__ __forceinline__ void project_block(uint3 blk, T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) {
     int x, y, z;
-    const bool ok = cell_coords(d, x, y, z);
+    const bool ok = cell_coords(d, blk, x, y, z);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
     if (ok) {
         const float inv_2h = 0.5f / h;
@@ -237,9 +249,12 @@ __global__ void __launch_bounds__(256) k_project(T* __restrict__ vx, T* __restri
     if (stats) block_accumulate4(se, se2, sb, sb2, stats);
 }
 
-__global__ void __launch_bounds__(256) k_residual_sums(const float* __restrict__ p, const float* __restrict__ div, Dims d, float h2, FlowBC b, DeviceStats* stats) {
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_project(T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) { project_block<T, P>(blockIdx, vx, vy, vz, packed, p, div, d, h, h2, b, stats); }
+
+__device__ __forceinline__ void residual_sums_block(uint3 blk, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h2, FlowBC b, DeviceStats* stats) {
     int x, y, z;
-    const bool ok = cell_coords(d, x, y, z);
+    const bool ok = cell_coords(d, blk, x, y, z);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
     if (ok) {
         const size_t i = lin(x, y, z, d);
@@ -254,6 +269,8 @@ __global__ void __launch_bounds__(256) k_residual_sums(const float* __restrict__
     }
     block_accumulate4(se, se2, sb, sb2, stats);
 }
+
+__global__ void __launch_bounds__(256) k_residual_sums(const float* __restrict__ p, const float* __restrict__ div, Dims d, float h2, FlowBC b, DeviceStats* stats) { residual_sums_block(blockIdx, p, div, d, h2, b, stats); }
 
 // rel_res = ||b - A p|| / ||b||, with b's mean removed when the pressure
 // operator is singular (no OUTFLOW face: constants are in its null space).
@@ -322,13 +339,107 @@ __global__ void k_warm_start_commit(DeviceStats* learned, const DeviceStats* pla
 // ----------------------------------------------------------- diagnostics --
 // Post-projection divergence (backend-cuda.cu:670) and |u| (:424-434) in one pass.
 template <typename T>
-__global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
+__device__ __forceinline__ void post_diagnostics_block(uint3 blk, float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
     int x, y, z;
-    if (!cell_coords(d, x, y, z)) return;
+    if (!cell_coords(d, blk, x, y, z)) return;
     const size_t i = lin(x, y, z, d);
     div[i] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
     const float ux = to_f(vx[i]), uy = to_f(vy[i]), uz = to_f(vz[i]);
     mag[i] = sqrtf(ux * ux + uy * uy + uz * uz);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) { post_diagnostics_block<T>(blockIdx, div, mag, vx, vy, vz, d, h, b); }
+
+// ------------------------------------------------------- work-table batch --
+// One launch per stage over every simulation of a batch (sf_batch.h); each
+// work item runs the single-simulation block body above.
+
+// v += dt f for the simulation's force fields in order, then the packed copy
+// (the batch always advects, so the SoA velocity is not written here).
+__global__ void __launch_bounds__(256) k_batch_force_pack(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_LINEAR];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_LINEAR]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const size_t n = static_cast<size_t>(m.d.nx) * m.d.ny * m.d.nz;
+        const size_t i = static_cast<size_t>(w - first[si]) * 256u + threadIdx.x;
+        if (i >= n) continue;
+        float vx = m.vel[0][i], vy = m.vel[1][i], vz = m.vel[2][i];
+        for (int k = 0; k < m.force_count; ++k) {
+            vx += m.dt * m.force[k][0][i];
+            vy += m.dt * m.force[k][1][i];
+            vz += m.dt * m.force[k][2][i];
+        }
+        reinterpret_cast<float4*>(m.packed)[i] = pack4<float4>(vx, vy, vz);
+    }
+}
+
+__device__ __forceinline__ uint3 cell_block_of(uint32_t local, const Dims& d) {
+    return batch_block(local, static_cast<uint32_t>((d.nx + kBX - 1) / kBX), static_cast<uint32_t>((d.ny + kBY - 1) / kBY));
+}
+
+__global__ void __launch_bounds__(256) k_batch_advect_velocity(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_CELL];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        advect_velocity_block<float, float4>(cell_block_of(w - first[si], m.d), reinterpret_cast<const float4*>(m.packed), m.temp[0], m.temp[1], m.temp[2], m.dt, m.d, m.h, m.flow);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_scalar_source_advect(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_CELL];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        scalar_source_advect_block<float, float4>(cell_block_of(w - first[si], m.d), reinterpret_cast<const float4*>(m.packed), m.sdata, m.source, m.stemp, m.dt, m.d, m.h, m.flow, m.sbc);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_divergence(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_CELL];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        divergence_block<float>(cell_block_of(w - first[si], m.d), m.divergence, m.vel[0], m.vel[1], m.vel[2], m.d, m.h, m.flow);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_project(BatchTable t, int pack) {
+    const uint32_t* first = t.first[SHAPE_CELL];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        project_block<float, float4>(cell_block_of(w - first[si], m.d), m.vel[0], m.vel[1], m.vel[2], pack ? reinterpret_cast<float4*>(m.packed) : nullptr, m.pressure, m.divergence, m.d, m.h, m.h * m.h, m.flow, nullptr);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_post_diagnostics(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_CELL];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        post_diagnostics_block<float>(cell_block_of(w - first[si], m.d), m.divergence, m.magnitude, m.vel[0], m.vel[1], m.vel[2], m.d, m.h, m.flow);
+    }
+}
+
+// Per simulation: zero the residual sums (before the batched residual sums)
+// or turn them into rel_res (after), one thread per simulation.
+__global__ void k_batch_stats(BatchTable t, int finalize, int iterations) {
+    const int si = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (si >= t.nsims) return;
+    const BatchSim& m = t.sims[si];
+    DeviceStats* st = m.stats;
+    if (!finalize) {
+        st->sum_e = st->sum_e2 = st->sum_b = st->sum_b2 = 0.0;
+        return;
+    }
+    double rhs = 0.0;
+    const double n = static_cast<double>(m.d.nx) * m.d.ny * m.d.nz;
+    st->rel_residual = relative_residual(st, n, m.flow.any_outflow ? 0 : 1, &rhs);
+    st->rhs_norm = rhs;
+    st->iterations = iterations;
 }
 
 }  // namespace
@@ -426,6 +537,60 @@ cudaError_t launch_post_diagnostics(float* div, float* mag, const void* vx, cons
     SFB_STORAGE(bf16, (k_post_diagnostics<float><<<cell_grid(d), cell_block(), 0, s>>>(div, mag, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), d, h, b)),
                 (k_post_diagnostics<bf16_t><<<cell_grid(d), cell_block(), 0, s>>>(div, mag, static_cast<const bf16_t*>(vx), static_cast<const bf16_t*>(vy), static_cast<const bf16_t*>(vz), d, h, b)));
     return cudaGetLastError();
+}
+
+// ------------------------------------------------------ work-table batch --
+namespace {
+unsigned batch_grid(uint32_t total, int sms, int per_sm) {
+    const uint32_t cap = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm);
+    return total < cap ? (total == 0 ? 1u : total) : cap;
+}
+}  // namespace
+
+cudaError_t launch_batch_force_pack(const BatchTable& t, cudaStream_t s) {
+    k_batch_force_pack<<<batch_grid(t.total[SHAPE_LINEAR], t.sms, 8), 256, 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_advect_velocity(const BatchTable& t, cudaStream_t s) {
+    k_batch_advect_velocity<<<batch_grid(t.total[SHAPE_CELL], t.sms, 4), cell_block(), 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_scalar_source_advect(const BatchTable& t, cudaStream_t s) {
+    k_batch_scalar_source_advect<<<batch_grid(t.total[SHAPE_CELL], t.sms, 4), cell_block(), 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_divergence(const BatchTable& t, cudaStream_t s) {
+    k_batch_divergence<<<batch_grid(t.total[SHAPE_CELL], t.sms, 8), cell_block(), 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_project(const BatchTable& t, int pack, cudaStream_t s) {
+    k_batch_project<<<batch_grid(t.total[SHAPE_CELL], t.sms, 8), cell_block(), 0, s>>>(t, pack);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_post_diagnostics(const BatchTable& t, cudaStream_t s) {
+    k_batch_post_diagnostics<<<batch_grid(t.total[SHAPE_CELL], t.sms, 8), cell_block(), 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_stats(const BatchTable& t, int finalize, int iterations, cudaStream_t s) {
+    k_batch_stats<<<static_cast<unsigned>((t.nsims + 63) / 64), 64, 0, s>>>(t, finalize, iterations);
+    return cudaGetLastError();
+}
+
+uint32_t batch_blocks(const Dims& d, int shape, int z_chunk) {
+    if (shape == SHAPE_LINEAR) return static_cast<uint32_t>((static_cast<size_t>(d.nx) * d.ny * d.nz + 255) / 256);
+    if (shape == SHAPE_CELL) {
+        const dim3 g = cell_grid(d);
+        return g.x * g.y * g.z;
+    }
+    const uint32_t bx = static_cast<uint32_t>((d.nx / 4 + 31) / 32), by = static_cast<uint32_t>((d.ny + 3) / 4);
+    const uint32_t zc = static_cast<uint32_t>(z_chunk < 1 ? 1 : z_chunk);
+    return bx * by * ((static_cast<uint32_t>(d.nz) + zc - 1) / zc);
 }
 
 }  // namespace sfb

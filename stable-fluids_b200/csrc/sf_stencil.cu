@@ -15,6 +15,7 @@
 
 #include <climits>
 
+#include "sf_batch.cuh"
 #include "sf_device.cuh"
 #include "sf_launch.h"
 #include "sf_stencil_tb.cuh"
@@ -182,12 +183,13 @@ __device__ __forceinline__ float4 vec_above4(const float* x, int i, int z, const
 }
 
 
-// One Jacobi sweep dst = update(src).
+// One Jacobi sweep dst = update(src), block `blk` of the launch (blockIdx
+// for one simulation, the work item's block in a batch).
 template <int KIND>
-__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
-    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+__device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const double recip = tb::recip64(divisor);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
@@ -221,10 +223,10 @@ __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict
 // unchanged (no thread of this launch changes them, so rewriting the value
 // just read is harmless and keeps every store a full 16 bytes).
 template <int KIND>
-__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
-    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+__device__ __forceinline__ void rbgs_vec4_block(uint3 blk, float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+    const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const double recip = tb::recip64(divisor);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
@@ -252,6 +254,16 @@ __global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const flo
         below = cur;
         cur = above;
     }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    jacobi_vec4_block<KIND>(blockIdx, dst, src, rhs, coef, z_chunk, d, g);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+    rbgs_vec4_block<KIND>(blockIdx, x, rhs, coef, parity, z_chunk, d, g);
 }
 
 
@@ -550,11 +562,12 @@ __device__ __forceinline__ double vec_warp_sum(double v) {
     return v;
 }
 
-__global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __restrict__ p, const float* __restrict__ div, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
-    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+// Every thread of the block must call it (block-wide reduction).
+__device__ __forceinline__ void residual_vec_block(uint3 blk, const float* __restrict__ p, const float* __restrict__ div, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
+    const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
     if (x0 < d.nx && y < d.ny) {
-        const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+        const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
         const VecGhost4 v = vec_ghost4(x0, y, d, g);
         const int sz = d.nx * d.ny;
         int i = x0 + d.nx * (y + d.ny * zb);
@@ -606,6 +619,10 @@ __global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __r
         double* dst = threadIdx.x == 0 ? &stats->sum_e : threadIdx.x == 1 ? &stats->sum_e2 : threadIdx.x == 2 ? &stats->sum_b : &stats->sum_b2;
         atomicAdd(dst, t);
     }
+}
+
+__global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __restrict__ p, const float* __restrict__ div, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
+    residual_vec_block(blockIdx, p, div, h2, z_chunk, d, g, stats);
 }
 
 template <typename T = float>
@@ -889,6 +906,93 @@ bool tb_supported(const StencilArgs& a) {
     return true;
 }
 
+// ------------------------------------------------------- work-table batch --
+// The sweeps of every simulation of a batch in one launch (sf_batch.h): work
+// item w is block w - first[s] of simulation s's own vectorised launch, run
+// by the same block body as a single-simulation sweep.
+__device__ __forceinline__ uint3 vec_block_of(uint32_t local, const Dims& d) {
+    return batch_block(local, static_cast<uint32_t>((d.nx / 4 + 31) / 32), static_cast<uint32_t>((d.ny + kVecRows - 1) / kVecRows));
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_batch_rbgs(BatchTable t, int parity) {
+    const uint32_t* first = t.first[SHAPE_VEC];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_VEC]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const float coef = KIND == KIND_PRESSURE ? m.h * m.h : (KIND == KIND_SCALAR ? m.alpha_s : m.alpha_v);
+        rbgs_vec4_block<KIND>(vec_block_of(w - first[si], m.d), batch_field(m, KIND, BF_X), batch_field(m, KIND, BF_B), coef, parity, m.z_chunk, m.d, m.ghost[KIND]);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_batch_jacobi(BatchTable t, int dst, int src) {
+    const uint32_t* first = t.first[SHAPE_VEC];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_VEC]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const float coef = KIND == KIND_PRESSURE ? m.h * m.h : (KIND == KIND_SCALAR ? m.alpha_s : m.alpha_v);
+        jacobi_vec4_block<KIND>(vec_block_of(w - first[si], m.d), batch_field(m, KIND, dst), batch_field(m, KIND, src), batch_field(m, KIND, BF_B), coef, m.z_chunk, m.d, m.ghost[KIND]);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kVecRows) k_batch_residual(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_VEC];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_VEC]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        residual_vec_block(vec_block_of(w - first[si], m.d), m.pressure, m.divergence, m.h * m.h, m.z_chunk, m.d, m.ghost[KIND_PRESSURE], m.stats);
+        __syncthreads();  // the block's reduction buffer is reused by the next item
+    }
+}
+
+// dst <- src (src >= 0) or dst <- 0, over the linear shape.
+__global__ void __launch_bounds__(256) k_batch_copy(BatchTable t, int kind, int dst, int src) {
+    const uint32_t* first = t.first[SHAPE_LINEAR];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_LINEAR]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const size_t n = static_cast<size_t>(m.d.nx) * m.d.ny * m.d.nz;
+        const size_t i = static_cast<size_t>(w - first[si]) * 256u + threadIdx.x;
+        if (i < n) batch_field(m, kind, dst)[i] = src >= 0 ? batch_field(m, kind, src)[i] : 0.0f;
+    }
+}
+
+// Scalar dissipation after its diffusion: rho *= 1 / (1 + dt k) (k_scale_field).
+__global__ void __launch_bounds__(256) k_batch_scale_scalar(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_LINEAR];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_LINEAR]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const size_t n = static_cast<size_t>(m.d.nx) * m.d.ny * m.d.nz;
+        const size_t i = static_cast<size_t>(w - first[si]) * 256u + threadIdx.x;
+        if (i < n) m.sdata[i] = m.sdata[i] * m.scale_s;
+    }
+}
+
+template <typename Kernel>
+unsigned batch_grid_vec(uint32_t total, int sms, Kernel kernel) {
+    static int per_sm = [&] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 32 * kVecRows, 0) != cudaSuccess || n < 1) n = 4;
+        return n;
+    }();
+    const uint32_t cap = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm);
+    return total < cap ? (total == 0 ? 1u : total) : cap;
+}
+
+unsigned batch_grid_linear(uint32_t total, int sms) {
+    const uint32_t cap = static_cast<uint32_t>(sms) * 8u;
+    return total < cap ? (total == 0 ? 1u : total) : cap;
+}
+
+template <int KIND>
+cudaError_t batch_sweep(const BatchTable& t, int scheme, int parity, int dst, int src, cudaStream_t s) {
+    if (scheme == SCHEME_RBGS) k_batch_rbgs<KIND><<<batch_grid_vec(t.total[SHAPE_VEC], t.sms, k_batch_rbgs<KIND>), dim3(32, kVecRows), 0, s>>>(t, parity);
+    else k_batch_jacobi<KIND><<<batch_grid_vec(t.total[SHAPE_VEC], t.sms, k_batch_jacobi<KIND>), dim3(32, kVecRows), 0, s>>>(t, dst, src);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
@@ -928,6 +1032,35 @@ cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
     case KIND_PRESSURE: return run_simple<KIND_PRESSURE, float>(a, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+// ------------------------------------------------------ work-table batch --
+GhostRule make_ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb) { return ghost_rule(kind, fb, sb); }
+
+cudaError_t launch_batch_sweep(const BatchTable& t, int kind, int scheme, int parity, int dst, int src, cudaStream_t s) {
+    switch (kind) {
+        case KIND_VEL_X: return batch_sweep<KIND_VEL_X>(t, scheme, parity, dst, src, s);
+        case KIND_VEL_Y: return batch_sweep<KIND_VEL_Y>(t, scheme, parity, dst, src, s);
+        case KIND_VEL_Z: return batch_sweep<KIND_VEL_Z>(t, scheme, parity, dst, src, s);
+        case KIND_SCALAR: return batch_sweep<KIND_SCALAR>(t, scheme, parity, dst, src, s);
+        case KIND_PRESSURE: return batch_sweep<KIND_PRESSURE>(t, scheme, parity, dst, src, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_batch_copy(const BatchTable& t, int kind, int dst, int src, cudaStream_t s) {
+    k_batch_copy<<<batch_grid_linear(t.total[SHAPE_LINEAR], t.sms), 256, 0, s>>>(t, kind, dst, src);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_scale_scalar(const BatchTable& t, cudaStream_t s) {
+    k_batch_scale_scalar<<<batch_grid_linear(t.total[SHAPE_LINEAR], t.sms), 256, 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_residual_sums(const BatchTable& t, cudaStream_t s) {
+    k_batch_residual<<<batch_grid_vec(t.total[SHAPE_VEC], t.sms, k_batch_residual), dim3(32, kVecRows), 0, s>>>(t);
+    return cudaGetLastError();
 }
 
 }  // namespace sfb

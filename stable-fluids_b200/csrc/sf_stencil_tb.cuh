@@ -50,17 +50,6 @@
 
 namespace sfb {
 
-// Ghost value of a face in a stencil: self (Neumann / copy), a constant
-// (Dirichlet), or k - self (reflection about a prescribed wall value).
-enum GhostMode : int32_t { GHOST_COPY = 0, GHOST_CONST = 1, GHOST_REFLECT = 2 };
-
-struct GhostRule {
-    int32_t mode[6];
-    float k[6];
-    int32_t periodic[3];
-    int32_t pad;
-};
-
 struct TbArgs {
     const float* src;  // x at the start of the pass (null: zero)
     const float* b;    // right-hand side

@@ -43,6 +43,18 @@ enum StencilKind : int32_t {
     KIND_PRESSURE = 4 // Poisson pressure (pressure ghosts)
 };
 
+// Ghost value of a face in a stencil: self (Neumann / copy), a constant
+// (Dirichlet), or k - self (reflection about a prescribed wall value).
+enum GhostMode : int32_t { GHOST_COPY = 0, GHOST_CONST = 1, GHOST_REFLECT = 2 };
+
+// Face ghost rules of one field kind (see ghost_rule in sf_stencil.cu).
+struct GhostRule {
+    int32_t mode[6];
+    float k[6];
+    int32_t periodic[3];
+    int32_t pad;
+};
+
 // Device-side solver statistics, one per context (global memory).
 struct DeviceStats {
     double sum_e;       // sum of e = b - A p

@@ -9,6 +9,7 @@ None (zero-fill, as the ABI defines for a null pointer).
 from __future__ import annotations
 
 import ctypes
+import os
 from ctypes import byref, c_uint32, c_void_p
 
 import numpy as np
@@ -190,11 +191,21 @@ class Simulation:
 
 
 class Batch:
-    """Several Simulations stepped together: one graph launch per batch step
-    runs every simulation's step graph concurrently (stable_fluids_b200_batch_*)."""
+    """Several Simulations stepped together (stable_fluids_b200_batch_*).
 
-    def __init__(self, simulations):
+    mode: BATCH_GRAPHS (default: one graph of the simulations' step graphs)
+    or BATCH_WORK_TABLE (one persistent launch per stage over L2-sized groups
+    of simulations; needs simulations with the same stage structure). autotune: time the sweep tile
+    options per grid size at creation (work table), caching them in
+    `tile_cache` (a JSON file) when given. After creation, `mode` is the
+    layout in use, `groups` the number of L2-sized groups the work table runs
+    one after another, and `z_chunks` the planes per thread block of each
+    simulation's sweeps (work table)."""
+
+    def __init__(self, simulations, mode: int | None = None, autotune: bool = False, tile_cache: str | os.PathLike | None = None):
         import torch
+
+        from . import B200BatchOptions, BATCH_GRAPHS
 
         self.sims = list(simulations)
         if not self.sims:
@@ -202,13 +213,24 @@ class Batch:
         self.lib = self.sims[0].lib
         ctxs = (c_void_p * len(self.sims))(*[s.ctx for s in self.sims])
         h = c_void_p()
-        rc = self.lib.stable_fluids_b200_batch_create(ctxs, len(self.sims), byref(h))
+        opts = B200BatchOptions()
+        opts.mode = BATCH_GRAPHS if mode is None else int(mode)
+        opts.autotune = 1 if autotune else 0
+        self._cache = os.fsencode(str(tile_cache)) if tile_cache is not None else None
+        opts.tile_cache = self._cache
+        rc = self.lib.stable_fluids_b200_batch_create_ex(ctxs, len(self.sims), byref(opts), byref(h))
         if rc != RESULT_OK:
-            raise StableFluidsError("stable_fluids_b200_batch_create", rc)
+            raise StableFluidsError("stable_fluids_b200_batch_create_ex", rc)
         self.handle = h
         n, k, st = ctypes.c_uint32(0), ctypes.c_int32(0), c_void_p()
         self.lib.stable_fluids_b200_batch_info(h, byref(n), byref(k), byref(st))
         self.kernels_per_step = k.value
+        m, g = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        zc = (ctypes.c_int32 * len(self.sims))()
+        self.lib.stable_fluids_b200_batch_layout(h, byref(m), byref(g), zc, len(self.sims))
+        self.mode = m.value
+        self.groups = g.value
+        self.z_chunks = list(zc)
         self.stream = torch.cuda.ExternalStream(st.value, device=self.sims[0].device)
 
     def step(self, n: int = 1):

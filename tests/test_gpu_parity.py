@@ -348,25 +348,107 @@ def test_blocked_jacobi_matches_single_sweeps(kind, sf, lib, cuda):
     assert_bit_equal(outs[1], outs[0])
 
 
-@pytest.mark.gpu
-def test_batch_step_matches_single_contexts(sf, lib, cuda):
-    """A batch of differently sized contexts stepped through one graph gives
-    the same bits as stepping each context on its own."""
-    scenes = sf.scenes.batch_scenes(count=4, seed=7, steps=3)
-    single = []
+def _batch_vs_single(sf, lib, scenes, options=None, **batch_kw):
+    """Steps each scene alone, then all of them as one batch; returns the
+    batch layout and, per simulation, (batch outputs, single outputs, batch
+    stats, single stats)."""
+    single, single_stats = [], []
     for sc in scenes:
-        sim = sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib)
+        sim = sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib, options=options)
         sf.scenes.run(sim, sc)
         single.append(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)))
+        single_stats.append(sim.stats())
         sim.close()
-    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib) for sc in scenes]
+    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib, options=options) for sc in scenes]
     for sim, sc in zip(sims, scenes):
         sf.scenes.apply_inputs(sim, sc, 0)
-    with sf.Batch(sims) as batch:
-        assert batch.kernels_per_step == sum(s.info().kernels_per_step for s in sims)
+    out = []
+    with sf.Batch(sims, **batch_kw) as batch:
         batch.step(scenes[0].steps)
-    for sim, sc, ref in zip(sims, scenes, single):
-        assert_bit_equal(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), ref)
+        info = {"mode": batch.mode, "kernels": batch.kernels_per_step, "z_chunks": batch.z_chunks}
+    for sim, sc, ref, ref_st in zip(sims, scenes, single, single_stats):
+        out.append((C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), ref, sim.stats(), ref_st))
+        sim.close()
+    return info, out
+
+
+@pytest.mark.gpu
+def test_batch_graphs_match_single_contexts(sf, lib, cuda):
+    """GRAPHS layout: the contexts' step graphs as children of one graph give
+    the same bits as stepping each context on its own."""
+    scenes = sf.scenes.batch_scenes(count=4, seed=7, steps=3)
+    kernels = []
+    for sc in scenes:
+        sim = sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib)
+        kernels.append(sim.info().kernels_per_step)
+        sim.close()
+    info, out = _batch_vs_single(sf, lib, scenes, mode=sf.BATCH_GRAPHS)
+    assert info["mode"] == sf.BATCH_GRAPHS and info["kernels"] == sum(kernels)
+    for got, ref, _, _ in out:
+        assert_bit_equal(got, ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_batch_work_table_matches_single_contexts(scheme, sf, lib, cuda):
+    """WORK_TABLE layout: one persistent launch per stage over all
+    simulations (uneven sizes) gives the same bits as stepping each context on
+    its own, for both schemes (Jacobi with the previous-pressure start and the
+    per-simulation FP64 residual)."""
+    scenes = sf.scenes.batch_scenes(count=5, seed=11, steps=3)
+    opts = sf.default_options(lib)
+    opts.scheme = scheme
+    if scheme == 1:
+        opts.warm_start = sf.WARM_START_PREVIOUS
+        opts.compute_residual = 1
+    info, out = _batch_vs_single(sf, lib, scenes, options=opts, mode=sf.BATCH_WORK_TABLE)
+    assert info["mode"] == sf.BATCH_WORK_TABLE
+    assert all(z > 0 for z in info["z_chunks"])
+    for got, ref, st, ref_st in out:
+        assert_bit_equal(got, ref)
+        if scheme == 1:
+            assert st.pressure_iterations == ref_st.pressure_iterations
+            assert st.rel_residual == pytest.approx(ref_st.rel_residual, rel=1e-9, abs=1e-30)
+
+
+@pytest.mark.gpu
+def test_batch_work_table_autotune_and_cache(sf, lib, cuda, tmp_path):
+    """The tile autotuner picks a z chunk per grid size, writes the JSON
+    cache, and a second batch reads the same choices back; results stay
+    bit-equal to single contexts."""
+    import json
+
+    scenes = sf.scenes.batch_scenes(count=4, seed=3, steps=2)
+    cache = tmp_path / "tiles.json"
+    info, out = _batch_vs_single(sf, lib, scenes, mode=sf.BATCH_WORK_TABLE, autotune=True, tile_cache=cache)
+    for got, ref, _, _ in out:
+        assert_bit_equal(got, ref)
+    table = json.loads(cache.read_text())
+    sizes = {sc.config.nx for sc in scenes}
+    assert len(table) == len(sizes)
+    for key, zc in table.items():
+        n = int(key.rsplit("|", 1)[1].split("x")[2])
+        assert 1 <= zc <= n
+    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib) for sc in scenes]
+    with sf.Batch(sims, mode=sf.BATCH_WORK_TABLE, autotune=True, tile_cache=cache) as batch:
+        assert batch.z_chunks == info["z_chunks"]
+    for sim in sims:
+        sim.close()
+
+
+@pytest.mark.gpu
+def test_batch_work_table_needs_common_stages(sf, lib, cuda):
+    """Contexts whose stage structure differs (here BF16 storage in one of
+    them) batch as GRAPHS and are refused for WORK_TABLE."""
+    scenes = sf.scenes.batch_scenes(count=2, seed=5, steps=1)
+    bf = sf.default_options(lib)
+    bf.storage = sf.STORAGE_BF16
+    sims = [sf.Simulation(scenes[0].config, scenes[0].scalars, scenes[0].vectors, lib=lib), sf.Simulation(scenes[1].config, scenes[1].scalars, scenes[1].vectors, lib=lib, options=bf)]
+    with sf.Batch(sims) as batch:
+        assert batch.mode == sf.BATCH_GRAPHS
+    with pytest.raises(sf.StableFluidsError):
+        sf.Batch(sims, mode=sf.BATCH_WORK_TABLE)
+    for sim in sims:
         sim.close()
 
 
