@@ -275,7 +275,7 @@ def train_network(sf, args, device):
 
 
 def time_pressure_sweep(sf, scene, device):
-    """Average duration of one Jacobi pressure sweep (k_jacobi_vec), CUDA
+    """Average duration of one Jacobi pressure sweep (k_jacobi_vec4), CUDA
     events on the context stream: the fixed-count pressure stage of a Jacobi
     context enqueued directly (80 sweeps per stage)."""
     import torch
@@ -589,8 +589,8 @@ def main():
     cells = n ** 3
     bytes_per_sweep = 12 * cells
     achieved = bytes_per_sweep / sweep_s / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_jacobi_vec (Jacobi pressure sweep)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": 179.16e6 if n == 256 else None, "traffic_source": "ncu capture of k_jacobi_vec at 256^3: dram__bytes_read.sum 138.9 MB + dram__bytes_write.sum 40.2 MB", "bytes_per_launch": bytes_per_sweep, "launch_us": sweep_s * 1e6, "unit_of_work": "one Jacobi sweep of 256^3 cells: read p + rhs, write p = 12 B/cell"}
+    roofline = {"bound": "hbm", "kernel": "k_jacobi_vec4 (Jacobi pressure sweep)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": 177.19e6 if n == 256 else None, "traffic_source": "ncu capture of k_jacobi_vec4 (pressure) at 256^3: dram__bytes_read.sum 138.9 MB + dram__bytes_write.sum 38.3 MB", "bytes_per_launch": bytes_per_sweep, "launch_us": sweep_s * 1e6, "unit_of_work": "one Jacobi sweep of 256^3 cells: read p + rhs, write p = 12 B/cell"}
     roofline_network = None
     if net is not None:
         net_s = time_network(net, n, torch.device("cuda", local))

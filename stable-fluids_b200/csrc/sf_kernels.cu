@@ -83,7 +83,7 @@ __global__ void k_force_pack(ForceArgs a) {
 // per component, backend-cuda.cu:330-340; the trace is deterministic so the
 // results are identical), then a trilinear sample of the packed velocity.
 template <typename T, typename P>
-__device__ __forceinline__ void advect_velocity_block(uint3 blk, const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) {
+__device__ __forceinline__ void advect_velocity_block(uint3 blk, const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, const Dims& d, float h, const FlowBC& b) {
     int x, y, z;
     if (!cell_coords(d, blk, x, y, z)) return;
     const float px = __fmul_rn(static_cast<float>(x) + 0.5f, h);
@@ -116,7 +116,7 @@ __device__ __forceinline__ float sourced_scalar(const T* __restrict__ q, const f
 // followed by :342-352): each gathered corner is rho + dt * S, exactly the
 // value the reference stores before it advects.
 template <typename T, typename P>
-__device__ __forceinline__ void scalar_source_advect_block(uint3 blk, const P* __restrict__ v, const T* __restrict__ q, const float* __restrict__ src, T* __restrict__ out, float dt, Dims d, float h, FlowBC fb, ScalarBC sb) {
+__device__ __forceinline__ void scalar_source_advect_block(uint3 blk, const P* __restrict__ v, const T* __restrict__ q, const float* __restrict__ src, T* __restrict__ out, float dt, const Dims& d, float h, const FlowBC& fb, const ScalarBC& sb) {
     int x, y, z;
     if (!cell_coords(d, blk, x, y, z)) return;
     const float px = __fmul_rn(static_cast<float>(x) + 0.5f, h);
@@ -159,7 +159,7 @@ __device__ __forceinline__ float divergence_at(const T* __restrict__ vx, const T
 
 // backend-cuda.cu:386-396
 template <typename T>
-__device__ __forceinline__ void divergence_block(uint3 blk, float* __restrict__ div, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
+__device__ __forceinline__ void divergence_block(uint3 blk, float* __restrict__ div, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, const Dims& d, float h, const FlowBC& b) {
     int x, y, z;
     if (!cell_coords(d, blk, x, y, z)) return;
     div[lin(x, y, z, d)] = divergence_at(vx, vy, vz, x, y, z, d, h, b);
@@ -216,7 +216,7 @@ __device__ __forceinline__ void block_accumulate4(double a, double b, double c, 
 // float4 velocity for the scalar advection, and (stats != nullptr) adds the
 // FP64 residual terms of A p = b: e = h^2 div - (sum6(p) - 6 p).
 template <typename T, typename P>
-__device__ __forceinline__ void project_block(uint3 blk, T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) {
+__device__ __forceinline__ void project_block(uint3 blk, T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, const Dims& d, float h, float h2, const FlowBC& b, DeviceStats* stats) {
     int x, y, z;
     const bool ok = cell_coords(d, blk, x, y, z);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
@@ -252,7 +252,7 @@ __device__ __forceinline__ void project_block(uint3 blk, T* __restrict__ vx, T* 
 template <typename T, typename P>
 __global__ void __launch_bounds__(256) k_project(T* __restrict__ vx, T* __restrict__ vy, T* __restrict__ vz, P* __restrict__ packed, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h, float h2, FlowBC b, DeviceStats* stats) { project_block<T, P>(blockIdx, vx, vy, vz, packed, p, div, d, h, h2, b, stats); }
 
-__device__ __forceinline__ void residual_sums_block(uint3 blk, const float* __restrict__ p, const float* __restrict__ div, Dims d, float h2, FlowBC b, DeviceStats* stats) {
+__device__ __forceinline__ void residual_sums_block(uint3 blk, const float* __restrict__ p, const float* __restrict__ div, const Dims& d, float h2, const FlowBC& b, DeviceStats* stats) {
     int x, y, z;
     const bool ok = cell_coords(d, blk, x, y, z);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
@@ -339,7 +339,7 @@ __global__ void k_warm_start_commit(DeviceStats* learned, const DeviceStats* pla
 // ----------------------------------------------------------- diagnostics --
 // Post-projection divergence (backend-cuda.cu:670) and |u| (:424-434) in one pass.
 template <typename T>
-__device__ __forceinline__ void post_diagnostics_block(uint3 blk, float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) {
+__device__ __forceinline__ void post_diagnostics_block(uint3 blk, float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, const Dims& d, float h, const FlowBC& b) {
     int x, y, z;
     if (!cell_coords(d, blk, x, y, z)) return;
     const size_t i = lin(x, y, z, d);

@@ -186,7 +186,7 @@ __device__ __forceinline__ float4 vec_above4(const float* x, int i, int z, const
 // One Jacobi sweep dst = update(src), block `blk` of the launch (blockIdx
 // for one simulation, the work item's block in a batch).
 template <int KIND>
-__device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+__device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, const Dims& d, const GhostRule& g) {
     const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
@@ -223,7 +223,7 @@ __device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__
 // unchanged (no thread of this launch changes them, so rewriting the value
 // just read is harmless and keeps every store a full 16 bytes).
 template <int KIND>
-__device__ __forceinline__ void rbgs_vec4_block(uint3 blk, float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+__device__ __forceinline__ void rbgs_vec4_block(uint3 blk, float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, const Dims& d, const GhostRule& g) {
     const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
@@ -563,7 +563,7 @@ __device__ __forceinline__ double vec_warp_sum(double v) {
 }
 
 // Every thread of the block must call it (block-wide reduction).
-__device__ __forceinline__ void residual_vec_block(uint3 blk, const float* __restrict__ p, const float* __restrict__ div, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
+__device__ __forceinline__ void residual_vec_block(uint3 blk, const float* __restrict__ p, const float* __restrict__ div, float h2, int z_chunk, const Dims& d, const GhostRule& g, DeviceStats* stats) {
     const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
     if (x0 < d.nx && y < d.ny) {
