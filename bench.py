@@ -95,6 +95,7 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=20, help="steps of the batched 64-simulation workload (0: skip)")
     p.add_argument("--bf16-size", type=int, default=384)
     p.add_argument("--bf16-steps", type=int, default=5, help="timed steps of the FP32-vs-BF16-storage comparison (0: skip)")
+    p.add_argument("--scene-steps", type=int, default=10, help="steps of the viewer-scene force generator comparison (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--fixed-pressure-iterations", type=int, default=0,
@@ -462,6 +463,47 @@ def bf16_storage(sf, n, steps, warmup, device):
     return out
 
 
+def scene_generator(sf, n, steps, device):
+    """The reference viewer's per-step force update (vulkan-app/scene_plume.cpp:
+    323-335) at n^3: the library's device generator (one kernel writing force x
+    and z into the context) against the viewer's host path -- force x and z
+    from the host masks (vectorised NumPy here, faster than the viewer's scalar
+    loop), then two host-to-device copies through update_vector_field. The
+    device path is timed with CUDA events, the host path with the host clock
+    around device synchronizations. The host path's cost does not depend on
+    the mask values, so it runs on seeded random masks of the same size."""
+    import numpy as np
+    import torch
+
+    scene = sf.scenes.plume("viewer", (n, n, n), diffuse_iterations=20, pressure_iterations=40)
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, device=device)
+    sim.plume_scene_setup()
+    sim.plume_scene_forces(0)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(sim.stream)
+    for k in range(steps):
+        sim.plume_scene_forces(k + 1)
+    end.record(sim.stream)
+    torch.cuda.synchronize()
+    dev_s = start.elapsed_time(end) / 1000.0 / steps
+    rng = np.random.default_rng(0)
+    drift, swirl_x, swirl_z, fy = (rng.random((n, n, n), dtype=np.float32) for _ in range(4))
+    t0 = time.perf_counter()
+    for k in range(steps):
+        phase = np.float32(k + 1) * np.float32(0.045)
+        dx, dz, sw = np.float32(1.15) * np.sin(phase), np.float32(0.85) * np.cos(phase * np.float32(0.71)), np.float32(1.65) * np.cos(phase * np.float32(0.53))
+        fx = dx * drift + sw * swirl_x
+        fz = dz * drift + sw * swirl_z
+        sim.set_vector(sim.vector_handles[0], fx, fy, fz)
+    torch.cuda.synchronize()
+    host_s = (time.perf_counter() - t0) / steps
+    sim.close()
+    bytes_written = 2 * 4 * n ** 3
+    return {"grid": [n, n, n], "steps": steps, "device_us_per_step": dev_s * 1e6, "device_gbs": bytes_written / dev_s / 1e9, "host_path_ms_per_step": host_s * 1e3,
+            "speedup": host_s / dev_s, "h2d_bytes_saved_per_step": bytes_written}
+
+
 def cpu_baseline(sf, scene, plain_iterations):
     """The FP32 C++/OpenMP transcription of the step (oracle/) on all host
     cores: one step without pressure sweeps and one with 16 Jacobi sweeps,
@@ -611,6 +653,7 @@ def main():
         batch = batched(sf, None, args.batch_steps, args.warmup, mode="graphs")
         batch["work_table_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="work_table").items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "z_chunks_by_size", "layout_create_s", "l2_groups")}
     mixed = bf16_storage(sf, args.bf16_size, args.bf16_steps, args.warmup, local) if args.bf16_steps > 0 else None
+    viewer = scene_generator(sf, n, args.scene_steps, local) if args.scene_steps > 0 else None
 
     config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
               "grid": [n, n, n], "solver": {"learned": "Jacobi sweeps from the learned warm start", "plain": "Jacobi sweeps from zero", "previous": "Jacobi sweeps from the previous pressure", "rbgs": "red-black Gauss-Seidel from zero"}[headline]
@@ -620,7 +663,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
             "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"],
             "speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
-            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch, "bf16_storage": mixed}
+            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch, "bf16_storage": mixed, "viewer_scene_forces": viewer}
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c

@@ -214,6 +214,27 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_step(void* batch);
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_info(void* batch, uint32_t* out_count, int32_t* out_kernels_per_step, void** out_stream);
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_destroy(void* batch);
 
+/* ---- The reference viewer's plume scene on the device ----
+ * Replaces the per-step host work of vulkan-app/scene_plume.cpp:323-335 (a
+ * loop over every cell building the force's x and z components from three
+ * host masks, two host-to-device copies and an update_vector_field copy) with
+ * one kernel that evaluates the masks in closed form and writes the force
+ * straight into the context's force field: nothing crosses PCIe. The scene
+ * geometry is the viewer's (source at (0.50, 0.13, 0.50) of the domain,
+ * radius 6 cells; swirl and drift spheres above it), derived from the
+ * context's grid; the arithmetic is the viewer's float arithmetic, one
+ * rounding per operation, so the fields are the ones the viewer uploads.
+ * Both calls are asynchronous on the context stream.
+ *
+ * setup (scene_plume.cpp:267-300): density source 32 w and force y 7.6 w for
+ * the source sphere's weight w; force x and z zero.
+ * forces (:323-330): force x and z of animation step `animation_step`
+ * (phase = step * 0.045, drift_x = 1.15 sin(phase), drift_z =
+ * 0.85 cos(0.71 phase), swirl = 1.65 cos(0.53 phase), evaluated on the host
+ * with the C library's sinf / cosf as the viewer does). */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_plume_scene_setup(void* context, StableFluidsScalarFieldHandle density, StableFluidsVectorFieldHandle force);
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_plume_scene_forces(void* context, StableFluidsVectorFieldHandle force, int32_t animation_step);
+
 /* No counterpart in the reference. The FP64 relative Poisson residual
  * ||b - A p|| / ||b|| (b = h^2 divergence, mean removed when no face is
  * OUTFLOW; A p = sum of the 6 neighbours - 6 p with the pressure ghost rules)

@@ -139,6 +139,8 @@ B200_SYMBOLS = (
     "stable_fluids_b200_network_gradients",
     "stable_fluids_b200_network_train_step",
     "stable_fluids_b200_attach_network",
+    "stable_fluids_b200_plume_scene_setup",
+    "stable_fluids_b200_plume_scene_forces",
     "stable_fluids_b200_batch_create",
     "stable_fluids_b200_batch_create_ex",
     "stable_fluids_b200_batch_layout",
@@ -188,6 +190,8 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_network_gradients.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, POINTER(c_double), P, P]
         lib.stable_fluids_b200_network_train_step.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, c_float, POINTER(c_double), P]
         lib.stable_fluids_b200_attach_network.argtypes = [P, P]
+        lib.stable_fluids_b200_plume_scene_setup.argtypes = [P, c_uint32, c_uint32]
+        lib.stable_fluids_b200_plume_scene_forces.argtypes = [P, c_uint32, c_int32]
         lib.stable_fluids_b200_batch_create.argtypes = [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]
         lib.stable_fluids_b200_batch_create_ex.argtypes = [POINTER(c_void_p), c_uint32, POINTER(B200BatchOptions), POINTER(c_void_p)]
         lib.stable_fluids_b200_batch_layout.argtypes = [P, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_int32), c_uint32]

@@ -799,6 +799,48 @@ StableFluidsResult stable_fluids_b200_enqueue_stage(void* context, uint32_t stag
     return STABLE_FLUIDS_RESULT_OK;
 }
 
+// The viewer's plume geometry from the context's grid (scene_plume.cpp:229-246),
+// in the same float expressions.
+static sfb::PlumeGeometry plume_geometry(const Context& c) {
+    sfb::PlumeGeometry g{};
+    const float h = c.config.cell_size;
+    const float extent_x = static_cast<float>(c.dims.nx) * h;
+    const float extent_y = static_cast<float>(c.dims.ny) * h;
+    const float extent_z = static_cast<float>(c.dims.nz) * h;
+    g.h = h;
+    g.source_x = extent_x * 0.50f;
+    g.source_y = extent_y * 0.13f;
+    g.source_z = extent_z * 0.50f;
+    g.source_r = h * 6.0f;
+    g.swirl_y = g.source_y + g.source_r * 0.90f;
+    g.drift_y = g.source_y + g.source_r * 1.35f;
+    g.swirl_r = g.source_r * 1.65f;
+    g.drift_r = g.source_r * 2.10f;
+    return g;
+}
+
+StableFluidsResult stable_fluids_b200_plume_scene_setup(void* context, StableFluidsScalarFieldHandle density, StableFluidsVectorFieldHandle force) {
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    auto* f = sfb::scalar_field(c, density);
+    if (f == nullptr || force == 0 || force > c.vectors.size()) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& v = c.vectors[force - 1u];
+    return sfb::launch_plume_setup(f->source, v.data[0], v.data[1], v.data[2], plume_geometry(c), c.dims, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
+StableFluidsResult stable_fluids_b200_plume_scene_forces(void* context, StableFluidsVectorFieldHandle force, int32_t animation_step) {
+    if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    if (force == 0 || force > c.vectors.size()) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& v = c.vectors[force - 1u];
+    // the animated scalars as the viewer computes them (scene_plume.cpp:323-326)
+    const float phase = static_cast<float>(animation_step) * 0.045f;
+    const float drift_x = 1.15f * std::sin(phase);
+    const float drift_z = 0.85f * std::cos(phase * 0.71f);
+    const float swirl = 1.65f * std::cos(phase * 0.53f);
+    return sfb::launch_plume_forces(v.data[0], v.data[2], plume_geometry(c), c.dims, drift_x, drift_z, swirl, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
 StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network) {
     if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     auto& c = *static_cast<Context*>(context);

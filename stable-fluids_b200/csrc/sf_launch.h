@@ -72,6 +72,16 @@ cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int 
 // Learned warm start: keeps the candidate in p or replaces it by alt,
 // whichever has the smaller relative residual (two kernels).
 cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* plain, Dims d, int singular, float* p, const float* alt, cudaStream_t s);
+// The reference viewer's plume scene (sf_scene.cu): geometry in world units,
+// derived from the grid by plume_geometry (host).
+struct PlumeGeometry {
+    float h;
+    float source_x, source_y, source_z, source_r;
+    float swirl_y, swirl_r;
+    float drift_y, drift_r;
+};
+cudaError_t launch_plume_setup(float* source, float* fx, float* fy, float* fz, const PlumeGeometry& g, Dims d, cudaStream_t s);
+cudaError_t launch_plume_forces(float* fx, float* fz, const PlumeGeometry& g, Dims d, float drift_x, float drift_z, float swirl, cudaStream_t s);
 cudaError_t launch_post_diagnostics(float* div, float* mag, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s);
 
 }  // namespace sfb

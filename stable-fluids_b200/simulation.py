@@ -165,6 +165,20 @@ class Simulation:
         self._check(self.lib.stable_fluids_b200_get_step_info(self.ctx, byref(i)), "get_step_info")
         return i
 
+    def plume_scene_setup(self, density: int | None = None, force: int | None = None):
+        """The reference viewer's plume inputs, generated on the device: density
+        source and force y of the source sphere, force x and z zero
+        (stable_fluids_b200_plume_scene_setup)."""
+        d = self.scalar_handles[0] if density is None else density
+        f = self.vector_handles[0] if force is None else force
+        self._check(self.lib.stable_fluids_b200_plume_scene_setup(self.ctx, d, f), "plume_scene_setup")
+
+    def plume_scene_forces(self, animation_step: int, force: int | None = None):
+        """Force x and z of the viewer's plume for one animation step, written on
+        the device into the force field (stable_fluids_b200_plume_scene_forces)."""
+        f = self.vector_handles[0] if force is None else force
+        self._check(self.lib.stable_fluids_b200_plume_scene_forces(self.ctx, f, int(animation_step)), "plume_scene_forces")
+
     def enqueue_stage(self, stage: int) -> int:
         """Enqueues one stage outside the step graph; returns its kernel count."""
         n = ctypes.c_int32(0)
