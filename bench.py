@@ -96,6 +96,7 @@ def parse():
     p.add_argument("--bf16-size", type=int, default=384)
     p.add_argument("--bf16-steps", type=int, default=5, help="timed steps of the FP32-vs-BF16-storage comparison (0: skip)")
     p.add_argument("--scene-steps", type=int, default=10, help="steps of the viewer-scene force generator comparison (0: skip)")
+    p.add_argument("--render-frames", type=int, default=5, help="frames of the headless volume rendering measurement (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--fixed-pressure-iterations", type=int, default=0,
@@ -504,6 +505,44 @@ def scene_generator(sf, n, steps, device):
             "speedup": host_s / dev_s, "h2d_bytes_saved_per_step": bytes_written}
 
 
+def volume_render(sf, n, device, width=1920, height=1080, steps=256, frames=5):
+    """Headless ray-march of the density of an n^3 plume (the viewer's volume
+    shader restated in CUDA) into a width x height RGBA float image:
+    ms per frame (CUDA events) and samples per second (width * height *
+    steps is the bound; rays leave the box or stop early)."""
+    import numpy as np
+    import torch
+
+    scene = sf.scenes.config1(n=n)
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, device=device)
+    sf.scenes.run(sim, scene, 3)
+    ext = np.array([n * scene.config.cell_size] * 3, np.float32)
+    centre = ext / 2
+    eye = centre + np.array([0.35, 0.25, -1.6], np.float32) * ext.max()
+    fwd = (centre - eye) / np.linalg.norm(centre - eye)
+    right = np.cross(np.array([0, 1, 0], np.float32), fwd)
+    right /= np.linalg.norm(right)
+    up = np.cross(fwd, right)
+    p = sf.B200VolumeRender()
+    for k, val in {"eye": eye, "right": right, "up": up, "forward": fwd, "volume_min": np.zeros(3), "volume_max": ext, "color_a": (0.1, 0.2, 0.9), "color_b": (1.0, 0.6, 0.1)}.items():
+        getattr(p, k)[:] = [float(t) for t in val]
+    p.aspect, p.tan_half_fov, p.value_scale, p.density = width / height, 0.55, 1.0, 40.0
+    p.value_min, p.value_max, p.steps, p.projection, p.width, p.height = 0.0, 2.0, steps, 0, width, height
+    img = sim.render_volume(sf.VIEW_SCALAR_FIELD_DATA, p, sim.scalar_handles[0])
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(sim.stream)
+    for _ in range(frames):
+        sim.render_volume(sf.VIEW_SCALAR_FIELD_DATA, p, sim.scalar_handles[0], out=img)
+    end.record(sim.stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / frames
+    coverage = float((img[..., 3] > 0).float().mean())
+    sim.close()
+    return {"grid": [n, n, n], "image": [width, height], "steps": steps, "ms_per_frame": ms, "frames_per_s": 1000.0 / ms,
+            "max_samples_per_s": width * height * steps / (ms / 1000.0), "pixels_with_density": coverage}
+
+
 def cpu_baseline(sf, scene, plain_iterations):
     """The FP32 C++/OpenMP transcription of the step (oracle/) on all host
     cores: one step without pressure sweeps and one with 16 Jacobi sweeps,
@@ -654,6 +693,7 @@ def main():
         batch["work_table_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="work_table").items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "z_chunks_by_size", "layout_create_s", "l2_groups")}
     mixed = bf16_storage(sf, args.bf16_size, args.bf16_steps, args.warmup, local) if args.bf16_steps > 0 else None
     viewer = scene_generator(sf, n, args.scene_steps, local) if args.scene_steps > 0 else None
+    render = volume_render(sf, n, local, frames=args.render_frames) if args.render_frames > 0 else None
 
     config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
               "grid": [n, n, n], "solver": {"learned": "Jacobi sweeps from the learned warm start", "plain": "Jacobi sweeps from zero", "previous": "Jacobi sweeps from the previous pressure", "rbgs": "red-black Gauss-Seidel from zero"}[headline]
@@ -663,7 +703,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
             "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"],
             "speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
-            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch, "bf16_storage": mixed, "viewer_scene_forces": viewer}
+            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch, "bf16_storage": mixed, "viewer_scene_forces": viewer, "volume_render": render}
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c

@@ -235,6 +235,36 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_batch_destroy(void* batc
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_plume_scene_setup(void* context, StableFluidsScalarFieldHandle density, StableFluidsVectorFieldHandle force);
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_plume_scene_forces(void* context, StableFluidsVectorFieldHandle force, int32_t animation_step);
 
+/* ---- Headless volume rendering of a field ----
+ * The reference viewer's volume shader (vulkan-app/shaders/field_volume.slang)
+ * restated as a CUDA kernel: one primary ray per pixel through the field's
+ * box, `steps` equal steps, trilinear samples, emission/absorption
+ * compositing front to back, early exit below 1 % transmittance. The image is
+ * written to a caller-provided device buffer of width * height RGBA float4
+ * texels (row 0 at the top; colour premultiplied by alpha), instead of a
+ * swapchain image. The fields mirror the shader's push constants. */
+typedef struct StableFluidsB200VolumeRender {
+    float eye[3], right[3], up[3], forward[3];   /* camera basis (world units) */
+    float volume_min[3], volume_max[3];          /* the field's box in world units */
+    float color_a[3], color_b[3];                /* ramp ends (signed range: negative / positive colour) */
+    float aspect;                                /* width / height (params0.x) */
+    float tan_half_fov;                          /* perspective (params0.y) */
+    float value_scale;                           /* field multiplier (params0.z) */
+    float density;                               /* extinction per unit length (params0.w) */
+    float value_min, value_max;                  /* mapped range (params3.xy); a range spanning 0 is signed */
+    float ortho_height;                          /* orthographic view height (params3.w) */
+    uint32_t steps;                              /* march steps (params1.w) */
+    uint32_t projection;                         /* 0 perspective, else orthographic (params2.x) */
+    int32_t width, height;                       /* image size in pixels */
+    uint32_t reserved[4];
+} StableFluidsB200VolumeRender;
+
+/* Renders the field `field` selects (a single-array view kind: scalar data or
+ * source, velocity magnitude, pressure, divergence; FP32 as get_view returns
+ * it) into out_rgba (device memory, width * height * 4 floats), enqueued on
+ * the context stream after the work queued there. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_render_volume(void* context, const StableFluidsViewRequest* field, const StableFluidsB200VolumeRender* params, float* out_rgba);
+
 /* No counterpart in the reference. The FP64 relative Poisson residual
  * ||b - A p|| / ||b|| (b = h^2 divergence, mean removed when no face is
  * OUTFLOW; A p = sum of the 6 neighbours - 6 p with the pressure ghost rules)

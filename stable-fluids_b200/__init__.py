@@ -139,6 +139,7 @@ B200_SYMBOLS = (
     "stable_fluids_b200_network_gradients",
     "stable_fluids_b200_network_train_step",
     "stable_fluids_b200_attach_network",
+    "stable_fluids_b200_render_volume",
     "stable_fluids_b200_plume_scene_setup",
     "stable_fluids_b200_plume_scene_forces",
     "stable_fluids_b200_batch_create",
@@ -158,6 +159,16 @@ BATCH_GRAPHS, BATCH_WORK_TABLE = 0, 1
 
 class B200BatchOptions(ctypes.Structure):
     _fields_ = [("mode", c_uint32), ("autotune", c_uint32), ("tile_cache", ctypes.c_char_p), ("reserved", c_uint32 * 4)]
+
+
+class B200VolumeRender(ctypes.Structure):
+    _fields_ = [
+        ("eye", c_float * 3), ("right", c_float * 3), ("up", c_float * 3), ("forward", c_float * 3),
+        ("volume_min", c_float * 3), ("volume_max", c_float * 3), ("color_a", c_float * 3), ("color_b", c_float * 3),
+        ("aspect", c_float), ("tan_half_fov", c_float), ("value_scale", c_float), ("density", c_float),
+        ("value_min", c_float), ("value_max", c_float), ("ortho_height", c_float),
+        ("steps", c_uint32), ("projection", c_uint32), ("width", c_int32), ("height", c_int32), ("reserved", c_uint32 * 4),
+    ]
 
 
 class B200StepInfo(ctypes.Structure):
@@ -190,6 +201,7 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_network_gradients.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, POINTER(c_double), P, P]
         lib.stable_fluids_b200_network_train_step.argtypes = [P, P, P, P, c_int32, c_int32, c_int32, c_float, c_float, POINTER(c_double), P]
         lib.stable_fluids_b200_attach_network.argtypes = [P, P]
+        lib.stable_fluids_b200_render_volume.argtypes = [P, POINTER(ViewRequest), POINTER(B200VolumeRender), P]
         lib.stable_fluids_b200_plume_scene_setup.argtypes = [P, c_uint32, c_uint32]
         lib.stable_fluids_b200_plume_scene_forces.argtypes = [P, c_uint32, c_int32]
         lib.stable_fluids_b200_batch_create.argtypes = [POINTER(c_void_p), c_uint32, POINTER(c_void_p)]

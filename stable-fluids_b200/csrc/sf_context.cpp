@@ -841,6 +841,40 @@ StableFluidsResult stable_fluids_b200_plume_scene_forces(void* context, StableFl
     return sfb::launch_plume_forces(v.data[0], v.data[2], plume_geometry(c), c.dims, drift_x, drift_z, swirl, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
 }
 
+StableFluidsResult stable_fluids_b200_render_volume(void* context, const StableFluidsViewRequest* field, const StableFluidsB200VolumeRender* params, float* out_rgba) {
+    sfb::Range range("stable.render_volume");
+    if (context == nullptr || field == nullptr || params == nullptr || out_rgba == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (params->width <= 0 || params->height <= 0 || params->width > 16384 || params->height > 16384) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    StableFluidsView v{};
+    const StableFluidsResult r = stable_fluids_get_view_cuda(context, field, &v);
+    if (r != STABLE_FLUIDS_RESULT_OK) return r;
+    if (v.layout != STABLE_FLUIDS_VIEW_LAYOUT_F32_3D || v.data0 == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;  // one array only
+    sfb::RenderParams p{};
+    for (int k = 0; k < 3; ++k) {
+        p.eye[k] = params->eye[k];
+        p.right[k] = params->right[k];
+        p.up[k] = params->up[k];
+        p.forward[k] = params->forward[k];
+        p.volume_min[k] = params->volume_min[k];
+        p.volume_max[k] = params->volume_max[k];
+        p.color_a[k] = params->color_a[k];
+        p.color_b[k] = params->color_b[k];
+    }
+    p.aspect = params->aspect;
+    p.tan_half_fov = params->tan_half_fov;
+    p.value_scale = params->value_scale;
+    p.density = params->density;
+    p.value_min = params->value_min;
+    p.value_max = params->value_max;
+    p.ortho_height = params->ortho_height;
+    p.steps = params->steps;
+    p.projection = params->projection;
+    p.width = params->width;
+    p.height = params->height;
+    return sfb::launch_render_volume(static_cast<const float*>(v.data0), c.dims, p, out_rgba, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
 StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network) {
     if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     auto& c = *static_cast<Context*>(context);

@@ -82,6 +82,18 @@ struct PlumeGeometry {
 };
 cudaError_t launch_plume_setup(float* source, float* fx, float* fy, float* fz, const PlumeGeometry& g, Dims d, cudaStream_t s);
 cudaError_t launch_plume_forces(float* fx, float* fz, const PlumeGeometry& g, Dims d, float drift_x, float drift_z, float swirl, cudaStream_t s);
+// Volume ray-march of one FP32 field (sf_render.cu); the fields of
+// StableFluidsB200VolumeRender.
+struct RenderParams {
+    float eye[3], right[3], up[3], forward[3];
+    float volume_min[3], volume_max[3];
+    float color_a[3], color_b[3];
+    float aspect, tan_half_fov, value_scale, density;
+    float value_min, value_max, ortho_height;
+    uint32_t steps, projection;
+    int32_t width, height;
+};
+cudaError_t launch_render_volume(const float* field, Dims d, const RenderParams& p, float* out_rgba, cudaStream_t s);
 cudaError_t launch_post_diagnostics(float* div, float* mag, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s);
 
 }  // namespace sfb
