@@ -177,7 +177,9 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* con
  *    diffusion > 0, viscosity > 0, at most 4 force fields, nx % 4 == 0.
  *  - GRAPHS: the contexts' own step graphs as children of one CUDA graph; the
  *    simulations' kernels run concurrently. Any contexts except ones with a
- *    residual-driven solve (conditional graph nodes).
+ *    residual-driven solve (conditional graph nodes) and except two contexts
+ *    attached to the same warm-start network (they would use its buffers at
+ *    the same time).
  *
  * Both give the same bits as stepping each context alone. On B200 with 64
  * uneven simulations (32^3..128^3) GRAPHS is the faster layout (its 64

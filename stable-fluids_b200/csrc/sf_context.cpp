@@ -1292,6 +1292,11 @@ cudaError_t build_work_table(Batch& b, bool autotune, const char* cache_path) {
 }
 
 cudaError_t build_child_graphs(Batch& b) {
+    // The children run concurrently: two contexts using one warm-start
+    // network would share its activation buffers at the same time.
+    for (size_t i = 0; i < b.contexts.size(); ++i)
+        for (size_t j = i + 1; j < b.contexts.size(); ++j)
+            if (b.contexts[i]->network != nullptr && b.contexts[i]->network == b.contexts[j]->network) return cudaErrorInvalidValue;
     cudaError_t e = cudaGraphCreate(&b.graph, 0);
     if (e != cudaSuccess) return e;
     for (Context* c : b.contexts) {

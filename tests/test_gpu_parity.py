@@ -482,3 +482,28 @@ def test_bf16_storage_against_fp64_oracle(scheme, sf, lib, orc, cuda):
     for k, (e32, e16) in errs.items():
         assert e16 <= 2e-2, (k, errs)
         assert e32 <= 1e-4, (k, errs)
+
+
+@pytest.mark.gpu
+def test_batch_refuses_contexts_sharing_a_network(sf, lib, cuda):
+    """Two learned-start contexts attached to one warm-start network would use
+    its activation buffers concurrently inside a batch graph: refused; with a
+    network each they batch."""
+    scene = sf.scenes.plume("shared-net", (16, 16, 16), sources=[(8, 5, 8, 3.0, 10.0, 5.0)], diffuse_iterations=2, pressure_iterations=24)
+    opts = sf.default_options(lib)
+    opts.scheme = sf.SCHEME_JACOBI
+    opts.warm_start = sf.WARM_START_LEARNED
+    sims = [sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=opts) for _ in range(2)]
+    with sf.WarmStartNetwork(seed=0, lib=lib) as net, sf.WarmStartNetwork(seed=1, lib=lib) as other:
+        for sim in sims:
+            net.attach(sim)
+        with pytest.raises(sf.StableFluidsError):
+            sf.Batch(sims)
+        other.attach(sims[1])
+        with sf.Batch(sims) as batch:
+            batch.step(2)
+        for sim in sims:
+            sf.WarmStartNetwork.detach(sim)
+    for sim in sims:
+        assert np.isfinite(sim.fetch(sf.VIEW_FLOW_PRESSURE)).all()
+        sim.close()
