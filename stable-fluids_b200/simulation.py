@@ -168,12 +168,15 @@ class Simulation:
     def render_volume(self, kind: int, params, handle: int = 0, out=None):
         """Ray-marches the field of view kind `kind` (a single-array kind) into an
         RGBA float image (stable_fluids_b200_render_volume): a torch tensor
-        (height, width, 4) on the simulation's device, written on its stream."""
+        (height, width, 4) on the simulation's device. The image is written on
+        the simulation's stream; torch's current stream is made to wait for it."""
         torch = self._torch
         if out is None:
-            out = torch.empty((params.height, params.width, 4), dtype=torch.float32, device=self.device)
+            with torch.cuda.stream(self.stream):
+                out = torch.empty((params.height, params.width, 4), dtype=torch.float32, device=self.device)
         req = ViewRequest(kind=kind, scalar_field=handle if kind in (0, 1) else 0, vector_field=0, consumer_stream=c_void_p(self.stream.cuda_stream))
         self._check(self.lib.stable_fluids_b200_render_volume(self.ctx, byref(req), byref(params), c_void_p(out.data_ptr())), "render_volume")
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
         return out
 
     def plume_scene_setup(self, density: int | None = None, force: int | None = None):
