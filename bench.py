@@ -428,7 +428,7 @@ def batched(sf, lib, steps, warmup, count=64, mode=None):
     for sim in sims:
         sim.close()
     sizes = sorted({sc.config.nx for sc in scenes})
-    label = {"work_table": "one persistent launch per stage over a work table of all simulations (autotuned z chunks)", "graphs": "one graph of the simulations' step graphs per batch step", None: "each context stepped on its own stream"}[mode]
+    label = {"work_table": "one persistent launch per stage over a work table of L2-sized groups of simulations, groups on 4 concurrent streams (autotuned z chunks)", "graphs": "one graph of the simulations' step graphs per batch step", None: "each context stepped on its own stream"}[mode]
     return {"cell_updates_per_s": cells * steps / t, "steps_per_s": steps / t, "sims": count, "cells": cells, "sizes": sizes, "steps": steps, "timing": timing, "mode": label, **extra}
 
 
@@ -689,8 +689,8 @@ def main():
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
     batch = None
     if args.batch_steps > 0:
-        batch = batched(sf, None, args.batch_steps, args.warmup, mode="graphs")
-        batch["work_table_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="work_table").items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "z_chunks_by_size", "layout_create_s", "l2_groups")}
+        batch = batched(sf, None, args.batch_steps, args.warmup, mode="work_table")
+        batch["graphs_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="graphs").items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "layout_create_s")}
     mixed = bf16_storage(sf, args.bf16_size, args.bf16_steps, args.warmup, local) if args.bf16_steps > 0 else None
     viewer = scene_generator(sf, n, args.scene_steps, local) if args.scene_steps > 0 else None
     render = volume_render(sf, n, local, frames=args.render_frames) if args.render_frames > 0 else None

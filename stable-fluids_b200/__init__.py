@@ -158,7 +158,7 @@ BATCH_GRAPHS, BATCH_WORK_TABLE = 0, 1
 
 
 class B200BatchOptions(ctypes.Structure):
-    _fields_ = [("mode", c_uint32), ("autotune", c_uint32), ("tile_cache", ctypes.c_char_p), ("reserved", c_uint32 * 4)]
+    _fields_ = [("mode", c_uint32), ("autotune", c_uint32), ("tile_cache", ctypes.c_char_p), ("chains", c_uint32), ("reserved", c_uint32 * 3)]
 
 
 class B200VolumeRender(ctypes.Structure):

@@ -924,8 +924,13 @@ struct Batch {
     BatchSim* d_sims = nullptr;
     uint32_t* d_first = nullptr;
     std::vector<BatchTable> tables;              // one per group
+    int chains = 1;                              // groups captured round-robin on this many concurrent streams
+    std::vector<cudaStream_t> chain_streams;     // chains - 1 extra capture streams
+    std::vector<cudaEvent_t> chain_events;       // fork + one join event per extra stream
 
     ~Batch() {
+        for (auto ev : chain_events) cudaEventDestroy(ev);
+        for (auto st : chain_streams) cudaStreamDestroy(st);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (done) cudaEventDestroy(done);
@@ -1041,15 +1046,15 @@ cudaError_t upload_table(Batch& b) {
 }
 
 // Groups of simulations whose sweep working set (iterate, right-hand side
-// and scratch: 12 bytes per cell) fits in half the L2 cache: the batched step
-// runs group after group, so a group's hundreds of sweeps reread its fields
-// from L2 instead of HBM. Largest simulations first, first fit. Fills
+// and scratch: 12 bytes per cell) fits in half the L2 cache divided among the
+// concurrent chains: each chain runs its groups one after another, so a
+// group's hundreds of sweeps reread its fields from L2 instead of HBM. Largest simulations first, first fit. Fills
 // b.sims / b.order / b.groups; `make` builds one entry from a context index.
 template <typename Make>
 void group_by_l2(Batch& b, Make make) {
     int dev = 0, l2 = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0) l2 = 50 << 20;
-    const size_t budget = static_cast<size_t>(l2) / 2 / 12;  // cells per group
+    const size_t budget = static_cast<size_t>(l2) / 2 / 12 / static_cast<size_t>(b.chains);  // cells per group (chains run concurrently)
     std::vector<int> idx(b.contexts.size());
     for (size_t i = 0; i < idx.size(); ++i) idx[i] = static_cast<int>(i);
     std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return b.contexts[x]->cells > b.contexts[y]->cells; });
@@ -1086,6 +1091,7 @@ void group_by_l2(Batch& b, Make make) {
 // state changes), one size class at a time with the others fixed. Results
 // are kept in a flat JSON object {"<gpu>|<nx>x<ny>x<nz>": z_chunk, ...}.
 constexpr int kDefaultZChunk = 16;
+constexpr int kDefaultChains = 4;  // concurrent group chains of a work-table batch (measured best on B200: 3-4)
 
 std::string tile_key(const std::string& gpu, const Dims& d) { return gpu + "|" + std::to_string(d.nx) + "x" + std::to_string(d.ny) + "x" + std::to_string(d.nz); }
 
@@ -1209,6 +1215,7 @@ struct BatchStages {
     Batch& b;
     const BatchTable& t;  // the group's work table
     const Context& r;     // every context has r's stage structure
+    cudaStream_t s;       // the capture stream of the group's chain
     cudaError_t e = cudaSuccess;
     int launches = 0;
 
@@ -1220,65 +1227,89 @@ struct BatchStages {
     // One solve: the buffer sequence of run_simple (no temporal blocking).
     void solve(int kind, int init, int iterations) {
         if (r.options.scheme == STABLE_FLUIDS_B200_SCHEME_RBGS) {
-            if (init == INIT_FROM_B) ok(launch_batch_copy(t, kind, BF_X, BF_B, b.stream));
-            else if (init == INIT_ZERO) ok(launch_batch_copy(t, kind, BF_X, -1, b.stream));
+            if (init == INIT_FROM_B) ok(launch_batch_copy(t, kind, BF_X, BF_B, s));
+            else if (init == INIT_ZERO) ok(launch_batch_copy(t, kind, BF_X, -1, s));
             for (int it = 0; it < iterations; ++it)
-                for (int parity = 0; parity < 2; ++parity) ok(launch_batch_sweep(t, kind, SCHEME_RBGS, parity, BF_X, BF_X, b.stream));
+                for (int parity = 0; parity < 2; ++parity) ok(launch_batch_sweep(t, kind, SCHEME_RBGS, parity, BF_X, BF_X, s));
             return;
         }
         int src = BF_X;
         if (init == INIT_FROM_B) src = BF_B;
         else if (init == INIT_ZERO) {
             const int zero = (iterations & 1) ? BF_SCRATCH : BF_X;
-            ok(launch_batch_copy(t, kind, zero, -1, b.stream));
+            ok(launch_batch_copy(t, kind, zero, -1, s));
             src = zero;
         }
         if (iterations == 0) {
-            if (src != BF_X) ok(launch_batch_copy(t, kind, BF_X, src, b.stream));
+            if (src != BF_X) ok(launch_batch_copy(t, kind, BF_X, src, s));
             return;
         }
         for (int u = 0; u < iterations; ++u) {
             const int left = iterations - u;
             int dst = (left & 1) ? BF_X : BF_SCRATCH;
             if (dst == src) dst = dst == BF_X ? BF_SCRATCH : BF_X;
-            ok(launch_batch_sweep(t, kind, SCHEME_JACOBI, 0, dst, src, b.stream));
+            ok(launch_batch_sweep(t, kind, SCHEME_JACOBI, 0, dst, src, s));
             src = dst;
         }
-        if (src != BF_X) ok(launch_batch_copy(t, kind, BF_X, src, b.stream));
+        if (src != BF_X) ok(launch_batch_copy(t, kind, BF_X, src, s));
     }
 
     cudaError_t whole_step() {
         const int diffuse = r.config.diffuse_iterations, pressure = r.config.pressure_iterations;
-        ok(launch_batch_force_pack(t, b.stream));
-        ok(launch_batch_advect_velocity(t, b.stream));
+        ok(launch_batch_force_pack(t, s));
+        ok(launch_batch_advect_velocity(t, s));
         for (int comp = 0; comp < 3; ++comp) solve(KIND_VEL_X + comp, INIT_FROM_B, diffuse);
-        ok(launch_batch_divergence(t, b.stream));
+        ok(launch_batch_divergence(t, s));
         solve(KIND_PRESSURE, r.options.warm_start == STABLE_FLUIDS_B200_WARM_START_ZERO ? INIT_ZERO : INIT_FROM_X, pressure);
-        ok(launch_batch_project(t, 1, b.stream));
+        ok(launch_batch_project(t, 1, s));
         if (r.residual_enabled) {
-            ok(launch_batch_stats(t, 0, 0, b.stream));
-            ok(launch_batch_residual_sums(t, b.stream));
-            ok(launch_batch_stats(t, 1, pressure, b.stream));
+            ok(launch_batch_stats(t, 0, 0, s));
+            ok(launch_batch_residual_sums(t, s));
+            ok(launch_batch_stats(t, 1, pressure, s));
         }
-        ok(launch_batch_scalar_source_advect(t, b.stream));
+        ok(launch_batch_scalar_source_advect(t, s));
         solve(KIND_SCALAR, INIT_FROM_B, diffuse);
-        if (r.scalars[0].desc.dissipation > 0.0f) ok(launch_batch_scale_scalar(t, b.stream));
-        ok(launch_batch_post_diagnostics(t, b.stream));
+        if (r.scalars[0].desc.dissipation > 0.0f) ok(launch_batch_scale_scalar(t, s));
+        ok(launch_batch_post_diagnostics(t, s));
         return e;
     }
 };
 
-cudaError_t build_work_table(Batch& b, bool autotune, const char* cache_path) {
+cudaError_t build_work_table(Batch& b, bool autotune, const char* cache_path, int chains) {
+    b.chains = std::max(1, std::min(chains, 8));
+    cudaError_t e = cudaSuccess;
+    for (int c = 1; c < b.chains; ++c) {
+        cudaStream_t st = nullptr;
+        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        b.chain_streams.push_back(st);
+    }
+    for (int c = 0; c < b.chains; ++c) {  // [0] forks the chains, [c] joins chain c
+        cudaEvent_t ev = nullptr;
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+        b.chain_events.push_back(ev);
+    }
     group_by_l2(b, [&](int i) { return make_batch_sim(*b.contexts[i], std::min(kDefaultZChunk, b.contexts[i]->dims.nz)); });
-    cudaError_t e = autotune ? tune_tiles(b, cache_path) : upload_table(b);
+    e = autotune ? tune_tiles(b, cache_path) : upload_table(b);
     if (e != cudaSuccess) return e;
     if ((e = cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
     cudaError_t rec = cudaSuccess;
+    const auto step = [&](cudaError_t x) {
+        if (rec == cudaSuccess) rec = x;
+    };
+    if (b.chains > 1) {
+        step(cudaEventRecord(b.chain_events[0], b.stream));
+        for (auto st : b.chain_streams) step(cudaStreamWaitEvent(st, b.chain_events[0], 0));
+    }
     b.kernels = 0;
-    for (const auto& t : b.tables) {  // group after group: each group's step reuses L2
-        BatchStages st{b, t, *b.contexts.front()};
+    for (size_t g = 0; g < b.tables.size(); ++g) {  // chain c runs groups c, c + chains, ...: each group's step reuses L2
+        const size_t c = g % static_cast<size_t>(b.chains);
+        BatchStages st{b, b.tables[g], *b.contexts.front(), c == 0 ? b.stream : b.chain_streams[c - 1]};
         if (rec == cudaSuccess) rec = st.whole_step();
         b.kernels += st.launches;
+    }
+    for (int c = 1; c < b.chains; ++c) {
+        step(cudaEventRecord(b.chain_events[c], b.chain_streams[c - 1]));
+        step(cudaStreamWaitEvent(b.stream, b.chain_events[c], 0));
     }
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(b.stream, &g);
@@ -1340,7 +1371,7 @@ StableFluidsResult stable_fluids_b200_batch_create_ex(void* const* contexts, uin
     if (options->mode == STABLE_FLUIDS_B200_BATCH_WORK_TABLE) {
         if (!sfb::work_table_compatible(b->contexts)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         b->mode = STABLE_FLUIDS_B200_BATCH_WORK_TABLE;
-        e = sfb::build_work_table(*b, options->autotune != 0, options->tile_cache);
+        e = sfb::build_work_table(*b, options->autotune != 0, options->tile_cache, options->chains == 0 ? sfb::kDefaultChains : static_cast<int>(options->chains));
     } else {
         b->mode = STABLE_FLUIDS_B200_BATCH_GRAPHS;
         e = sfb::build_child_graphs(*b);

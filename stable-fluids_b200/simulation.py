@@ -223,14 +223,15 @@ class Batch:
 
     mode: BATCH_GRAPHS (default: one graph of the simulations' step graphs)
     or BATCH_WORK_TABLE (one persistent launch per stage over L2-sized groups
-    of simulations; needs simulations with the same stage structure). autotune: time the sweep tile
+    of simulations, groups on `chains` concurrent streams (0: 4); needs
+    simulations with the same stage structure; the faster layout). autotune: time the sweep tile
     options per grid size at creation (work table), caching them in
     `tile_cache` (a JSON file) when given. After creation, `mode` is the
     layout in use, `groups` the number of L2-sized groups the work table runs
     one after another, and `z_chunks` the planes per thread block of each
     simulation's sweeps (work table)."""
 
-    def __init__(self, simulations, mode: int | None = None, autotune: bool = False, tile_cache: str | os.PathLike | None = None):
+    def __init__(self, simulations, mode: int | None = None, autotune: bool = False, tile_cache: str | os.PathLike | None = None, chains: int = 0):
         import torch
 
         from . import B200BatchOptions, BATCH_GRAPHS
@@ -244,6 +245,7 @@ class Batch:
         opts = B200BatchOptions()
         opts.mode = BATCH_GRAPHS if mode is None else int(mode)
         opts.autotune = 1 if autotune else 0
+        opts.chains = int(chains)
         self._cache = os.fsencode(str(tile_cache)) if tile_cache is not None else None
         opts.tile_cache = self._cache
         rc = self.lib.stable_fluids_b200_batch_create_ex(ctxs, len(self.sims), byref(opts), byref(h))

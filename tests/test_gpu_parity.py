@@ -389,19 +389,19 @@ def test_batch_graphs_match_single_contexts(sf, lib, cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("scheme", [0, 1])
-def test_batch_work_table_matches_single_contexts(scheme, sf, lib, cuda):
+@pytest.mark.parametrize("scheme,chains", [(0, 1), (1, 1), (0, 3)])
+def test_batch_work_table_matches_single_contexts(scheme, chains, sf, lib, cuda):
     """WORK_TABLE layout: one persistent launch per stage over all
     simulations (uneven sizes) gives the same bits as stepping each context on
     its own, for both schemes (Jacobi with the previous-pressure start and the
-    per-simulation FP64 residual)."""
+    per-simulation FP64 residual) and with the groups on concurrent streams."""
     scenes = sf.scenes.batch_scenes(count=5, seed=11, steps=3)
     opts = sf.default_options(lib)
     opts.scheme = scheme
     if scheme == 1:
         opts.warm_start = sf.WARM_START_PREVIOUS
         opts.compute_residual = 1
-    info, out = _batch_vs_single(sf, lib, scenes, options=opts, mode=sf.BATCH_WORK_TABLE)
+    info, out = _batch_vs_single(sf, lib, scenes, options=opts, mode=sf.BATCH_WORK_TABLE, chains=chains)
     assert info["mode"] == sf.BATCH_WORK_TABLE
     assert all(z > 0 for z in info["z_chunks"])
     for got, ref, st, ref_st in out:
