@@ -195,7 +195,8 @@ def max_over_ranks(x: float, world: int, device=None) -> float:
 def solver_options(sf, variant, tol, cap, trial):
     o = sf.default_options()
     o.scheme = sf.SCHEME_RBGS if variant == "rbgs" else sf.SCHEME_JACOBI
-    o.warm_start = {"learned": sf.WARM_START_LEARNED, "plain": sf.WARM_START_ZERO, "previous": sf.WARM_START_PREVIOUS, "rbgs": sf.WARM_START_ZERO}[variant]
+    o.warm_start = {"learned": sf.WARM_START_LEARNED, "learned_coarse": sf.WARM_START_LEARNED, "plain": sf.WARM_START_ZERO, "previous": sf.WARM_START_PREVIOUS, "rbgs": sf.WARM_START_ZERO}[variant]
+    o.warm_start_coarsening = 1 if variant == "learned_coarse" else 0
     o.compute_residual = 1
     o.residual_tolerance = tol
     o.residual_check_interval = CHECK_INTERVAL
@@ -224,7 +225,7 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
         config = type(scene.config).from_buffer_copy(scene.config)
         config.pressure_iterations = args.fixed_pressure_iterations
     sim = sf.Simulation(config, scene.scalars, scene.vectors, options=opts, device=device)
-    if variant == "learned":
+    if variant.startswith("learned"):
         net.attach(sim)
     sf.scenes.apply_inputs(sim, scene, 0)
     sim.step(args.warmup)
@@ -245,13 +246,13 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
     barrier(world)
     t = sum(a.elapsed_time(b) for a, b in events) / 1000.0
     t = max_over_ranks(t, world)
-    trial_done = args.trial if variant == "learned" else 0
+    trial_done = args.trial if variant.startswith("learned") else 0
     if args.fixed_pressure_iterations:
         launches = info.kernels_per_step * args.steps
     else:
         launches = sum(launches_per_step(info.kernels_per_step, i, trial_done, variant == "rbgs") for i in its)
     out = {"steps_per_s": world * args.steps / t, "ms_per_step": 1000.0 * t / args.steps, "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > args.tolerance for r in res), "gpu_launches": launches}
-    if variant == "learned":
+    if variant.startswith("learned"):
         out["used_fallback"] = fallback
         out["trial_sweeps"] = args.trial
     return sim, out
@@ -643,12 +644,12 @@ def main():
 
     variants = [v for v in args.variants.split(",") if v]
     headline = "learned" if "learned" in variants else variants[0]  # profiling runs may leave the network out
-    net, train_info = train_network(sf, args, local) if "learned" in variants else (None, None)
+    net, train_info = train_network(sf, args, local) if any(v.startswith("learned") for v in variants) else (None, None)
 
     results, sims = {}, {}
     with Clocks(local, not args.no_clocks and rank == 0) as clk:
         for v in variants:
-            sim, out = run_variant(sf, scene, v, args, world, local, net if v == "learned" else None)
+            sim, out = run_variant(sf, scene, v, args, world, local, net if v.startswith("learned") else None)
             results[v] = out
             if v == "learned":
                 sims[v] = sim

@@ -62,7 +62,12 @@ typedef struct StableFluidsB200Options {
                                           * previous-pressure start before the one with the smaller
                                           * rel_res is kept (0 = compare the starts themselves) */
     uint32_t storage;                 /* StableFluidsB200Storage */
-    uint32_t reserved[7];
+    uint32_t warm_start_coarsening;   /* learned warm start: 1 = the network runs on the grid
+                                       * coarsened 2x in each axis (cell averages of the
+                                       * divergence and the previous pressure), and its
+                                       * correction is prolonged trilinearly to the grid; needs
+                                       * even nx, ny, nz (else the full grid is used) */
+    uint32_t reserved[6];
 } StableFluidsB200Options;
 
 /* Statistics of the most recent step (device values copied to the host). */

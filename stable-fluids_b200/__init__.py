@@ -104,7 +104,7 @@ class B200Options(ctypes.Structure):
         ("scheme", c_uint32), ("warm_start", c_uint32), ("iterations_per_pass", c_int32),
         ("residual_tolerance", c_float), ("max_pressure_iterations", c_int32),
         ("residual_check_interval", c_int32), ("compute_residual", c_uint32),
-        ("warm_start_trial_iterations", c_int32), ("storage", c_uint32), ("reserved", c_uint32 * 7),
+        ("warm_start_trial_iterations", c_int32), ("storage", c_uint32), ("warm_start_coarsening", c_uint32), ("reserved", c_uint32 * 6),
     ]
 
 

@@ -89,6 +89,12 @@ struct Context {
     float* alt = nullptr;
     float* alt_scratch = nullptr;
     DeviceStats* alt_stats = nullptr;
+    // coarse-grid prediction: restricted divergence and previous pressure,
+    // the network's coarse output (null: the network runs on the full grid)
+    float* coarse_b = nullptr;
+    float* coarse_p = nullptr;
+    float* coarse_out = nullptr;
+    Dims coarse_dims() const { return Dims{dims.nx / 2, dims.ny / 2, dims.nz / 2, 0}; }
     std::vector<ScalarField> scalars;
     std::vector<VectorField> vectors;
 
@@ -182,6 +188,7 @@ void apply_env_overrides(StableFluidsB200Options& o) {
         else if (s == "learned" || s == "2") o.warm_start = STABLE_FLUIDS_B200_WARM_START_LEARNED;
     }
     if (env_flag("STABLE_FLUIDS_B200_COMPUTE_RESIDUAL")) o.compute_residual = 1;
+    if (env_flag("STABLE_FLUIDS_B200_WARM_START_COARSEN")) o.warm_start_coarsening = 1;
     if (const char* v = std::getenv("STABLE_FLUIDS_B200_STORAGE")) {
         const std::string_view s(v);
         if (s == "bf16" || s == "BF16" || s == "1") o.storage = STABLE_FLUIDS_B200_STORAGE_BF16;
@@ -342,7 +349,16 @@ struct Stages {
         if (!residual_driven) trial = std::min(trial, c.config.pressure_iterations);
         ok(cudaMemcpyAsync(c.alt, c.pressure, c.field_bytes, cudaMemcpyDeviceToDevice, c.stream), 0);
         int predicted = 0;
-        if (ok(net::predict(c.network, c.divergence, h() * h(), c.pressure, c.pressure, c.dims, c.stream, &predicted), 0)) launches += predicted;
+        if (c.coarse_b != nullptr) {
+            // the network on the 2x coarser grid (cell size 2h), its correction prolonged
+            const float h2c = (2.0f * h()) * (2.0f * h());
+            ok(launch_restrict2(c.divergence, c.coarse_b, c.dims, c.stream));
+            ok(launch_restrict2(c.pressure, c.coarse_p, c.dims, c.stream));
+            if (ok(net::predict(c.network, c.coarse_b, h2c, c.coarse_p, c.coarse_out, c.coarse_dims(), c.stream, &predicted), 0)) launches += predicted;
+            ok(launch_prolong_add(c.coarse_out, c.coarse_p, c.pressure, c.dims, c.stream));
+        } else if (ok(net::predict(c.network, c.divergence, h() * h(), c.pressure, c.pressure, c.dims, c.stream, &predicted), 0)) {
+            launches += predicted;
+        }
         if (trial > 0) {
             ok(launch_stencil(stencil(KIND_PRESSURE, INIT_FROM_X, trial, h() * h(), c.pressure, c.divergence), c.stream), 0);
             auto a = stencil(KIND_PRESSURE, INIT_FROM_X, trial, h() * h(), c.alt, c.divergence);
@@ -563,6 +579,12 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
             plan.add(reinterpret_cast<void**>(&c->alt), fb);
             plan.add(reinterpret_cast<void**>(&c->alt_scratch), fb);
             plan.add(reinterpret_cast<void**>(&c->alt_stats), sizeof(DeviceStats));
+            if (options.warm_start_coarsening != 0 && c->dims.nx % 2 == 0 && c->dims.ny % 2 == 0 && c->dims.nz % 2 == 0) {
+                const size_t cb = fb / 8;
+                plan.add(reinterpret_cast<void**>(&c->coarse_b), cb);
+                plan.add(reinterpret_cast<void**>(&c->coarse_p), cb);
+                plan.add(reinterpret_cast<void**>(&c->coarse_out), cb);
+            }
         }
         for (auto& f : c->scalars) {
             plan.add(reinterpret_cast<void**>(&f.data), sb);
@@ -882,7 +904,7 @@ StableFluidsResult stable_fluids_b200_attach_network(void* context, void* networ
     auto* n = static_cast<sfb::net::Net*>(network);
     if (cudaStreamSynchronize(c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     // the network's buffers for this grid are allocated before the capture
-    if (n != nullptr && sfb::net::prepare(n, c.dims) != cudaSuccess) {
+    if (n != nullptr && sfb::net::prepare(n, c.coarse_b != nullptr ? c.coarse_dims() : c.dims) != cudaSuccess) {
         cudaGetLastError();
         return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     }

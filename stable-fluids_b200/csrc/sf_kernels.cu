@@ -442,6 +442,41 @@ __global__ void k_batch_stats(BatchTable t, int finalize, int iterations) {
     st->iterations = iterations;
 }
 
+// ----------------------------------------- coarse learned warm start --
+// Mean of each 2x2x2 block (fine dims even).
+__global__ void __launch_bounds__(256) k_restrict2(const float* __restrict__ fine, float* __restrict__ coarse, Dims f) {
+    const Dims c{f.nx / 2, f.ny / 2, f.nz / 2, 0};
+    int x, y, z;
+    if (!cell_coords(c, blockIdx, x, y, z)) return;
+    const size_t sy = static_cast<size_t>(f.nx), sz = static_cast<size_t>(f.nx) * f.ny;
+    const size_t i = lin(2 * x, 2 * y, 2 * z, f);
+    const float s = ((fine[i] + fine[i + 1]) + (fine[i + sy] + fine[i + sy + 1])) + ((fine[i + sz] + fine[i + sz + 1]) + (fine[i + sz + sy] + fine[i + sz + sy + 1]));
+    coarse[lin(x, y, z, c)] = 0.125f * s;
+}
+
+// Cell-centred trilinear prolongation of the coarse correction: fine cell 2X
+// sits at coarse coordinate X - 1/4 and 2X + 1 at X + 1/4 (weights 3/4, 1/4;
+// clamped at the faces).
+__global__ void __launch_bounds__(256) k_prolong_add(const float* __restrict__ cnew, const float* __restrict__ cold, float* __restrict__ p, Dims f) {
+    const Dims c{f.nx / 2, f.ny / 2, f.nz / 2, 0};
+    int x, y, z;
+    if (!cell_coords(f, blockIdx, x, y, z)) return;
+    const int X = x >> 1, Y = y >> 1, Z = z >> 1;
+    const int X2 = (x & 1) ? min(X + 1, c.nx - 1) : max(X - 1, 0);
+    const int Y2 = (y & 1) ? min(Y + 1, c.ny - 1) : max(Y - 1, 0);
+    const int Z2 = (z & 1) ? min(Z + 1, c.nz - 1) : max(Z - 1, 0);
+    const auto corr = [&](int a, int b, int d) {
+        const size_t k = lin(a, b, d, c);
+        return cnew[k] - cold[k];
+    };
+    const float c00 = 0.75f * corr(X, Y, Z) + 0.25f * corr(X2, Y, Z);
+    const float c10 = 0.75f * corr(X, Y2, Z) + 0.25f * corr(X2, Y2, Z);
+    const float c01 = 0.75f * corr(X, Y, Z2) + 0.25f * corr(X2, Y, Z2);
+    const float c11 = 0.75f * corr(X, Y2, Z2) + 0.25f * corr(X2, Y2, Z2);
+    const float v = 0.75f * (0.75f * c00 + 0.25f * c10) + 0.25f * (0.75f * c01 + 0.25f * c11);
+    p[lin(x, y, z, f)] += v;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- launchers --
@@ -591,6 +626,17 @@ uint32_t batch_blocks(const Dims& d, int shape, int z_chunk) {
     const uint32_t bx = static_cast<uint32_t>((d.nx / 4 + 31) / 32), by = static_cast<uint32_t>((d.ny + 3) / 4);
     const uint32_t zc = static_cast<uint32_t>(z_chunk < 1 ? 1 : z_chunk);
     return bx * by * ((static_cast<uint32_t>(d.nz) + zc - 1) / zc);
+}
+
+cudaError_t launch_restrict2(const float* fine, float* coarse, Dims fine_dims, cudaStream_t s) {
+    const Dims c{fine_dims.nx / 2, fine_dims.ny / 2, fine_dims.nz / 2, 0};
+    k_restrict2<<<cell_grid(c), cell_block(), 0, s>>>(fine, coarse, fine_dims);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prolong_add(const float* coarse_new, const float* coarse_old, float* fine_p, Dims fine_dims, cudaStream_t s) {
+    k_prolong_add<<<cell_grid(fine_dims), cell_block(), 0, s>>>(coarse_new, coarse_old, fine_p, fine_dims);
+    return cudaGetLastError();
 }
 
 }  // namespace sfb

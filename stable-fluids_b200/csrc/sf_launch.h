@@ -72,6 +72,12 @@ cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int 
 // Learned warm start: keeps the candidate in p or replaces it by alt,
 // whichever has the smaller relative residual (two kernels).
 cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* plain, Dims d, int singular, float* p, const float* alt, cudaStream_t s);
+// Learned warm start on the coarsened grid: coarse = mean of each 2x2x2
+// block of fine (fine dims even); fine_p += trilinear prolongation of
+// (coarse_new - coarse_old) to the fine cell centres.
+cudaError_t launch_restrict2(const float* fine, float* coarse, Dims fine_dims, cudaStream_t s);
+cudaError_t launch_prolong_add(const float* coarse_new, const float* coarse_old, float* fine_p, Dims fine_dims, cudaStream_t s);
+
 // The reference viewer's plume scene (sf_scene.cu): geometry in world units,
 // derived from the grid by plume_geometry (host).
 struct PlumeGeometry {

@@ -171,6 +171,33 @@ def test_selection_never_worse_than_previous(sf, lib, cuda, net):
     assert learned[0].pressure_iterations == previous[0].pressure_iterations
 
 
+def test_coarse_grid_prediction(sf, lib, cuda, net):
+    """warm_start_coarsening = 1: the network runs on the 2x coarser grid
+    (restricted divergence and previous pressure) and its correction is
+    prolonged; the step graph gains the two restrictions and the prolongation,
+    and with the trial as long as the solve the kept start is still at least as
+    good as the previous pressure."""
+    net.set_parameters(random_parameters(7))
+    scene = scene_32(sf, steps=3)
+    kernels, stats = {}, {}
+    for coarse in (0, 1):
+        o = jacobi_options(sf, lib, sf.WARM_START_LEARNED, trial=scene.config.pressure_iterations)
+        o.warm_start_coarsening = coarse
+        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=o)
+        net.attach(sim)
+        kernels[coarse] = sim.info().kernels_per_step
+        sf.scenes.run(sim, scene)
+        stats[coarse] = sim.stats()
+        assert np.isfinite(sim.fetch(sf.VIEW_FLOW_PRESSURE)).all()
+        sim.close()
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=jacobi_options(sf, lib, sf.WARM_START_PREVIOUS))
+    sf.scenes.run(sim, scene)
+    previous = sim.stats()
+    sim.close()
+    assert kernels[1] == kernels[0] + 3
+    assert stats[1].rel_residual <= previous.rel_residual * (1 + 1e-6)
+
+
 def test_training_gives_better_starts(sf, lib, cuda):
     """Train on pairs from one plume run and check on held-out steps of the
     same run that the predicted start has a smaller residual than the
