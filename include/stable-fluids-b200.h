@@ -194,8 +194,9 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* con
  * steps/s). The batch is
  * ordered after the work queued on each context's stream and each context's
  * stream after the batch, so update/view calls keep working as for a single
- * context. The batch reads the contexts' configuration when it is created:
- * rebuild it after stable_fluids_b200_attach_network. */
+ * context. The batch reads the contexts' configuration and field addresses
+ * when it is created: rebuild it after stable_fluids_b200_attach_network, and
+ * destroy it before any of its contexts. */
 typedef enum StableFluidsB200BatchMode {
     STABLE_FLUIDS_B200_BATCH_GRAPHS = 0,     /* the default; any batchable contexts */
     STABLE_FLUIDS_B200_BATCH_WORK_TABLE = 1, /* BACKEND_FAILURE when the contexts do not allow it */
