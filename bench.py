@@ -244,14 +244,15 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
         fallback.append(st.used_fallback)
     torch.cuda.synchronize()
     barrier(world)
-    t = sum(a.elapsed_time(b) for a, b in events) / 1000.0
+    per_step = [a.elapsed_time(b) for a, b in events]
+    t = sum(per_step) / 1000.0
     t = max_over_ranks(t, world)
     trial_done = args.trial if variant.startswith("learned") else 0
     if args.fixed_pressure_iterations:
         launches = info.kernels_per_step * args.steps
     else:
         launches = sum(launches_per_step(info.kernels_per_step, i, trial_done, variant == "rbgs") for i in its)
-    out = {"steps_per_s": world * args.steps / t, "ms_per_step": 1000.0 * t / args.steps, "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > args.tolerance for r in res), "gpu_launches": launches}
+    out = {"steps_per_s": world * args.steps / t, "ms_per_step": 1000.0 * t / args.steps, "ms_per_step_median": statistics.median(per_step), "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > args.tolerance for r in res), "gpu_launches": launches}
     if variant.startswith("learned"):
         out["used_fallback"] = fallback
         out["trial_sweeps"] = args.trial
