@@ -423,133 +423,106 @@ bool vec_ok(const StencilArgs& a, int width = 4) {
     return a.dims.nx % width == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
 }
 
-// Two Jacobi sweeps per pass (temporal blocking): a CTA owns a TX x TY
-// column of the grid over a z chunk and marches up it. Per plane step it
-// stages the input plane q + 1 (tile + 2-cell halo) and the right-hand side
-// (tile + 1-cell halo) in shared memory, computes the first sweep on plane q
-// over the tile + 1-cell halo into a 3-plane ring, and the second sweep on
-// plane q - 1 over the tile from that ring, writing only the result of both
-// sweeps to HBM: 12 bytes per cell per two sweeps. The halo ring of the first
-// sweep is recomputed by neighbouring CTAs. Face ghosts are applied inline
-// from the kind's GhostRule (periodic axes read wrapped coordinates), and
-// the per-cell arithmetic is k_jacobi_vec's, so two sweeps here are
-// bit-identical to two single sweeps. The next plane's loads are issued into
-// registers before the current plane is computed.
-constexpr int kTbX = 32, kTbY = 32, kTbThreads = 256;
-constexpr int kTb0W = kTbX + 4, kTb0H = kTbY + 4;  // sweep-1 input tile
-constexpr int kTb1W = kTbX + 2, kTb1H = kTbY + 2;  // sweep-1 output / rhs tile
-constexpr int kTbLoad0 = (kTb0W * kTb0H + kTbThreads - 1) / kTbThreads;
-constexpr int kTbLoad1 = (kTb1W * kTb1H + kTbThreads - 1) / kTbThreads;
-
-__device__ __forceinline__ int wrap_if(int c, int n, int periodic) { return periodic ? (c < 0 ? c + n : (c >= n ? c - n : c)) : c; }
+// Two Jacobi sweeps per pass (temporal blocking), for the vectorised grids
+// (nx % 4 == 0): a CTA owns an output tile of kT2OX x kT2OY cells over a z
+// chunk and marches up it. Each of its kT2G x kT2R threads owns one float4 of
+// the input tile (the output tile plus a halo of two float4 groups in x and
+// two rows in y) and keeps its column's input planes q-1, q, q+1 and its
+// first-sweep planes in registers, so z neighbours never touch shared
+// memory. Per plane q: every thread stores its input float4 of plane q into a
+// two-slot shared ring and one barrier follows; the inner (kT2G-2) x
+// (kT2R-2) threads compute the first sweep at plane q from the x/y
+// neighbours in shared memory and store it into a second two-slot ring; the
+// output threads compute the second sweep at plane q-1 from the first-sweep
+// ring (written one plane earlier, before this plane's barrier) and write it.
+// Loads of plane q+2 are issued two planes ahead. One barrier per plane is
+// enough: a ring slot is rewritten only two planes after it was read, and
+// every thread has passed the barrier in between. Face ghosts are the
+// GhostRule of the float4 sweep (self value substituted and mirrored, copied
+// or fixed), periodic axes are read wrapped, and the per-cell arithmetic and
+// sum order are k_jacobi_vec4's, so two sweeps here are bit-identical to two
+// single sweeps. Algorithmic traffic: 12 B per cell per two sweeps.
+constexpr int kT2G = 12, kT2R = 20;                       // input float4 groups per row, input rows
+constexpr int kT2Threads = kT2G * kT2R;                   // 240
+constexpr int kT2OX = 4 * (kT2G - 4), kT2OY = kT2R - 4;   // output tile: 32 x 16 cells
+constexpr int kT2W = 4 * kT2G;                            // floats per shared row
 
 template <int KIND>
-__global__ void __launch_bounds__(kTbThreads) k_jacobi_tb2(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
-    __shared__ float s0[3][kTb0H][kTb0W];  // input planes, slot = plane mod 3
-    __shared__ float s1[3][kTb1H][kTb1W];  // first-sweep planes, slot = plane mod 3
-    __shared__ float sr[4][kTb1H][kTb1W];  // right-hand side planes, slot = plane mod 4
-    const int tid = static_cast<int>(threadIdx.x);
-    const int x0 = static_cast<int>(blockIdx.x) * kTbX, y0 = static_cast<int>(blockIdx.y) * kTbY;
+__global__ void __launch_bounds__(kT2Threads) k_jacobi_tb2(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    __shared__ __align__(16) float s_in[2][kT2R][kT2W];
+    __shared__ __align__(16) float s_s1[2][kT2R][kT2W];
+    const int t = static_cast<int>(threadIdx.x);
+    const int gi = t % kT2G, ri = t / kT2G;
+    const int gx = static_cast<int>(blockIdx.x) * kT2OX + 4 * (gi - 2);  // first cell of this thread's float4 (unwrapped)
+    const int gy = static_cast<int>(blockIdx.y) * kT2OY + ri - 2;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const double recip = tb::recip64(divisor);
-    const int sy = d.nx, sz = d.nx * d.ny;
-    const int px = g.periodic[0], py = g.periodic[1], pz = g.periodic[2];
-    const auto mod3 = [](int q) { return ((q % 3) + 3) % 3; };
-    const auto mod4 = [](int q) { return q & 3; };  // two's complement: also right for q < 0
-
-    // in-plane offset of each element this thread stages (-1: outside the grid)
-    int off0[kTbLoad0], off1[kTbLoad1];
-#pragma unroll
-    for (int k = 0; k < kTbLoad0; ++k) {
-        const int i = tid + k * kTbThreads;
-        off0[k] = -1;
-        if (i < kTb0W * kTb0H) {
-            const int gx = wrap_if(x0 - 2 + i % kTb0W, d.nx, px), gy = wrap_if(y0 - 2 + i / kTb0W, d.ny, py);
-            if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny)) off0[k] = gx + sy * gy;
-        }
+    // the stored column this float4 reads: wrapped on periodic axes, absent outside a non-periodic one
+    int lx = gx, ly = gy;
+    bool live = true;
+    if (lx < 0 || lx >= d.nx) {
+        if (g.periodic[0]) lx = ((lx % d.nx) + d.nx) % d.nx;
+        else live = false;
     }
-#pragma unroll
-    for (int k = 0; k < kTbLoad1; ++k) {
-        const int i = tid + k * kTbThreads;
-        off1[k] = -1;
-        if (i < kTb1W * kTb1H) {
-            const int gx = wrap_if(x0 - 1 + i % kTb1W, d.nx, px), gy = wrap_if(y0 - 1 + i / kTb1W, d.ny, py);
-            if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny)) off1[k] = gx + sy * gy;
-        }
+    if (ly < 0 || ly >= d.ny) {
+        if (g.periodic[1]) ly = ((ly % d.ny) + d.ny) % d.ny;
+        else live = false;
     }
-    // stored plane of plane index q (periodic wrap), -1 outside a non-periodic grid
-    const auto plane = [&](int q) { return pz ? (q < 0 ? q + d.nz : (q >= d.nz ? q - d.nz : q)) : (static_cast<unsigned>(q) < static_cast<unsigned>(d.nz) ? q : -1); };
-    float r0[kTbLoad0], r1[kTbLoad1];
-    const auto fetch = [&](int q) {  // input and rhs of plane q into registers
+    const int col = live ? lx + d.nx * ly : 0;
+    const int sz = d.nx * d.ny;
+    const bool s1_thread = live && gi >= 1 && gi <= kT2G - 2 && ri >= 1 && ri <= kT2R - 2;
+    const bool out_thread = gi >= 2 && gi <= kT2G - 3 && ri >= 2 && ri <= kT2R - 3 && gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny;
+    const bool fx_lo = !g.periodic[0] && gx == 0, fx_hi = !g.periodic[0] && gx + 4 == d.nx;
+    const bool fy_lo = !g.periodic[1] && gy == 0, fy_hi = !g.periodic[1] && gy == d.ny - 1;
+    const auto plane = [&](int q) { return g.periodic[2] ? (q < 0 ? q + d.nz : (q >= d.nz ? q - d.nz : q)) : (static_cast<unsigned>(q) < static_cast<unsigned>(d.nz) ? q : -1); };
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const auto load = [&](const float* f, int q) {
         const int pq = plane(q);
-#pragma unroll
-        for (int k = 0; k < kTbLoad0; ++k) r0[k] = (pq >= 0 && off0[k] >= 0) ? src[off0[k] + sz * pq] : 0.0f;
-#pragma unroll
-        for (int k = 0; k < kTbLoad1; ++k) r1[k] = (pq >= 0 && off1[k] >= 0) ? rhs[off1[k] + sz * pq] : 0.0f;
+        return (live && pq >= 0) ? ld4(f + col + sz * pq) : zero;
     };
-    const auto stage = [&](int q) {  // registers -> the ring slots of plane q
-#pragma unroll
-        for (int k = 0; k < kTbLoad0; ++k) {
-            const int i = tid + k * kTbThreads;
-            if (i < kTb0W * kTb0H) (&s0[mod3(q)][0][0])[i] = r0[k];
-        }
-#pragma unroll
-        for (int k = 0; k < kTbLoad1; ++k) {
-            const int i = tid + k * kTbThreads;
-            if (i < kTb1W * kTb1H) (&sr[mod4(q)][0][0])[i] = r1[k];
-        }
+    // one update of this thread's float4 from the ring slot `ring` (x/y
+    // neighbours) and its own z neighbours, with the face ghosts
+    const auto sweep = [&](const float (*ring)[kT2W], float4 cur, float4 below, float4 above, float4 r, int q) {
+        float a = ring[ri][4 * gi - 1], b = ring[ri][4 * gi + 4];
+        float4 c = *reinterpret_cast<const float4*>(&ring[ri - 1][4 * gi]);
+        float4 e = *reinterpret_cast<const float4*>(&ring[ri + 1][4 * gi]);
+        if (fx_lo) a = tb::ghost(g, XM, cur.x);
+        if (fx_hi) b = tb::ghost(g, XP, cur.w);
+        if (fy_lo) c = ghost4(g, YM, cur);
+        if (fy_hi) e = ghost4(g, YP, cur);
+        if (!g.periodic[2] && q == 0) below = ghost4(g, ZM, cur);
+        if (!g.periodic[2] && q == d.nz - 1) above = ghost4(g, ZP, cur);
+        float4 o;
+        o.x = vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip);
+        o.y = vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip);
+        o.z = vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip);
+        o.w = vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip);
+        return o;
     };
-    // one cell update from a 3-plane ring (slot = plane mod 3); (hx, hy) are
-    // the cell's ring coordinates, q its plane, (gx, gy) its grid coordinates
-    const auto cell = [&](const float* ring, int W, int H, int hx, int hy, int q, int gx, int gy, float b) {
-        const int n = W * H, at = hy * W + hx;
-        const float* c = ring + mod3(q) * n + at;
-        const float self = *c;
-        const float xm = (!px && gx == 0) ? tb::ghost(g, XM, self) : c[-1];
-        const float xp = (!px && gx == d.nx - 1) ? tb::ghost(g, XP, self) : c[1];
-        const float ym = (!py && gy == 0) ? tb::ghost(g, YM, self) : c[-W];
-        const float yp = (!py && gy == d.ny - 1) ? tb::ghost(g, YP, self) : c[W];
-        const float zm = (!pz && q == 0) ? tb::ghost(g, ZM, self) : ring[mod3(q - 1) * n + at];
-        const float zp = (!pz && q == d.nz - 1) ? tb::ghost(g, ZP, self) : ring[mod3(q + 1) * n + at];
-        return tb::divide(tb::numerator<KIND>(xm + xp + ym + yp + zm + zp, b, coef), divisor, recip);
-    };
-
-    // Iteration q stages input plane q + 1, runs the first sweep on plane q
-    // and the second sweep on plane q - 1. Input planes zb - 2 and zb - 1 are
-    // staged before the loop.
-    fetch(zb - 2);
-    stage(zb - 2);
-    fetch(zb - 1);
-    stage(zb - 1);
-    fetch(zb);
+    // registers at the start of plane q = zb - 1: input q-1, q, q+1 and q+2 (in flight), rhs q and q+1
+    float4 in_m = load(src, zb - 2), in_c = load(src, zb - 1), in_p = load(src, zb), in_n = load(src, zb + 1);
+    float4 rhs_c = load(rhs, zb - 1), rhs_n = load(rhs, zb), rhs_m = zero;
+    float4 s1_mm = zero, s1_m = zero;
     for (int q = zb - 1; q <= ze; ++q) {
-        stage(q + 1);
-        if (q + 2 <= ze + 1) fetch(q + 2);
-        __syncthreads();  // input plane q + 1 staged; the second sweep of q - 2 done with s1 slot mod3(q)
-        if (plane(q) >= 0) {
-#pragma unroll
-            for (int k = 0; k < kTbLoad1; ++k) {
-                const int i = tid + k * kTbThreads;
-                if (i < kTb1W * kTb1H) {
-                    const int hx = i % kTb1W, hy = i / kTb1W;
-                    const int gx = wrap_if(x0 - 1 + hx, d.nx, px), gy = wrap_if(y0 - 1 + hy, d.ny, py);
-                    if (static_cast<unsigned>(gx) < static_cast<unsigned>(d.nx) && static_cast<unsigned>(gy) < static_cast<unsigned>(d.ny))
-                        s1[mod3(q)][hy][hx] = cell(&s0[0][0][0], kTb0W, kTb0H, hx + 1, hy + 1, q, gx, gy, sr[mod4(q)][hy][hx]);
-                }
-            }
-        }
-        __syncthreads();  // first-sweep plane q complete
+        *reinterpret_cast<float4*>(&s_in[q & 1][ri][4 * gi]) = in_c;
+        const float4 in_nn = (q + 3 <= ze + 1) ? load(src, q + 3) : zero;
+        const float4 rhs_nn = (q + 2 <= ze) ? load(rhs, q + 2) : zero;
+        __syncthreads();  // input plane q staged; the first sweep of plane q - 1 is visible
+        float4 s1 = zero;
+        if (s1_thread && plane(q) >= 0) s1 = sweep(s_in[q & 1], in_c, in_m, in_p, rhs_c, plane(q));
+        *reinterpret_cast<float4*>(&s_s1[q & 1][ri][4 * gi]) = s1;
         const int qo = q - 1;
-        if (qo >= zb && qo < ze) {
-#pragma unroll
-            for (int k = 0; k < (kTbX * kTbY) / kTbThreads; ++k) {
-                const int i = tid + k * kTbThreads;
-                const int tx = i % kTbX, ty = i / kTbX;
-                const int gx = x0 + tx, gy = y0 + ty;
-                if (gx < d.nx && gy < d.ny) dst[gx + sy * gy + sz * qo] = cell(&s1[0][0][0], kTb1W, kTb1H, tx + 1, ty + 1, qo, gx, gy, sr[mod4(qo)][ty + 1][tx + 1]);
-            }
-        }
+        if (out_thread && qo >= zb && qo < ze) *reinterpret_cast<float4*>(dst + col + sz * qo) = sweep(s_s1[qo & 1], s1_m, s1_mm, s1, rhs_m, qo);
+        s1_mm = s1_m;
+        s1_m = s1;
+        in_m = in_c;
+        in_c = in_p;
+        in_p = in_n;
+        in_n = in_nn;
+        rhs_m = rhs_c;
+        rhs_c = rhs_n;
+        rhs_n = rhs_nn;
     }
 }
 
@@ -640,13 +613,13 @@ template <typename Kernel>
 TbShape2 tb2_shape(const Dims& d, Kernel kernel) {
     static int per_sm = [&] {
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kTbThreads, 0) != cudaSuccess || n < 1) n = 2;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kT2Threads, 0) != cudaSuccess || n < 1) n = 2;
         return n;
     }();
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int bx = (d.nx + kTbX - 1) / kTbX, by = (d.ny + kTbY - 1) / kTbY;
+    const int bx = (d.nx + kT2OX - 1) / kT2OX, by = (d.ny + kT2OY - 1) / kT2OY;
     long long chunks = static_cast<long long>(sms) * per_sm / (static_cast<long long>(bx) * by);
     if (chunks < 1) chunks = 1;
     int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
@@ -707,7 +680,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
         // With blocking requested, sweeps go two per pass (k_jacobi_tb2, FP32)
         // where the grid suits the vectorised kernels, an odd sweep first as
-        // a single sweep. (On B200 the single-sweep kernel is faster today.)
+        // a single sweep. (On B200 two single sweeps are faster: the fused
+        // pass is instruction-bound.)
         constexpr bool kFp32 = sizeof(T) == sizeof(float);
         const int pairs = (kFp32 && vec && a.blocked) ? a.iterations / 2 : 0;
         const int singles = a.iterations - 2 * pairs;
@@ -733,7 +707,7 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             T* dst = (left & 1) ? ax : ascr;
             if (dst == src) dst = (dst == ax) ? ascr : ax;
             if (u >= singles) {
-                if constexpr (kFp32) k_jacobi_tb2<KIND><<<tb.grid, kTbThreads, 0, s>>>(dst, src, ab, a.coef, tb.z_chunk, d, g);
+                if constexpr (kFp32) k_jacobi_tb2<KIND><<<tb.grid, kT2Threads, 0, s>>>(dst, src, ab, a.coef, tb.z_chunk, d, g);
             } else if (vec) {
                 jacobi_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, ab, a.coef, vs.z_chunk, d, g);
             } else {
