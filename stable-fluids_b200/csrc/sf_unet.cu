@@ -125,8 +125,9 @@ int sm_count() {
 
 // 3x3x3 convolution on the tensor cores (tc::k_conv3d_tc): tensor maps for
 // the channels-last input (boxes of 8 channels x (TX + 2) x (TY + 2) x 1
-// voxels) and the [27][COUT][CIN] weights (boxes of 8 input channels x COUT
-// x 27 taps), then one persistent CTA per SM.
+// voxels) and the [dz][dy][dx][COUT][CIN] weights, viewed as (cin, cout, dx,
+// dy, dz) with boxes of 8 input channels x COUT x 1 x 1 x 3 (the dz taps of
+// one in-plane shift), then one persistent CTA per SM.
 template <int CIN, int COUT, int EPI>
 cudaError_t conv(const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, void* out, int out_ch, int out_off, Dims d, cudaStream_t s, unsigned* error) {
     using C = tc::Cfg<CIN, COUT>;
@@ -139,16 +140,18 @@ cudaError_t conv(const __nv_bfloat16* in, const __nv_bfloat16* w, const float* b
     const cuuint32_t es[4] = {1u, 1u, 1u, 1u};
     if (encode(&map_in, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(in), gd, gs, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue;
-    const cuuint64_t wd[3] = {static_cast<cuuint64_t>(CIN), static_cast<cuuint64_t>(COUT), 27u};
-    const cuuint64_t ws[2] = {static_cast<cuuint64_t>(CIN) * 2, static_cast<cuuint64_t>(COUT) * CIN * 2};
-    const cuuint32_t wbox[3] = {8u, static_cast<cuuint32_t>(COUT), 27u};
-    if (encode(&map_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(w), wd, ws, wbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    const cuuint64_t tap = static_cast<cuuint64_t>(COUT) * CIN * 2;  // bytes per tap
+    const cuuint64_t wd[5] = {static_cast<cuuint64_t>(CIN), static_cast<cuuint64_t>(COUT), 3u, 3u, 3u};
+    const cuuint64_t ws[4] = {static_cast<cuuint64_t>(CIN) * 2, tap, 3 * tap, 9 * tap};
+    const cuuint32_t wbox[5] = {8u, static_cast<cuuint32_t>(COUT), 1u, 1u, 3u};
+    const cuuint32_t wes[5] = {1u, 1u, 1u, 1u, 1u};
+    if (encode(&map_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(w), wd, ws, wbox, wes, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue;
     auto kern = tc::k_conv3d_tc<CIN, COUT, EPI>;
     const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
     if (attr != cudaSuccess) return attr;
-    tc::ConvArgs a{out, bias, out_ch, out_off, d, (d.nx + tc::TX - 1) / tc::TX, (d.ny + C::TY - 1) / C::TY, error};
-    const int tiles = a.tiles_x * a.tiles_y * d.nz;
+    tc::ConvArgs a{out, bias, out_ch, out_off, d, (d.nx + tc::TX - 1) / tc::TX, (d.ny + C::TY - 1) / C::TY, (d.nz + C::ZO - 1) / C::ZO, error};
+    const int tiles = a.tiles_x * a.tiles_y * a.tiles_z;
     const int grid = tiles < sm_count() ? tiles : sm_count();
     kern<<<grid, tc::kThreadsTC, C::BYTES, s>>>(map_in, map_w, a);
     return cudaGetLastError();

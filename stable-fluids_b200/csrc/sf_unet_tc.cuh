@@ -3,26 +3,39 @@
 // accumulators in tensor memory, operands brought into shared memory by TMA.
 //
 // Implicit GEMM. A CTA owns an output tile of TX = 32 columns x TY rows of
-// one z plane. The input halo of the tile (3 planes x (TY + 2) rows x
-// P = TX + 2 columns) is stored per 8-channel chunk as rows of 16 bytes,
-// row index r = hy * P + hx -- exactly the order in which a TMA box of
-// 8 channels x P x (TY + 2) voxels lands -- so that the halo row of output
-// voxel (y, x) shifted by tap (dy, dx) is r = m + dy * P + dx with
-// m = y * P + x: the A operand of one tap is a contiguous run of rows. GEMM
-// row m walks the tile with a pitch of P (the two extra columns per row are
-// computed and dropped), and M-blocks of 128 rows cover TY * P rows. In the
-// no-swizzle K-major canonical layout that is a descriptor with 16-byte rows,
-// 128-byte core-matrix groups (SBO) and the chunk stride as LBO, whose start
-// address moves by 16 bytes per row of shift. The weights of a tap are the B
-// operand ([cout][cin] rows, K-major, the same layout).
+// ZO consecutive z planes. The input halo of the tile (ZO + 2 planes x
+// (TY + 2) rows x P = TX + 2 columns) is stored per 8-channel chunk as rows
+// of 16 bytes, row index r = hy * P + hx -- exactly the order in which a TMA
+// box of 8 channels x P x (TY + 2) voxels lands -- so that the halo row of
+// output voxel (y, x) shifted by tap (dy, dx) is r = m + dy * P + dx with
+// m = y * P + x: the A operand of one in-plane shift is a contiguous run of
+// rows. GEMM row m walks the tile with a pitch of P (the two extra columns per
+// row are computed and dropped), and M-blocks of 128 rows cover TY * P rows.
+// In the no-swizzle K-major canonical layout that is a descriptor with 16-byte
+// rows, 128-byte core-matrix groups (SBO) and the chunk stride as LBO, whose
+// start address moves by 16 bytes per row of shift.
+//
+// Several output planes per MMA. Input plane ip (z = z0 - 1 + ip) meets
+// output plane o (z = z0 + o) through tap dz = ip - o, so one MMA per input
+// plane and in-plane shift (dy, dx) serves every output plane o with
+// 0 <= ip - o <= 2 at once: its B operand stacks the weights of those taps
+// (N = COUT per plane) and its D columns are those planes' accumulators. The
+// weights are kept as [dy][dx][dz][cout] rows per 8-channel chunk, so the
+// taps of one (dy, dx) are adjacent rows; output plane o's accumulator sits at
+// column (ZO - 1 - o) * COUT, so increasing dz meets increasing columns. Each
+// output still sums its taps in (dz, dy, dx) order, one K = 16 MMA step per
+// tap and channel group. An MMA costs about the same issue time for any
+// N <= 64 on B200, so layers with COUT = 16 use ZO = 4 (1.9x fewer MMAs per
+// voxel); wider layers use ZO = 1.
 //
 // Channels are processed in groups of 16 (one K = 16 MMA step); a pipeline
 // item is (tile, group). Warp-specialised, persistent CTA (one per SM):
 //   warp 0 (one thread) : TMA loads of items into S shared-memory stages
 //                         (and of the weights, once, when they fit);
-//   warp 1 (one thread) : 27 x M-blocks MMAs per item into one of two TMEM
-//                         accumulator buffers, tcgen05.commit to release the
-//                         stage and, after a tile's last group, its buffer;
+//   warp 1 (one thread) : (ZO + 2) x 9 x M-blocks MMAs per item into one of
+//                         two TMEM accumulator buffers, tcgen05.commit to
+//                         release the stage and, after a tile's last group,
+//                         its buffer;
 //   warps 2-5           : epilogue -- tcgen05.ld of the accumulators (warp w
 //                         reads TMEM lanes 32 (w % 4) .. +31), bias,
 //                         activation, channels-last BF16 (or FP32 channel 0)
@@ -87,9 +100,18 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
     asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
                  : "memory");
 }
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4, uint32_t bar) {
+    asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
                  : "memory");
+}
+
+// The weights of one 8-channel chunk c (input channels 8c .. 8c + 7) into
+// shared memory as rows [dy][dx][dz][cout]: one box of the 3 dz taps per
+// (dy, dx). The tensor map views the [dz][dy][dx][cout][cin] weights as
+// (cin, cout, dx, dy, dz).
+__device__ __forceinline__ void tma_load_weight_chunk(uint32_t dst, const CUtensorMap* map, int c, uint32_t box_bytes, uint32_t bar) {
+    for (int dy = 0; dy < 3; ++dy)
+        for (int dx = 0; dx < 3; ++dx) tma_load_5d(dst + static_cast<uint32_t>(dy * 3 + dx) * box_bytes, map, c * 8, 0, dx, dy, 0, bar);
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -101,10 +123,9 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 }
 
 // Instruction descriptor: kind::f16, A = B = BF16 (K-major), D = F32, M = 128.
-template <int N>
-__host__ __device__ constexpr uint32_t instr_desc() {
-    static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N for M = 128");
-    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+// N must be a multiple of 16 in [16, 256].
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
@@ -131,22 +152,25 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 enum Epilogue : int { RELU_BF16 = 0, LINEAR_BF16 = 1, LINEAR_F32_CH0 = 2 };
 
-// Shared-memory plan of one (CIN, COUT) convolution. The weights of all
-// taps and channels stay resident when they fit beside two input stages;
-// otherwise each stage carries the weights of its channel group. TY = 15
-// (4 M-blocks) when it fits, else 7 (2 M-blocks); three stages when they fit.
+// Shared-memory plan of one (CIN, COUT) convolution. ZO output planes per
+// tile (ZO + 2 input planes per stage). The weights of all taps and channels
+// stay resident when they fit beside two input stages; otherwise each stage
+// carries the weights of its channel group. TY = 15 (4 M-blocks) when it
+// fits, else 7 (2 M-blocks); three stages when they fit.
 template <int CIN, int COUT>
 struct Cfg {
+    static constexpr int ZO = COUT == 16 ? 4 : 1;
+    static constexpr int PLANES = ZO + 2;
     static constexpr int LIMIT = 232448 - 1024;
     static constexpr int W_ALL = 27 * CIN * COUT * 2;
-    static constexpr int IN15 = 6 * Geo<15>::R * 16, IN7 = 6 * Geo<7>::R * 16;
+    static constexpr int IN15 = 2 * PLANES * Geo<15>::R * 16, IN7 = 2 * PLANES * Geo<7>::R * 16;
     static constexpr bool RES = W_ALL + 2 * IN7 <= LIMIT;
     static constexpr int TY = (!RES || W_ALL + 2 * IN15 <= LIMIT) ? 15 : 7;
     static constexpr int MB = Geo<TY>::MB;
     static constexpr int R = Geo<TY>::R;
     static constexpr int PLANE_CHUNK = R * 16;               // one 8-channel chunk of one plane (a multiple of 128 bytes)
-    static constexpr int IN = 6 * PLANE_CHUNK;               // 3 planes x 2 chunks
-    static constexpr int WCHUNK = 27 * COUT * 16;            // one 8-channel chunk of all taps' weights
+    static constexpr int IN = 2 * PLANES * PLANE_CHUNK;      // PLANES planes x 2 chunks
+    static constexpr int WCHUNK = 27 * COUT * 16;            // one 8-channel chunk of all taps' weights, rows [dy][dx][dz][cout]
     static constexpr int STAGE = IN + (RES ? 0 : 2 * WCHUNK);
     static constexpr int S = (RES && W_ALL + 3 * IN <= LIMIT) ? 3 : 2;
     static constexpr int STAGE_OFF = RES ? W_ALL : 0;
@@ -154,11 +178,15 @@ struct Cfg {
     static constexpr int BIAS_OFF = BAR_OFF + 128;
     static constexpr int BYTES = BIAS_OFF + COUT * 4;
     static constexpr int BOX_BYTES = 8 * 2 * P * (TY + 2);   // one input TMA box
-    static constexpr int ITEM_TX = 6 * BOX_BYTES + (RES ? 0 : 2 * WCHUNK);
-    static constexpr int COLS = 2 * MB * COUT;               // two accumulator buffers
+    static constexpr int WBOX_BYTES = 8 * 2 * 3 * COUT;      // one weight TMA box: the 3 dz taps of one (dy, dx)
+    static constexpr int ITEM_TX = 2 * PLANES * BOX_BYTES + (RES ? 0 : 2 * WCHUNK);
+    static constexpr int TILE_COLS = ZO * COUT;              // accumulator columns of one M-block
+    static constexpr int COLS = 2 * MB * TILE_COLS;          // two accumulator buffers
     static constexpr int ALLOC = COLS <= 32 ? 32 : COLS <= 64 ? 64 : COLS <= 128 ? 128 : COLS <= 256 ? 256 : 512;
     static_assert(BYTES <= 232448, "shared memory");
     static_assert(COLS <= 512, "tensor memory");
+    static_assert(COUT % 16 == 0 && (ZO == 1 ? COUT : 3 * COUT) <= 256, "MMA N");
+    static_assert(9 * WBOX_BYTES == WCHUNK && WBOX_BYTES % 128 == 0, "weight boxes fill a chunk, 128-byte aligned");
     static_assert(BOX_BYTES <= PLANE_CHUNK && PLANE_CHUNK % 128 == 0 && WCHUNK % 128 == 0 && W_ALL % 128 == 0 && STAGE % 128 == 0, "layout");
 };
 
@@ -167,7 +195,7 @@ struct ConvArgs {
     const float* bias;         // COUT (may be null)
     int out_ch, out_off;
     Dims d;
-    int tiles_x, tiles_y;      // tiles per plane
+    int tiles_x, tiles_y, tiles_z;  // tiles per axis (tiles_z = ceil(nz / ZO))
     unsigned* error;
 };
 
@@ -182,8 +210,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
     static_assert(CIN % 16 == 0, "channel groups of 16");
     using C = Cfg<CIN, COUT>;
     constexpr int GROUPS = CIN / 16;
-    constexpr int S = C::S, MB = C::MB, TY = C::TY;
-    constexpr uint32_t IDESC = instr_desc<COUT>();
+    constexpr int S = C::S, MB = C::MB, TY = C::TY, ZO = C::ZO;
     extern __shared__ __align__(1024) unsigned char smem[];
     const int warp = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
     const uint32_t sbase = smem_u32(smem);
@@ -199,7 +226,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
 
     // rows past the halo are read by the shifted A operands: zero them once
     for (int s = 0; s < S; ++s)
-        for (int i = static_cast<int>(threadIdx.x); i < 6 * (C::PLANE_CHUNK - C::BOX_BYTES) / 16; i += kThreadsTC) {
+        for (int i = static_cast<int>(threadIdx.x); i < 2 * C::PLANES * (C::PLANE_CHUNK - C::BOX_BYTES) / 16; i += kThreadsTC) {
             const int chunk = i / ((C::PLANE_CHUNK - C::BOX_BYTES) / 16), r = i % ((C::PLANE_CHUNK - C::BOX_BYTES) / 16);
             *reinterpret_cast<uint4*>(smem + C::STAGE_OFF + s * C::STAGE + chunk * C::PLANE_CHUNK + C::BOX_BYTES + r * 16) = make_uint4(0, 0, 0, 0);
         }
@@ -227,7 +254,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    const int tiles = a.tiles_x * a.tiles_y * a.d.nz;
+    const int tiles = a.tiles_x * a.tiles_y * a.tiles_z;
     const int my_tiles = tiles > static_cast<int>(blockIdx.x) ? (tiles - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1 : 0;
     const int items = my_tiles * GROUPS;
     const auto tile_of = [&](int k) { return static_cast<int>(blockIdx.x) + k * static_cast<int>(gridDim.x); };
@@ -236,20 +263,21 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
         // ---- producer
         if constexpr (C::RES) {
             mbar_expect_tx(wbar, static_cast<uint32_t>(C::W_ALL));
-            for (int c = 0; c < CIN / 8; ++c) tma_load_3d(sbase + static_cast<uint32_t>(c * C::WCHUNK), &map_w, c * 8, 0, 0, wbar);
+            for (int c = 0; c < CIN / 8; ++c) tma_load_weight_chunk(sbase + static_cast<uint32_t>(c * C::WCHUNK), &map_w, c, C::WBOX_BYTES, wbar);
         }
         for (int i = 0; i < items; ++i) {
             const int s = i % S, u = i / S;
             if (u >= 1 && !mbar_wait(empty(s), static_cast<uint32_t>((u - 1) & 1), abort, a.error)) break;
             const int tile = tile_of(i / GROUPS), g = i % GROUPS;
             const int tx = tile % a.tiles_x, rest = tile / a.tiles_x;
-            const int ty = rest % a.tiles_y, z = rest / a.tiles_y;
+            const int ty = rest % a.tiles_y, z0 = (rest / a.tiles_y) * ZO;
             const uint32_t st = sbase + static_cast<uint32_t>(C::STAGE_OFF + s * C::STAGE);
             mbar_expect_tx(full(s), static_cast<uint32_t>(C::ITEM_TX));
-            for (int plane = 0; plane < 3; ++plane)
-                for (int ch = 0; ch < 2; ++ch) tma_load_4d(st + static_cast<uint32_t>((plane * 2 + ch) * C::PLANE_CHUNK), &map_in, g * 16 + ch * 8, tx * TX - 1, ty * TY - 1, z - 1 + plane, full(s));
+            // input planes z0 - 1 .. z0 + ZO (out-of-range planes read as zeros)
+            for (int plane = 0; plane < C::PLANES; ++plane)
+                for (int ch = 0; ch < 2; ++ch) tma_load_4d(st + static_cast<uint32_t>((plane * 2 + ch) * C::PLANE_CHUNK), &map_in, g * 16 + ch * 8, tx * TX - 1, ty * TY - 1, z0 - 1 + plane, full(s));
             if constexpr (!C::RES)
-                for (int ch = 0; ch < 2; ++ch) tma_load_3d(st + static_cast<uint32_t>(C::IN + ch * C::WCHUNK), &map_w, g * 16 + ch * 8, 0, 0, full(s));
+                for (int ch = 0; ch < 2; ++ch) tma_load_weight_chunk(st + static_cast<uint32_t>(C::IN + ch * C::WCHUNK), &map_w, 2 * g + ch, C::WBOX_BYTES, full(s));
         }
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer
@@ -265,16 +293,33 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
             const uint32_t wb = C::RES ? sbase + static_cast<uint32_t>(2 * g * C::WCHUNK) : st + static_cast<uint32_t>(C::IN);
             const uint64_t da0 = smem_desc(st, C::PLANE_CHUNK, 128);
             const uint64_t db0 = smem_desc(wb, C::WCHUNK, 128);
-            const uint32_t d0 = tmem + static_cast<uint32_t>(ab * MB * COUT);
+            const uint32_t d0 = tmem + static_cast<uint32_t>(ab * MB * C::TILE_COLS);
 #pragma unroll 1
-            for (int tap = 0; tap < 27; ++tap) {
-                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                const uint64_t db = db0 + static_cast<uint64_t>(tap * COUT);  // + tap * COUT * 16 bytes, in 16-byte units
-                const uint32_t acc = (g > 0 || tap > 0) ? 1u : 0u;
+            for (int ip = 0; ip < C::PLANES; ++ip) {
+                // output planes o_lo .. o_hi meet input plane ip, through taps dz = ip - o
+                const int o_hi = ip < ZO - 1 ? ip : ZO - 1, o_lo = ip > 2 ? ip - 2 : 0;
+                const int nblk = o_hi - o_lo + 1, dz_lo = ip - o_hi;
+                // plane o_hi = ip is touched for the first time here (g == 0, shift (0, 0)):
+                // its block gets its own overwriting MMA
+                const bool fresh = g == 0 && o_hi == ip;
+                const uint32_t col = static_cast<uint32_t>((ZO - 1 - o_hi) * COUT);
+                const uint64_t a_plane = da0 + static_cast<uint64_t>(ip * 2 * (C::PLANE_CHUNK / 16));
+#pragma unroll 1
+                for (int sh = 0; sh < 9; ++sh) {
+                    const int dy = sh / 3, dx = sh % 3;
+                    const uint64_t db = db0 + static_cast<uint64_t>((sh * 3 + dz_lo) * COUT);  // rows of 16 bytes
+                    const bool split = fresh && sh == 0;
 #pragma unroll
-                for (int mb = 0; mb < MB; ++mb) {
-                    const uint64_t da = da0 + static_cast<uint64_t>(dz * 2 * (C::PLANE_CHUNK / 16) + mb * 128 + dy * P + dx);
-                    mma_bf16(d0 + static_cast<uint32_t>(mb * COUT), da, db, IDESC, acc);
+                    for (int mb = 0; mb < MB; ++mb) {
+                        const uint64_t da = a_plane + static_cast<uint64_t>(mb * 128 + dy * P + dx);
+                        const uint32_t dm = d0 + static_cast<uint32_t>(mb * C::TILE_COLS) + col;
+                        if (split) {
+                            mma_bf16(dm, da, db, instr_desc(COUT), 0u);
+                            if (nblk > 1) mma_bf16(dm + COUT, da, db + COUT, instr_desc(static_cast<uint32_t>((nblk - 1) * COUT)), 1u);
+                        } else {
+                            mma_bf16(dm, da, db, instr_desc(static_cast<uint32_t>(nblk * COUT)), 1u);
+                        }
+                    }
                 }
             }
             mma_commit(empty(s));
@@ -289,18 +334,20 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
             tc_fence_after();
             const int tile = tile_of(k);
             const int tx = tile % a.tiles_x, rest = tile / a.tiles_x;
-            const int ty = rest % a.tiles_y, z = rest / a.tiles_y;
+            const int ty = rest % a.tiles_y, z0 = (rest / a.tiles_y) * ZO;
 #pragma unroll 1
-            for (int mb = 0; mb < MB; ++mb) {
+            for (int mo = 0; mo < MB * ZO; ++mo) {
+                const int mb = mo / ZO, o = mo % ZO, z = z0 + o;
                 const int m = mb * 128 + q * 32 + lane;
                 const int y = m / P, x = m % P;
                 const int gx = tx * TX + x, gy = ty * TY + y;
-                const bool live = x < TX && y < TY && gx < a.d.nx && gy < a.d.ny;
+                const bool live = x < TX && y < TY && gx < a.d.nx && gy < a.d.ny && z < a.d.nz;
                 const size_t v = live ? static_cast<size_t>(gx) + static_cast<size_t>(a.d.nx) * (gy + static_cast<size_t>(a.d.ny) * z) : 0;
+                const uint32_t col = static_cast<uint32_t>(ab * MB * C::TILE_COLS + mb * C::TILE_COLS + (ZO - 1 - o) * COUT);
 #pragma unroll
                 for (int c0 = 0; c0 < COUT; c0 += 16) {
                     float acc[16];
-                    tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(ab * MB * COUT + mb * COUT + c0), acc);
+                    tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + col + static_cast<uint32_t>(c0), acc);
                     tmem_wait_ld();
                     if (!live) continue;
                     if constexpr (EPI == LINEAR_F32_CH0) {
