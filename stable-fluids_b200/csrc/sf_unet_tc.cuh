@@ -32,10 +32,12 @@
 // item is (tile, group). Warp-specialised, persistent CTA (one per SM):
 //   warp 0 (one thread) : TMA loads of items into S shared-memory stages
 //                         (and of the weights, once, when they fit);
-//   warp 1 (one thread) : (ZO + 2) x 9 x M-blocks MMAs per item into one of
-//                         two TMEM accumulator buffers, tcgen05.commit to
-//                         release the stage and, after a tile's last group,
-//                         its buffer;
+//   warp 1              : walks the items as a converged warp; one elected
+//                         lane issues (ZO + 2) x 9 x M-blocks MMAs per item
+//                         (fully unrolled, compile-time operand offsets) into
+//                         one of two TMEM accumulator buffers, and
+//                         tcgen05.commit to release the stage and, after a
+//                         tile's last group, its buffer;
 //   warps 2-5           : epilogue -- tcgen05.ld of the accumulators (warp w
 //                         reads TMEM lanes 32 (w % 4) .. +31), bias,
 //                         activation, channels-last BF16 (or FP32 channel 0)
@@ -150,6 +152,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// One lane of a converged warp (elect.sync over the full mask).
+__device__ __forceinline__ bool elect_one() {
+    uint32_t pred;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "elect.sync _|p, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(pred));
+    return pred != 0;
+}
+
 enum Epilogue : int { RELU_BF16 = 0, LINEAR_BF16 = 1, LINEAR_F32_CH0 = 2 };
 
 // Shared-memory plan of one (CIN, COUT) convolution. ZO output planes per
@@ -198,6 +211,40 @@ struct ConvArgs {
     int tiles_x, tiles_y, tiles_z;  // tiles per axis (tiles_z = ceil(nz / ZO))
     unsigned* error;
 };
+
+// The MMAs of one pipeline item (one tile, one 16-channel group), fully
+// unrolled so that every operand is a compile-time offset from the stage,
+// weight and accumulator bases. Input plane ip meets output planes
+// o_lo .. o_hi through taps dz = ip - o; the block of plane o_hi = ip is
+// written for the first time at shift (0, 0) of group 0 (`first`), so it
+// gets its own MMA that overwrites instead of accumulating.
+template <typename C, int COUT>
+__device__ __forceinline__ void issue_item(uint64_t da0, uint64_t db0, uint32_t d0, bool first) {
+    constexpr int ZO = C::ZO;
+    const uint32_t acc0 = first ? 0u : 1u;
+#pragma unroll
+    for (int ip = 0; ip < C::PLANES; ++ip) {
+        const int o_hi = ip < ZO - 1 ? ip : ZO - 1, o_lo = ip > 2 ? ip - 2 : 0;
+        const int nblk = o_hi - o_lo + 1, dz_lo = ip - o_hi;
+        const uint32_t col = static_cast<uint32_t>((ZO - 1 - o_hi) * COUT);
+#pragma unroll
+        for (int sh = 0; sh < 9; ++sh) {
+            const int dy = sh / 3, dx = sh % 3;
+            const uint64_t db = db0 + static_cast<uint64_t>((sh * 3 + dz_lo) * COUT);  // rows of 16 bytes
+#pragma unroll
+            for (int mb = 0; mb < C::MB; ++mb) {
+                const uint64_t da = da0 + static_cast<uint64_t>(ip * 2 * (C::PLANE_CHUNK / 16) + mb * 128 + dy * P + dx);
+                const uint32_t dm = d0 + static_cast<uint32_t>(mb * C::TILE_COLS) + col;
+                if (o_hi == ip && sh == 0) {
+                    mma_bf16(dm, da, db, instr_desc(COUT), acc0);
+                    if (nblk > 1) mma_bf16(dm + COUT, da, db + COUT, instr_desc(static_cast<uint32_t>((nblk - 1) * COUT)), 1u);
+                } else {
+                    mma_bf16(dm, da, db, instr_desc(static_cast<uint32_t>(nblk * COUT)), 1u);
+                }
+            }
+        }
+    }
+}
 
 // Roles: warp 0 loads (one thread issues the TMA boxes), warp 1 issues the
 // MMAs (one thread), warps 2..5 run the epilogue (warp w reads TMEM lanes
@@ -279,51 +326,29 @@ __global__ void __launch_bounds__(kThreadsTC, 1) k_conv3d_tc(const __grid_consta
             if constexpr (!C::RES)
                 for (int ch = 0; ch < 2; ++ch) tma_load_weight_chunk(st + static_cast<uint32_t>(C::IN + ch * C::WCHUNK), &map_w, 2 * g + ch, C::WBOX_BYTES, full(s));
         }
-    } else if (warp == 1 && lane == 0) {
-        // ---- MMA issuer
+    } else if (warp == 1) {
+        // ---- MMA issuer: the whole warp walks the items (its values stay
+        // warp-uniform); one elected lane issues the MMAs and the commits
+        const auto wait_all = [&](uint32_t bar, uint32_t parity) { return __all_sync(0xffffffffu, mbar_wait(bar, parity, abort, a.error)); };
         bool ok = true;
-        if constexpr (C::RES) ok = mbar_wait(wbar, 0, abort, a.error);
+        if constexpr (C::RES) ok = wait_all(wbar, 0);
         for (int i = 0; i < items && ok; ++i) {
             const int s = i % S, u = i / S;
             const int k = i / GROUPS, g = i % GROUPS, ab = k & 1;
-            if (g == 0 && k >= 2 && !mbar_wait(acc_empty(ab), static_cast<uint32_t>(((k >> 1) - 1) & 1), abort, a.error)) break;
-            if (!mbar_wait(full(s), static_cast<uint32_t>(u & 1), abort, a.error)) break;
+            if (g == 0 && k >= 2 && !wait_all(acc_empty(ab), static_cast<uint32_t>(((k >> 1) - 1) & 1))) break;
+            if (!wait_all(full(s), static_cast<uint32_t>(u & 1))) break;
             tc_fence_after();
             const uint32_t st = sbase + static_cast<uint32_t>(C::STAGE_OFF + s * C::STAGE);
             const uint32_t wb = C::RES ? sbase + static_cast<uint32_t>(2 * g * C::WCHUNK) : st + static_cast<uint32_t>(C::IN);
             const uint64_t da0 = smem_desc(st, C::PLANE_CHUNK, 128);
             const uint64_t db0 = smem_desc(wb, C::WCHUNK, 128);
             const uint32_t d0 = tmem + static_cast<uint32_t>(ab * MB * C::TILE_COLS);
-#pragma unroll 1
-            for (int ip = 0; ip < C::PLANES; ++ip) {
-                // output planes o_lo .. o_hi meet input plane ip, through taps dz = ip - o
-                const int o_hi = ip < ZO - 1 ? ip : ZO - 1, o_lo = ip > 2 ? ip - 2 : 0;
-                const int nblk = o_hi - o_lo + 1, dz_lo = ip - o_hi;
-                // plane o_hi = ip is touched for the first time here (g == 0, shift (0, 0)):
-                // its block gets its own overwriting MMA
-                const bool fresh = g == 0 && o_hi == ip;
-                const uint32_t col = static_cast<uint32_t>((ZO - 1 - o_hi) * COUT);
-                const uint64_t a_plane = da0 + static_cast<uint64_t>(ip * 2 * (C::PLANE_CHUNK / 16));
-#pragma unroll 1
-                for (int sh = 0; sh < 9; ++sh) {
-                    const int dy = sh / 3, dx = sh % 3;
-                    const uint64_t db = db0 + static_cast<uint64_t>((sh * 3 + dz_lo) * COUT);  // rows of 16 bytes
-                    const bool split = fresh && sh == 0;
-#pragma unroll
-                    for (int mb = 0; mb < MB; ++mb) {
-                        const uint64_t da = a_plane + static_cast<uint64_t>(mb * 128 + dy * P + dx);
-                        const uint32_t dm = d0 + static_cast<uint32_t>(mb * C::TILE_COLS) + col;
-                        if (split) {
-                            mma_bf16(dm, da, db, instr_desc(COUT), 0u);
-                            if (nblk > 1) mma_bf16(dm + COUT, da, db + COUT, instr_desc(static_cast<uint32_t>((nblk - 1) * COUT)), 1u);
-                        } else {
-                            mma_bf16(dm, da, db, instr_desc(static_cast<uint32_t>(nblk * COUT)), 1u);
-                        }
-                    }
-                }
+            if (elect_one()) {
+                issue_item<C, COUT>(da0, db0, d0, g == 0);
+                mma_commit(empty(s));
+                if (g == GROUPS - 1) mma_commit(acc_full(ab));
             }
-            mma_commit(empty(s));
-            if (g == GROUPS - 1) mma_commit(acc_full(ab));
+            __syncwarp();
         }
     } else if (warp >= 2) {
         // ---- epilogue
