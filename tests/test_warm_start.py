@@ -72,7 +72,13 @@ def test_predict_matches_oracle(net, shape):
     assert rel(got0, ref0) <= PRED_TOL
 
 
-@pytest.mark.parametrize("shape", [(8, 12, 20), (16, 16, 16)])
+# (12, 16, 32): the half-resolution level has 6 planes, so the data-gradient
+# convolution of the 16 -> 32 layer (4 output planes per tile) ends on a
+# partial tile; a wrong partial tile would put a third of that layer's output
+# off and the enc0 gradients far outside the tolerance. (Smaller grids of
+# this kind sit too close to the BF16 rounding noise: 2-5 % on some layers
+# for some seeds, with or without partial tiles.)
+@pytest.mark.parametrize("shape", [(8, 12, 20), (16, 16, 16), (12, 16, 32)])
 def test_gradients_match_oracle(net, shape):
     params = random_parameters(3)
     net.set_parameters(params)
