@@ -24,9 +24,10 @@
 // taps of one (dy, dx) are adjacent rows; output plane o's accumulator sits at
 // column (ZO - 1 - o) * COUT, so increasing dz meets increasing columns. Each
 // output still sums its taps in (dz, dy, dx) order, one K = 16 MMA step per
-// tap and channel group. An MMA costs about the same issue time for any
-// N <= 64 on B200, so layers with COUT = 16 use ZO = 4 (1.9x fewer MMAs per
-// voxel); wider layers use ZO = 1.
+// tap and channel group. Every MMA reads its 4 KB A tile from shared memory
+// whatever its N, so wider MMAs amortise it: layers with COUT = 16 use ZO = 4
+// (tiles of 32 x 7 x 4 voxels, 1.8x fewer MMAs per voxel than one plane of
+// 32 x 15); wider layers use ZO = 1.
 //
 // Channels are processed in groups of 16 (one K = 16 MMA step); a pipeline
 // item is (tile, group). Warp-specialised, persistent CTA (one per SM):
