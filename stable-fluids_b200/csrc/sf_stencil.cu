@@ -546,6 +546,9 @@ __device__ __forceinline__ void residual_vec_block(uint3 blk, const float* __res
         int i = x0 + d.nx * (y + d.ny * zb);
         float4 cur = ld4(p + i);
         float4 below = vec_below4(p, i, zb, d, g, cur);
+        // two planes per iteration, so the next plane's loads overlap this
+        // plane's FP64 arithmetic (the sums keep their order)
+#pragma unroll 2
         for (int z = zb; z < ze; ++z, i += sz) {
             const float4 above = vec_above4(p, i, z, d, g, cur);
             float a = p[i + v.ox_lo], b = p[i + v.ox_hi];
