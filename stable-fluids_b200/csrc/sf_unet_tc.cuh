@@ -248,9 +248,10 @@ __device__ __forceinline__ void issue_item(uint64_t da0, uint64_t db0, uint32_t 
 }
 
 // Roles: warp 0 loads (one thread issues the TMA boxes), warp 1 issues the
-// MMAs (the converged warp, one elected lane), warps 2..5 run the epilogue (warp w reads TMEM lanes
-// 32 (w % 4) .. +31). Pipeline items are (tile, 16-channel group) in order;
-// stage i % S holds item i; accumulator buffer k % 2 holds tile k.
+// MMAs (the converged warp, one elected lane), warps 2..5 run the epilogue
+// (warp w reads TMEM lanes 32 (w % 4) .. +31). Pipeline items are (tile,
+// 16-channel group) in order; stage i % S holds item i; accumulator buffer
+// k % 2 holds tile k.
 constexpr int kThreadsTC = 192;
 
 template <int CIN, int COUT, int EPI>
