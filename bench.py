@@ -22,10 +22,13 @@ Solver variants, all timed the same way (W untimed steps, then K steps):
 
   value : whole-job steps/s of the learned variant, inputs resident on the
           device, CUDA events on the simulation stream, max over ranks.
-  e2e   : the learned variant through the public C ABI with host buffers:
-          every step uploads the force field from pinned host memory
-          (stable_fluids_update_vector_field_cuda with host pointers) and
-          reads the density back to pinned host memory.
+  e2e   : the learned variant through the public C ABI with host buffers,
+          on a fresh context that replays the device-timed steps (same W
+          untimed steps, same K timed steps, so the same solves): every step
+          uploads the force field from pinned host memory
+          (stable_fluids_update_vector_field_cuda with host pointers), reads
+          the step's statistics and reads the density back to pinned host
+          memory; one pair of CUDA events around the K steps.
   roofline : the dominant kernel, the Jacobi pressure sweep (12 B/cell),
           timed with CUDA events on the context stream; the network's
           convolutions are reported beside it against the bf16 peak.
@@ -90,7 +93,7 @@ def parse():
     p.add_argument("--train-epochs", type=int, default=12)
     p.add_argument("--train-seconds", type=float, default=90.0)
     p.add_argument("--learning-rate", type=float, default=3e-4)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=None, help="end-to-end timing through the C ABI: the first N of the device-timed steps (default: all K; 0: skip)")
     p.add_argument("--fixed-steps", type=int, default=20)
     p.add_argument("--batch-steps", type=int, default=20, help="steps of the batched 64-simulation workload (0: skip)")
     p.add_argument("--bf16-size", type=int, default=384)
@@ -331,32 +334,45 @@ def network_flops(n):
     return 2.0 * macs
 
 
-def e2e_run(sf, sim, scene, steps):
-    """Steps through the public ABI with host buffers: per step the force
-    field goes up from pinned host memory and the density comes back."""
+def e2e_run(sf, scene, args, steps, device, net):
+    """The learned variant through the public ABI with host buffers, on a
+    fresh context replaying the device-timed run's steps: the same W untimed
+    steps, then the first `steps` of its K timed steps (the same solves), each
+    of which uploads the force field
+    from pinned host memory, step, read the step's statistics and read the
+    density back to pinned host memory."""
     import numpy as np
     import torch
 
-    n = sim.cells
-    host_force = [torch.from_numpy(np.ascontiguousarray(f, dtype=np.float32)).pin_memory() for f in scene.force]
-    host_rho = torch.empty(n, dtype=torch.float32).pin_memory()
-    h = sim.scalar_handles[0]
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    start.record(sim.stream)
-    for _ in range(steps):
-        rc = sim.lib.stable_fluids_update_vector_field_cuda(sim.ctx, 1, host_force[0].data_ptr(), host_force[1].data_ptr(), host_force[2].data_ptr())
-        if rc != 0:
-            raise RuntimeError(f"update_vector_field with host pointers failed ({rc})")
-        sim.step(1)
-        rho = sim.view(sf.VIEW_SCALAR_FIELD_DATA, h)
-        with torch.cuda.stream(sim.stream):
-            host_rho.copy_(rho.reshape(-1), non_blocking=True)
-    end.record(sim.stream)
-    torch.cuda.synchronize()
-    t = start.elapsed_time(end) / 1000.0
-    return t, 3 * n * 4, n * 4
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=solver_options(sf, "learned", args.tolerance, args.cap, args.trial), device=device)
+    try:
+        net.attach(sim)
+        sf.scenes.apply_inputs(sim, scene, 0)
+        sim.step(args.warmup)
+        n = sim.cells
+        host_force = [torch.from_numpy(np.ascontiguousarray(f, dtype=np.float32)).pin_memory() for f in scene.force]
+        host_rho = torch.empty(n, dtype=torch.float32).pin_memory()
+        h = sim.scalar_handles[0]
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        its = []
+        torch.cuda.synchronize()
+        start.record(sim.stream)
+        for _ in range(steps):
+            rc = sim.lib.stable_fluids_update_vector_field_cuda(sim.ctx, 1, host_force[0].data_ptr(), host_force[1].data_ptr(), host_force[2].data_ptr())
+            if rc != 0:
+                raise RuntimeError(f"update_vector_field with host pointers failed ({rc})")
+            sim.step(1)
+            its.append(sim.stats().pressure_iterations)
+            rho = sim.view(sf.VIEW_SCALAR_FIELD_DATA, h)
+            with torch.cuda.stream(sim.stream):
+                host_rho.copy_(rho.reshape(-1), non_blocking=True)
+        end.record(sim.stream)
+        torch.cuda.synchronize()
+        t = start.elapsed_time(end) / 1000.0
+    finally:
+        sim.close()
+    return t, 3 * n * 4, n * 4, its
 
 
 def fixed_iterations(sf, lib, scene, steps, warmup, device, world):
@@ -647,15 +663,12 @@ def main():
     headline = "learned" if "learned" in variants else variants[0]  # profiling runs may leave the network out
     net, train_info = train_network(sf, args, local) if any(v.startswith("learned") for v in variants) else (None, None)
 
-    results, sims = {}, {}
+    results = {}
     with Clocks(local, not args.no_clocks and rank == 0) as clk:
         for v in variants:
             sim, out = run_variant(sf, scene, v, args, world, local, net if v.startswith("learned") else None)
             results[v] = out
-            if v == "learned":
-                sims[v] = sim
-            else:
-                sim.close()
+            sim.close()
     learned = results[headline]
     value = learned["steps_per_s"]
 
@@ -682,12 +695,11 @@ def main():
                             "frac": flops / net_s / 1e12 / tc_peak, "flop_per_launch": flops, "launch_ms": net_s * 1e3, "unit_of_work": f"one prediction at {n}^3, real channels only"}
 
     e2e = None
-    if args.e2e_steps > 0 and "learned" in sims:
-        te, h2d, d2h = e2e_run(sf, sims["learned"], scene, args.e2e_steps)
+    e2e_steps = args.steps if args.e2e_steps is None else min(args.e2e_steps, args.steps)
+    if e2e_steps > 0 and "learned" in results and not args.fixed_pressure_iterations:
+        te, h2d, d2h, e2e_its = e2e_run(sf, scene, args, e2e_steps, local, net)
         te = max_over_ranks(te, world)
-        e2e = {"value": world * args.e2e_steps / te, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps}
-    for sim in sims.values():
-        sim.close()
+        e2e = {"value": world * e2e_steps / te, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps, "pressure_iterations": e2e_its}
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
     batch = None
     if args.batch_steps > 0:
