@@ -46,10 +46,15 @@ Solver variants, all timed the same way (W untimed steps, then K steps):
 --impl reference runs the reference's own implementation of the path -- its
 CUDA backend compiled unmodified from backend-cuda.cu (oracle/_ref; the
 reference has no CPU implementation) -- on the same scene through the same
-C ABI. The reference cannot iterate to a residual, so it runs with the fixed
-pressure-iteration count that the reference arithmetic (red-black from zero,
-bit-identical in this library) needs to reach 1e-3 in every timed step,
-found by a calibration run before timing.
+C ABI. That process loads the reference library only. The reference cannot
+iterate to a residual, so it runs with a fixed pressure-iteration count per
+step: the counts the reference arithmetic (red-black Gauss-Seidel from zero,
+bit-identical in this library) needs to reach the tolerance in each step are
+read from bench_calibration.json, which `python bench.py --calibrate` writes
+with this library's red-black variant. The line's value is the reference at
+the mean of the timed steps' needs (the same total iterations as running
+each step at its own need); the reference at the largest need (the fixed
+count that reaches the tolerance in every timed step) is reported beside it.
 
 Multi-GPU (torchrun, N>1): the step does not shard; each rank runs its own
 replica of the workload ("scaling": "weak").
@@ -73,6 +78,10 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "steps/s at 256³: learned-warm-start vs plain Jacobi at equal ‖∇·u‖ residual"
 CHECK_INTERVAL = 16
+CALIBRATION = ROOT / "bench_calibration.json"
+# DRAM bytes (read + write) of one Jacobi pressure pass from an ncu capture,
+# by grid size; filled from profiles/ once captured.
+PASS_TRAFFIC: dict[int, tuple[float, str]] = {}
 
 
 def parse():
@@ -104,6 +113,8 @@ def parse():
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--fixed-pressure-iterations", type=int, default=0,
                    help="profiling: run the variants with this fixed sweep count instead of the residual-driven solve (ncu cannot see kernels inside conditional graph nodes)")
+    p.add_argument("--calibrate", action="store_true", help="write bench_calibration.json: the red-black iterations each step of the scene needs (this library's rbgs variant), for --impl reference")
+    p.add_argument("--calibrate-steps", type=int, default=40)
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -208,13 +219,13 @@ def solver_options(sf, variant, tol, cap, trial):
     return o
 
 
-def launches_per_step(info_kernels, iterations, trial_done, scheme_rbgs):
+def launches_per_step(info, iterations, trial_done):
     """Kernels one residual-driven step launches: the captured step counts
-    the loop body once; each further pass of the body launches the interval's
-    sweeps (2 per red-black iteration) + the residual sum + the check."""
-    body = CHECK_INTERVAL * (2 if scheme_rbgs else 1) + 2
+    the loop body once; each further pass of the body launches the
+    interval's stencil passes + the residual sums + the check
+    (info.kernels_per_check)."""
     passes = max((iterations - trial_done) // CHECK_INTERVAL, 1)
-    return info_kernels + (passes - 1) * body
+    return info.kernels_per_step + (passes - 1) * info.kernels_per_check
 
 
 def run_variant(sf, scene, variant, args, world, device, net=None):
@@ -254,7 +265,7 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
     if args.fixed_pressure_iterations:
         launches = info.kernels_per_step * args.steps
     else:
-        launches = sum(launches_per_step(info.kernels_per_step, i, trial_done, variant == "rbgs") for i in its)
+        launches = sum(launches_per_step(info, i, trial_done) for i in its)
     out = {"steps_per_s": world * args.steps / t, "ms_per_step": 1000.0 * t / args.steps, "ms_per_step_median": statistics.median(per_step), "pressure_iterations": its, "rel_residual": res, "hit_cap": any(r > args.tolerance for r in res), "gpu_launches": launches}
     if variant.startswith("learned"):
         out["used_fallback"] = fallback
@@ -281,16 +292,19 @@ def train_network(sf, args, device):
     return net, info
 
 
-def time_pressure_sweep(sf, scene, device):
-    """Average duration of one Jacobi pressure sweep (k_jacobi_vec4), CUDA
-    events on the context stream: the fixed-count pressure stage of a Jacobi
-    context enqueued directly (80 sweeps per stage)."""
+def time_pressure_sweep(sf, scene, device, sweeps=96):
+    """The Jacobi pressure solve's kernel, timed with CUDA events on the
+    context stream: the fixed-count pressure stage of a Jacobi context
+    (`sweeps` sweeps, a multiple of every pass size) enqueued directly,
+    three times. Returns (seconds per launch, sweeps per launch)."""
     import torch
 
     o = sf.default_options()
     o.scheme = sf.SCHEME_JACOBI
     o.warm_start = sf.WARM_START_PREVIOUS
-    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=o, device=device)
+    cfg = type(scene.config).from_buffer_copy(scene.config)
+    cfg.pressure_iterations = sweeps
+    sim = sf.Simulation(cfg, scene.scalars, scene.vectors, options=o, device=device)
     sf.scenes.apply_inputs(sim, scene, 0)
     sim.step(1)
     sim.enqueue_stage(sf.STAGE_PRESSURE)
@@ -303,7 +317,8 @@ def time_pressure_sweep(sf, scene, device):
     end.record(sim.stream)
     torch.cuda.synchronize()
     sim.close()
-    return start.elapsed_time(end) / 1000.0 / max(launches, 1)
+    launches = max(launches, 1)
+    return start.elapsed_time(end) / 1000.0 / launches, 3 * sweeps / launches
 
 
 def time_network(net, n, device, repeats=3):
@@ -585,52 +600,89 @@ def cpu_baseline(sf, scene, plain_iterations):
             "sample": f"1 step of the {n}^3 plume without pressure sweeps ({times[0]:.2f} s) and 1 with 48 Jacobi sweeps ({times[48]:.2f} s) on {threads} threads; steps/s = 1 / (t_step + N x t_sweep) with N = {plain_iterations:.0f}, the mean sweep count of the plain variant (same arithmetic)"}
 
 
-def reference_arm(sf, args, scene, world, rank, local):
-    """The reference backend (oracle/_ref) at equal residual: calibrate the
-    iteration count with this library's red-black solve from zero (the
-    reference's arithmetic, bit-identical), then time the reference with that
-    fixed count."""
+def calibration_key(args):
+    return {"grid": [args.size] * 3, "tolerance": args.tolerance, "check_interval": CHECK_INTERVAL, "cap": args.cap, "scene": "config1 plume, seed 1"}
+
+
+def calibrate(sf, args, scene, local):
+    """Writes bench_calibration.json: the red-black iterations each step of
+    the benchmark scene needs to reach the tolerance, from zero (this
+    library's rbgs variant, bit-identical to the reference's arithmetic),
+    stepping from the scene's first step on."""
+    opts = solver_options(sf, "rbgs", args.tolerance, args.cap, 0)
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=local)
+    sf.scenes.apply_inputs(sim, scene, 0)
+    needs = []
+    for _ in range(args.calibrate_steps):
+        sim.step(1)
+        needs.append(sim.stats().pressure_iterations)
+    sim.close()
+    doc = {**calibration_key(args), "rbgs_iterations_per_step": needs,
+           "written_by": "python bench.py --calibrate (the library's red-black variant, residual-driven, from zero)"}
+    CALIBRATION.write_text(json.dumps(doc, indent=1) + "\n")
+    return doc
+
+
+def read_calibration(args, first, count):
+    """Per-step red-black needs of steps first .. first + count - 1 (0-based)
+    from bench_calibration.json, or None if the file does not cover them."""
+    try:
+        doc = json.loads(CALIBRATION.read_text())
+    except (OSError, ValueError):
+        return None
+    if any(doc.get(k) != v for k, v in calibration_key(args).items()):
+        return None
+    needs = doc.get("rbgs_iterations_per_step", [])
+    return needs[first:first + count] if len(needs) >= first + count else None
+
+
+def time_reference(sf, lib, scene, iterations, steps, warmup, local):
+    """Steps/s of the reference library with a fixed pressure-iteration count."""
     import torch
 
-    from oracle import oracle as orc
-
-    if rank != 0:
-        return None
-    # calibration (untimed): iterations the reference arithmetic needs in each step
-    opts = solver_options(sf, "rbgs", args.tolerance, args.cap, 0)
-    cal = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=local)
-    sf.scenes.apply_inputs(cal, scene, 0)
-    needed = []
-    for _ in range(args.warmup + args.steps):
-        cal.step(1)
-        needed.append(cal.stats().pressure_iterations)
-    cal.close()
-    iterations = max(needed[args.warmup:])
-    lib = sf.load_library(orc.REF_LIB_PATH)
     cfg = type(scene.config).from_buffer_copy(scene.config)
     cfg.pressure_iterations = iterations
     sim = sf.Simulation(cfg, scene.scalars, scene.vectors, lib=lib, device=local)
     sf.scenes.apply_inputs(sim, scene, 0)
-    sim.step(args.warmup)
+    sim.step(warmup)
     torch.cuda.synchronize()
-    with Clocks(local, not args.no_clocks) as clk:
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(sim.stream)
-        sim.step(args.steps)
-        end.record(sim.stream)
-        torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(sim.stream)
+    sim.step(steps)
+    end.record(sim.stream)
+    torch.cuda.synchronize()
     t = start.elapsed_time(end) / 1000.0
     sim.close()
-    value = args.steps / t
+    return steps / t
+
+
+def reference_arm(sf, args, scene, world, rank, local):
+    """The reference backend (oracle/_ref) at equal residual, with the
+    per-step iteration needs read from bench_calibration.json. Only the
+    reference library is loaded in this process."""
+    from oracle import oracle as orc
+
+    if rank != 0:
+        return None
     n = args.size
-    config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g}, 1 scalar + 1 force field, Stam walls", "grid": [n, n, n],
-              "solver": f"reference red-black Gauss-Seidel from zero, {iterations} iterations per step (the most any timed step needs for rel_res <= {args.tolerance:g}; per-step needs {needed[args.warmup:]})",
+    needs = read_calibration(args, args.warmup, args.steps)
+    if needs is None:
+        return {"impl": "reference", "unavailable": f"bench_calibration.json does not cover steps {args.warmup}..{args.warmup + args.steps - 1} of the {n}^3 scene at tolerance {args.tolerance:g}; run `python bench.py --calibrate --calibrate-steps {args.warmup + args.steps}`"}
+    lib = sf.load_library(orc.REF_LIB_PATH)
+    mean_need = int(round(statistics.mean(needs)))
+    with Clocks(local, not args.no_clocks) as clk:
+        value = time_reference(sf, lib, scene, mean_need, args.steps, args.warmup, local)
+    at_max = time_reference(sf, lib, scene, max(needs), args.steps, args.warmup, local)
+    config = {"workload": f"plume {n}^3 FP32, 20 diffusion its, pressure to rel_res <= {args.tolerance:g}, Stam walls", "grid": [n, n, n],
+              "solver": f"reference red-black Gauss-Seidel from zero, {mean_need} iterations per step: the mean of the timed steps' needs {needs} (bench_calibration.json)",
               "l2": "working set > L2 (no flush needed)", "parallelism": "single GPU"}
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)",
+            "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)",
             "config": config, "cell_updates_per_s": value * n ** 3,
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": f"{args.steps} steps; the reference has no CPU implementation, so its own CUDA backend (backend-cuda.cu built unmodified for sm_100a) runs on the GPU"},
-            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "at_max_need": {"steps_per_s": at_max, "pressure_iterations": max(needs), "note": "the fixed count that reaches the tolerance in every timed step"},
+            "reference_run": {"kind": "reference", "device": "the same B200 (the reference has no CPU implementation; backend-cuda.cu built unmodified for sm_100a, oracle/_ref)",
+                              "sample": f"{args.warmup} untimed + {args.steps} timed steps per iteration count"}}
     line["fixed_iterations"] = fixed_iterations(sf, lib, scene, args.fixed_steps, args.warmup, local, 1)
     if args.batch_steps > 0:
         line["batched"] = batched(sf, lib, args.batch_steps, args.warmup, mode=None)
@@ -649,6 +701,11 @@ def main():
     scene = sf.scenes.config1(n=args.size)
     n = args.size
 
+    if args.calibrate:
+        if rank == 0:
+            doc = calibrate(sf, args, scene, local)
+            print(json.dumps({"calibration": str(CALIBRATION.name), "rbgs_iterations_per_step": doc["rbgs_iterations_per_step"]}))
+        return
     if args.impl == "reference":
         line = reference_arm(sf, args, scene, world, rank, local)
         if line is not None:
@@ -681,12 +738,15 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     tc_peak = float(peaks.get("bf16_tflops", 1590.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    sweep_s = time_pressure_sweep(sf, scene, local)
+    launch_s, sweeps_per_launch = time_pressure_sweep(sf, scene, local)
     cells = n ** 3
-    bytes_per_sweep = 12 * cells
-    achieved = bytes_per_sweep / sweep_s / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_jacobi_vec4 (Jacobi pressure sweep)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": 177.19e6 if n == 256 else None, "traffic_source": "ncu capture of k_jacobi_vec4 (pressure) at 256^3: dram__bytes_read.sum 138.9 MB + dram__bytes_write.sum 38.3 MB", "bytes_per_launch": bytes_per_sweep, "launch_us": sweep_s * 1e6, "unit_of_work": "one Jacobi sweep of 256^3 cells: read p + rhs, write p = 12 B/cell"}
+    bytes_per_launch = 12 * cells
+    achieved = bytes_per_launch / launch_s / 1e9
+    traffic = PASS_TRAFFIC.get(n)
+    roofline = {"bound": "hbm", "kernel": f"k_wave (Jacobi pressure pass, {sweeps_per_launch:g} sweeps per launch)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": traffic[0] if traffic else None, "traffic_source": traffic[1] if traffic else None, "bytes_per_launch": bytes_per_launch, "launch_us": launch_s * 1e6,
+                "sweeps_per_launch": sweeps_per_launch, "sweep_us": launch_s * 1e6 / sweeps_per_launch,
+                "unit_of_work": f"one pass of {sweeps_per_launch:g} Jacobi sweeps over {n}^3 cells: read p + rhs, write p = 12 B/cell"}
     roofline_network = None
     if net is not None:
         net_s = time_network(net, n, torch.device("cuda", local))
@@ -709,20 +769,39 @@ def main():
     viewer = scene_generator(sf, n, args.scene_steps, local) if args.scene_steps > 0 else None
     render = volume_render(sf, n, local, frames=args.render_frames) if args.render_frames > 0 else None
 
-    config = {"workload": f"plume {n}^3 FP32, 20 diffusion iterations, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), 1 scalar + 1 force field, Stam walls",
+    config = {"workload": f"plume {n}^3 FP32, 20 diffusion its, pressure to rel_res <= {args.tolerance:g} (checked every {CHECK_INTERVAL} sweeps), Stam walls",
               "grid": [n, n, n], "solver": {"learned": "Jacobi sweeps from the learned warm start", "plain": "Jacobi sweeps from zero", "previous": "Jacobi sweeps from the previous pressure", "rbgs": "red-black Gauss-Seidel from zero"}[headline]
             + (f", {args.fixed_pressure_iterations} sweeps per step (profiling)" if args.fixed_pressure_iterations else ""), "l2": "working set > L2 (no flush needed)",
               "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    # the rbgs variant must still need what bench_calibration.json (the
+    # reference arm's iteration counts) says
+    calibration_check = None
+    if "rbgs" in results and not args.fixed_pressure_iterations:
+        expected = read_calibration(args, args.warmup, args.steps)
+        got = results["rbgs"]["pressure_iterations"]
+        calibration_check = "no calibration for these steps" if expected is None else ("match" if expected == got else f"MISMATCH: calibration {expected}, this run {got}")
+        if expected is not None and expected != got:
+            print(f"bench: rbgs iterations differ from {CALIBRATION.name}: {expected} vs {got}", file=sys.stderr)
+    ratios = {"speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
+              "learned_vs_previous": value / results["previous"]["steps_per_s"] if "previous" in results and headline == "learned" else None,
+              "mean_sweeps": {v: statistics.mean(r["pressure_iterations"]) for v, r in results.items()}}
+    # Bulky per-step detail first; the compact summary of every leg last, so
+    # that it survives in a record that keeps only the end of the line.
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
-            "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"],
-            "speedup_vs_plain_jacobi": value / results["plain"]["steps_per_s"] if "plain" in results else None,
-            "variants": results, "training": train_info, "roofline": roofline, "roofline_network": roofline_network, "e2e": e2e, "fixed_iterations": fixed, "batched": batch, "bf16_storage": mixed, "viewer_scene_forces": viewer, "volume_render": render}
+            "variants": results, "training": train_info, "batched": batch, "viewer_scene_forces": viewer, "volume_render": render, "roofline_network": roofline_network,
+            "e2e": e2e, "roofline": roofline, "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"]}
     c = clk.summary() if rank == 0 else None
     if c:
         line["clocks"] = c
     if rank == 0 and world == 1 and not args.no_cpu_baseline and "plain" in results and not args.fixed_pressure_iterations:
         line["cpu_baseline"] = cpu_baseline(sf, scene, statistics.mean(results["plain"]["pressure_iterations"]))
+    line["summary"] = {**ratios, "steps_per_s": {v: round(r["steps_per_s"], 3) for v, r in results.items()}, "calibration_check": calibration_check,
+                       "e2e_steps_per_s": e2e["value"] if e2e else None, "jacobi_sweep_us": roofline["sweep_us"], "roofline_frac": roofline["frac"],
+                       "network_ms": roofline_network["launch_ms"] if roofline_network else None,
+                       "fixed_iterations_steps_per_s": fixed["steps_per_s"] if fixed else None,
+                       "batched_gcups": {"work_table": batch["cell_updates_per_s"] / 1e9, "graphs": batch["graphs_layout"]["cell_updates_per_s"] / 1e9} if batch else None,
+                       "bf16": {k: mixed[k] for k in ("fp32_steps_per_s", "bf16_steps_per_s", "rel_l2_bf16_vs_fp32")} if mixed else None}
     if net is not None:
         net.close()
     if rank == 0:

@@ -110,6 +110,11 @@ typedef struct StableFluidsB200StepInfo {
     int32_t iterations_per_pass;
     int32_t blocked;                  /* 1: temporally blocked stencil passes */
     uint64_t device_bytes;            /* device memory the context holds */
+    int32_t kernels_per_check;        /* residual-driven solve: kernel launches of one
+                                         pass of the loop body (the interval's sweeps,
+                                         the residual sums and the check); counted once
+                                         in kernels_per_step */
+    int32_t reserved;
 } StableFluidsB200StepInfo;
 
 /* Enqueues one stage of the step on the context stream, outside the step

@@ -172,7 +172,7 @@ class B200VolumeRender(ctypes.Structure):
 
 
 class B200StepInfo(ctypes.Structure):
-    _fields_ = [("kernels_per_step", c_int32), ("scheme", c_uint32), ("iterations_per_pass", c_int32), ("blocked", c_int32), ("device_bytes", c_uint64)]
+    _fields_ = [("kernels_per_step", c_int32), ("scheme", c_uint32), ("iterations_per_pass", c_int32), ("blocked", c_int32), ("device_bytes", c_uint64), ("kernels_per_check", c_int32), ("reserved", c_int32)]
 
 
 def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "sf_batch.h"
+#include "sf_boundary.h"
 #include "sf_launch.h"
 #include "sf_types.h"
 #include "sf_unet.h"
@@ -103,6 +104,7 @@ struct Context {
     cudaEvent_t ready = nullptr;
     bool residual_enabled = false;
     int step_kernels = 0;  // kernel nodes in the step graph
+    int check_kernels = 0;  // kernel nodes in the residual loop's body
     bool blocked = true;   // temporally blocked stencil passes
 
     ~Context() {
@@ -116,19 +118,7 @@ struct Context {
     }
 };
 
-bool valid_flow_type(uint32_t t) { return t <= STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC; }
 bool valid_scalar_type(uint32_t t) { return t <= STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC; }
-
-// backend-cuda.cu:516-520 -- known kinds, periodic faces come in pairs.
-bool validate_flow(const StableFluidsFlowBoundaryConfig& b) {
-    const StableFluidsFlowBoundaryFaceDesc* f = &b.x_minus;
-    for (int a = 0; a < 3; ++a) {
-        const auto lo = f[2 * a].type, hi = f[2 * a + 1].type;
-        if (!valid_flow_type(lo) || !valid_flow_type(hi)) return false;
-        if ((lo == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC) != (hi == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC)) return false;
-    }
-    return true;
-}
 
 // backend-cuda.cu:521-525
 bool validate_scalar(const StableFluidsScalarBoundaryConfig& b) {
@@ -139,21 +129,6 @@ bool validate_scalar(const StableFluidsScalarBoundaryConfig& b) {
         if ((lo == STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC) != (hi == STABLE_FLUIDS_SCALAR_BOUNDARY_PERIODIC)) return false;
     }
     return true;
-}
-
-FlowBC flatten(const StableFluidsFlowBoundaryConfig& b) {
-    FlowBC o{};
-    const StableFluidsFlowBoundaryFaceDesc* f = &b.x_minus;
-    for (int k = 0; k < 6; ++k) {
-        o.type[k] = static_cast<int32_t>(f[k].type);
-        o.vel[k][0] = f[k].velocity_x;
-        o.vel[k][1] = f[k].velocity_y;
-        o.vel[k][2] = f[k].velocity_z;
-        o.pressure[k] = f[k].pressure;
-        if (f[k].type == STABLE_FLUIDS_FLOW_BOUNDARY_OUTFLOW) o.any_outflow = 1;
-    }
-    for (int a = 0; a < 3; ++a) o.periodic[a] = f[2 * a].type == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC && f[2 * a + 1].type == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC;
-    return o;
 }
 
 ScalarBC flatten(const StableFluidsScalarBoundaryConfig& b) {
@@ -416,9 +391,11 @@ struct Stages {
         if (!ok(cudaStreamBeginCaptureToGraph(c.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), 0)) return;
         const cudaStream_t main = c.stream;
         c.stream = c.body_stream;
+        const int before = launches;
         ok(launch_stencil(stencil(KIND_PRESSURE, INIT_FROM_X, interval, h() * h(), c.pressure, c.divergence), c.stream), 0);
         ok(launch_residual_sums(c.pressure, c.divergence, c.dims, h() * h(), c.flow, c.stats, c.stream));
         ok(launch_residual_check(c.stats, c.dims, singular, 0, interval, tol, max_it, handle, c.stream));
+        c.check_kernels = launches - before;
         c.stream = main;
         cudaGraph_t captured = nullptr;
         ok(cudaStreamEndCapture(c.body_stream, &captured), 0);
@@ -514,7 +491,8 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
     if (cfg.diffuse_iterations < 0 || cfg.pressure_iterations < 0) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (desc->scalar_field_count > 0 && desc->scalar_fields == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (desc->vector_field_count > 0 && desc->vector_fields == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-    if (!validate_flow(cfg.flow_boundary)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    FlowBC flow{};
+    if (!flatten_flow(cfg.flow_boundary, flow)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;  // backend-cuda.cu:516-520
     for (uint32_t i = 0; i < desc->scalar_field_count; ++i)
         if (!validate_scalar(desc->scalar_fields[i].boundary)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
 
@@ -531,7 +509,7 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
     c->dims = Dims{cfg.nx, cfg.ny, cfg.nz, 0};
     c->cells = static_cast<size_t>(cfg.nx) * static_cast<size_t>(cfg.ny) * static_cast<size_t>(cfg.nz);
     c->field_bytes = c->cells * sizeof(float);
-    c->flow = flatten(cfg.flow_boundary);
+    c->flow = flow;
     c->residual_enabled = options.compute_residual != 0 || options.residual_tolerance > 0.0f;
     // Temporally blocked passes when asked for (iterations_per_pass >= 1);
     // the default one-launch-per-colour kernels are faster on B200 today.
@@ -1466,6 +1444,7 @@ StableFluidsResult stable_fluids_b200_get_step_info(void* context, StableFluidsB
     o.scheme = c.options.scheme;
     o.iterations_per_pass = c.options.iterations_per_pass;
     o.blocked = c.blocked ? 1 : 0;
+    o.kernels_per_check = c.check_kernels;
     *out_info = o;
     return STABLE_FLUIDS_RESULT_OK;
 }

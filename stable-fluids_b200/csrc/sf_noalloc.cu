@@ -17,15 +17,17 @@
 //     on the GPU (different streams, no ordering between them) race and give
 //     wrong results; calls ordered on one stream are fine. Each call
 //     overwrites the partial sums it reads, so nothing has to be cleared.
-//   - the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//   - every call looks up the array's device address on the current device
+//     (cudaGetSymbolAddress); the first call on a device may load the
+//     library's device code there, so make that first call before any
+//     stream capture.
+//   - every invalid argument is rejected before any CUDA call.
 
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
+#include "sf_boundary.h"
 #include "sf_device.cuh"
 #include "sf_types.h"
 #include "stable-fluids-b200.h"
@@ -34,7 +36,6 @@ namespace sfb {
 namespace {
 
 constexpr int kMaxPlanes = 4096;
-constexpr int kMaxDevices = 64;
 constexpr int kThreads = 256;
 
 // Partial sums per z plane: sum e, sum e^2, sum b, sum b^2 (e = b - A p).
@@ -101,22 +102,16 @@ __global__ void k_finish(const double (*partials)[4], int nz, double n, int sing
     out[1] = sqrt(b2);
 }
 
-// Device address of the partials array, looked up once per device with that
-// device current.
-double (*partials_on_device(int device))[4] {
-    static std::mutex mu;
-    static void* addr[kMaxDevices] = {};
-    if (device < 0 || device >= kMaxDevices) return nullptr;
-    std::lock_guard<std::mutex> lock(mu);
-    if (addr[device] == nullptr) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_residual_partials) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        addr[device] = p;
+// Device address of the partials array on the current device and context.
+// Looked up on every call (a cheap runtime query), so a reset device or a
+// different context never sees a stale address.
+double (*partials_address())[4] {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_residual_partials) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
     }
-    return static_cast<double (*)[4]>(addr[device]);
+    return static_cast<double (*)[4]>(p);
 }
 
 }  // namespace
@@ -124,31 +119,15 @@ double (*partials_on_device(int device))[4] {
 
 extern "C" StableFluidsResult stable_fluids_b200_pressure_residual_noalloc(const float* pressure, const float* divergence, int32_t nx, int32_t ny, int32_t nz, float cell_size, const StableFluidsFlowBoundaryConfig* flow_boundary, double* out_residual, void* stream) {
     using namespace sfb;
+    // every rejection happens here, before any CUDA call
     if (pressure == nullptr || divergence == nullptr || flow_boundary == nullptr || out_residual == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (nx <= 0 || ny <= 0 || nz <= 0 || !(cell_size > 0.0f) || !std::isfinite(cell_size)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     if (nz > kMaxPlanes) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;  // beyond the fixed scratch: rejected
     if (static_cast<long long>(nx) * ny > (1ll << 30)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-    auto partials = partials_on_device(device);
-    if (partials == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-
     FlowBC b{};
-    const StableFluidsFlowBoundaryFaceDesc* f = &flow_boundary->x_minus;
-    for (int k = 0; k < 6; ++k) {
-        if (f[k].type > STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        b.type[k] = static_cast<int32_t>(f[k].type);
-        b.vel[k][0] = f[k].velocity_x;
-        b.vel[k][1] = f[k].velocity_y;
-        b.vel[k][2] = f[k].velocity_z;
-        b.pressure[k] = f[k].pressure;
-        if (f[k].type == STABLE_FLUIDS_FLOW_BOUNDARY_OUTFLOW) b.any_outflow = 1;
-    }
-    for (int a = 0; a < 3; ++a) {
-        const bool lo = f[2 * a].type == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC, hi = f[2 * a + 1].type == STABLE_FLUIDS_FLOW_BOUNDARY_PERIODIC;
-        if (lo != hi) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
-        b.periodic[a] = lo ? 1 : 0;
-    }
+    if (!flatten_flow(*flow_boundary, b)) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto partials = partials_address();
+    if (partials == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     const Dims d{nx, ny, nz, 0};
     const float h2 = cell_size * cell_size;
     const auto s = static_cast<cudaStream_t>(stream);

@@ -100,3 +100,28 @@ def test_enum_values(sf):
     assert (sf.FLOW_NO_SLIP_WALL, sf.FLOW_FREE_SLIP_WALL, sf.FLOW_OUTFLOW, sf.FLOW_PERIODIC) == (0, 1, 2, 3)
     assert (sf.SCALAR_FIXED_VALUE, sf.SCALAR_ZERO_FLUX, sf.SCALAR_PERIODIC) == (0, 1, 2)
     assert sf.VIEW_FLOW_DIVERGENCE == 6 and sf.VIEW_LAYOUT_F32_3D_SOA3 == 1
+
+
+EXT_STRUCTS = {"StableFluidsB200Options": "B200Options", "StableFluidsB200StepStats": "B200StepStats", "StableFluidsB200StepInfo": "B200StepInfo",
+               "StableFluidsB200BatchOptions": "B200BatchOptions", "StableFluidsB200VolumeRender": "B200VolumeRender"}
+
+
+def test_ctypes_mirror_matches_extension_header(sf, tmp_path):
+    """The binding's copies of the extension structs (stable-fluids-b200.h)
+    have the compiler's sizes and field offsets."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "stable-fluids-b200.h"', "int main(void) {"]
+    for cname, pyname in EXT_STRUCTS.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in getattr(sf, pyname)._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "probe_ext.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe_ext"
+    subprocess.run(["gcc", "-std=c11", "-I", str(INCLUDE), str(src), "-o", str(exe)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines())
+    for cname, pyname in EXT_STRUCTS.items():
+        cls = getattr(sf, pyname)
+        assert int(got[f"{cname} sizeof"]) == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, (cname, fname)

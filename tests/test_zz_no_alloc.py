@@ -56,3 +56,35 @@ def test_noalloc_residual_rejects_grids_beyond_its_scratch(sf, lib, cuda):
     walls = sf.scenes.stam_walls()[0]
     rc = lib.stable_fluids_b200_pressure_residual_noalloc(dummy.data_ptr(), dummy.data_ptr(), 2, 2, 4097, 0.1, ctypes.byref(walls), out.data_ptr(), None)
     assert rc == sf.RESULT_BACKEND_FAILURE
+
+
+@pytest.mark.gpu
+def test_noalloc_residual_rejects_invalid_arguments(sf, lib, cuda):
+    """Every invalid argument is refused before any work is enqueued: null
+    pointers, a non-positive or NaN cell size, an unknown face kind and an
+    unpaired periodic face. A valid call with the same buffers succeeds."""
+    torch = cuda
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    field = torch.zeros(4 * 4 * 4, dtype=torch.float32, device="cuda")
+    sc = sf.scenes
+    walls = sc.stam_walls()[0]
+    unpaired = sc.flow_boundary([sf.FLOW_PERIODIC, sf.FLOW_FREE_SLIP_WALL] + [sf.FLOW_FREE_SLIP_WALL] * 4)
+    unknown = sc.flow_boundary([7] + [sf.FLOW_FREE_SLIP_WALL] * 5)
+    fn = lib.stable_fluids_b200_pressure_residual_noalloc
+    p, q, o = field.data_ptr(), field.data_ptr(), out.data_ptr()
+    bad = [
+        (None, q, 4, 4, 4, 0.25, ctypes.byref(walls), o),
+        (p, None, 4, 4, 4, 0.25, ctypes.byref(walls), o),
+        (p, q, 4, 4, 4, 0.25, None, o),
+        (p, q, 4, 4, 4, 0.25, ctypes.byref(walls), None),
+        (p, q, 4, 4, 4, 0.0, ctypes.byref(walls), o),
+        (p, q, 4, 4, 4, float("nan"), ctypes.byref(walls), o),
+        (p, q, 0, 4, 4, 0.25, ctypes.byref(walls), o),
+        (p, q, 4, 4, 4, 0.25, ctypes.byref(unknown), o),
+        (p, q, 4, 4, 4, 0.25, ctypes.byref(unpaired), o),
+    ]
+    for args in bad:
+        assert fn(*args, None) == sf.RESULT_BACKEND_FAILURE, args
+    assert fn(p, q, 4, 4, 4, 0.25, ctypes.byref(walls), o, None) == sf.RESULT_OK
+    torch.cuda.synchronize()
+    assert out[0].item() == 0.0  # zero right-hand side: residual defined as 0
