@@ -357,10 +357,13 @@ struct Sim {
 
     // One colour of a diffusion RBGS iteration, backend-cuda.cu:354-375:
     // x = (b + alpha * sum6(x)) / (1 + 6 alpha), neighbour order
-    // x-, x+, y-, y+, z-, z+; JACOBI reads src_x and writes dst_x.
+    // x-, x+, y-, y+, z-, z+; JACOBI (parity < 0) reads src_x, writes dst_x
+    // and multiplies by the rounded reciprocal instead of dividing (the
+    // library's Jacobi arithmetic; the reference has no Jacobi scheme).
     template <class Load>
     void diffuse_pass(R* dst, const R* srcx, const R* b, R alpha, int parity, const Load& load) {
         const R denom = mad(R(6), alpha, R(1));
+        const R inv = R(1) / denom;
 #pragma omp parallel for schedule(static)
         for (int z = 0; z < d.nz; ++z)
             for (int y = 0; y < d.ny; ++y)
@@ -368,7 +371,7 @@ struct Sim {
                     if (parity >= 0 && ((x + y + z) & 1) != parity) continue;
                     const R nb = load(srcx, x - 1, y, z) + load(srcx, x + 1, y, z) + load(srcx, x, y - 1, z) + load(srcx, x, y + 1, z) + load(srcx, x, y, z - 1) + load(srcx, x, y, z + 1);
                     const std::size_t i = at(x, y, z, d);
-                    dst[i] = mad(alpha, nb, b[i]) / denom;
+                    dst[i] = parity >= 0 ? mad(alpha, nb, b[i]) / denom : mad(alpha, nb, b[i]) * inv;
                 }
     }
 
@@ -400,9 +403,11 @@ struct Sim {
                 }
     }
 
-    // backend-cuda.cu:398-407 -- p = (sum6(p) - h^2 div) / 6.
+    // backend-cuda.cu:398-407 -- p = (sum6(p) - h^2 div) / 6; JACOBI
+    // (parity < 0) multiplies by the rounded reciprocal RN(1/6) instead.
     void pressure_pass(R* dst, const R* src, R h2, int parity) {
         const auto& bc = cfg.flow_boundary;
+        const R inv6 = R(1) / R(6);
 #pragma omp parallel for schedule(static)
         for (int z = 0; z < d.nz; ++z)
             for (int y = 0; y < d.ny; ++y)
@@ -411,7 +416,7 @@ struct Sim {
                     const R nb = load_pressure(src, x - 1, y, z, d, bc) + load_pressure(src, x + 1, y, z, d, bc) + load_pressure(src, x, y - 1, z, d, bc) + load_pressure(src, x, y + 1, z, d, bc) + load_pressure(src, x, y, z - 1, d, bc)
                                + load_pressure(src, x, y, z + 1, d, bc);
                     const std::size_t i = at(x, y, z, d);
-                    dst[i] = mad(-h2, divergence[i], nb) / R(6);
+                    dst[i] = parity >= 0 ? mad(-h2, divergence[i], nb) / R(6) : mad(-h2, divergence[i], nb) * inv6;
                 }
     }
 

@@ -19,6 +19,7 @@
 #include "sf_device.cuh"
 #include "sf_launch.h"
 #include "sf_stencil_tb.cuh"
+#include "sf_stencil_wave.cuh"
 
 namespace sfb {
 
@@ -93,8 +94,7 @@ __global__ void __launch_bounds__(256) k_jacobi(T* __restrict__ dst, const T* __
     const int z0 = static_cast<int>(blockIdx.z) * kColourPlanes;
     if (cx >= d.nx || y >= d.ny) return;
     const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const double recip = tb::recip64(divisor);
+    const float inv = wave::jacobi_inverse(KIND, coef);
     const bool xy_interior = cx >= 1 && cx <= d.nx - 2 && y >= 1 && y <= d.ny - 2;
 #pragma unroll
     for (int k = 0; k < kColourPlanes; ++k) {
@@ -108,8 +108,7 @@ __global__ void __launch_bounds__(256) k_jacobi(T* __restrict__ dst, const T* __
         } else {
             nb = neighbour_sum<KIND>(src, cx, y, z, d, fb, sb);
         }
-        const float num = tb::numerator<KIND>(nb, to_f(rhs[i]), coef);
-        dst[i] = from_f<T>(tb::divide(num, divisor, recip));
+        dst[i] = from_f<T>(wave::jacobi_update<KIND>(nb, to_f(rhs[i]), coef, inv));
     }
 }
 
@@ -190,8 +189,7 @@ __device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__
     const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
     const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const double recip = tb::recip64(divisor);
+    const float inv = wave::jacobi_inverse(KIND, coef);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
     int i = x0 + d.nx * (y + d.ny * zb);
@@ -208,10 +206,10 @@ __device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__
         if (v.gy_lo) c = ghost4(g, YM, c);
         if (v.gy_hi) e = ghost4(g, YP, e);
         float4 o;
-        o.x = vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip);
-        o.y = vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip);
-        o.z = vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip);
-        o.w = vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip);
+        o.x = wave::jacobi_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, inv);
+        o.y = wave::jacobi_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, inv);
+        o.z = wave::jacobi_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, inv);
+        o.w = wave::jacobi_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, inv);
         *reinterpret_cast<float4*>(dst + i) = o;
         below = cur;
         cur = above;
@@ -314,6 +312,7 @@ __device__ __forceinline__ void march_bf16(__nv_bfloat16* dst, const __nv_bfloat
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const double recip = tb::recip64(divisor);
+    const float inv = wave::jacobi_inverse(KIND, coef);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
     int i = x0 + d.nx * (y + d.ny * zb);
@@ -342,8 +341,8 @@ __device__ __forceinline__ void march_bf16(__nv_bfloat16* dst, const __nv_bfloat
                 o.y = pack_bf2(cur.z, vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip));
             }
         } else {
-            o.x = pack_bf2(vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip), vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip));
-            o.y = pack_bf2(vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip), vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip));
+            o.x = pack_bf2(wave::jacobi_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, inv), wave::jacobi_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, inv));
+            o.y = pack_bf2(wave::jacobi_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, inv), wave::jacobi_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, inv));
         }
         *reinterpret_cast<uint2*>(dst + at) = o;
         below = cur;
@@ -421,109 +420,6 @@ bool vec_ok(const StencilArgs& a, int width = 4) {
     const auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
     const size_t cells = static_cast<size_t>(a.dims.nx) * a.dims.ny * a.dims.nz;
     return a.dims.nx % width == 0 && cells < (1ull << 31) && al(a.x) && al(a.b) && (a.scratch == nullptr || al(a.scratch));
-}
-
-// Two Jacobi sweeps per pass (temporal blocking), for the vectorised grids
-// (nx % 4 == 0): a CTA owns an output tile of kT2OX x kT2OY cells over a z
-// chunk and marches up it. Each of its kT2G x kT2R threads owns one float4 of
-// the input tile (the output tile plus a halo of two float4 groups in x and
-// two rows in y) and keeps its column's input planes q-1, q, q+1 and its
-// first-sweep planes in registers, so z neighbours never touch shared
-// memory. Per plane q: every thread stores its input float4 of plane q into a
-// two-slot shared ring and one barrier follows; the inner (kT2G-2) x
-// (kT2R-2) threads compute the first sweep at plane q from the x/y
-// neighbours in shared memory and store it into a second two-slot ring; the
-// output threads compute the second sweep at plane q-1 from the first-sweep
-// ring (written one plane earlier, before this plane's barrier) and write it.
-// Loads of plane q+2 are issued two planes ahead. One barrier per plane is
-// enough: a ring slot is rewritten only two planes after it was read, and
-// every thread has passed the barrier in between. Face ghosts are the
-// GhostRule of the float4 sweep (self value substituted and mirrored, copied
-// or fixed), periodic axes are read wrapped, and the per-cell arithmetic and
-// sum order are k_jacobi_vec4's, so two sweeps here are bit-identical to two
-// single sweeps. Algorithmic traffic: 12 B per cell per two sweeps.
-constexpr int kT2G = 12, kT2R = 20;                       // input float4 groups per row, input rows
-constexpr int kT2Threads = kT2G * kT2R;                   // 240
-constexpr int kT2OX = 4 * (kT2G - 4), kT2OY = kT2R - 4;   // output tile: 32 x 16 cells
-constexpr int kT2W = 4 * kT2G;                            // floats per shared row
-
-template <int KIND>
-__global__ void __launch_bounds__(kT2Threads) k_jacobi_tb2(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
-    __shared__ __align__(16) float s_in[2][kT2R][kT2W];
-    __shared__ __align__(16) float s_s1[2][kT2R][kT2W];
-    const int t = static_cast<int>(threadIdx.x);
-    const int gi = t % kT2G, ri = t / kT2G;
-    const int gx = static_cast<int>(blockIdx.x) * kT2OX + 4 * (gi - 2);  // first cell of this thread's float4 (unwrapped)
-    const int gy = static_cast<int>(blockIdx.y) * kT2OY + ri - 2;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const double recip = tb::recip64(divisor);
-    // the stored column this float4 reads: wrapped on periodic axes, absent outside a non-periodic one
-    int lx = gx, ly = gy;
-    bool live = true;
-    if (lx < 0 || lx >= d.nx) {
-        if (g.periodic[0]) lx = ((lx % d.nx) + d.nx) % d.nx;
-        else live = false;
-    }
-    if (ly < 0 || ly >= d.ny) {
-        if (g.periodic[1]) ly = ((ly % d.ny) + d.ny) % d.ny;
-        else live = false;
-    }
-    const int col = live ? lx + d.nx * ly : 0;
-    const int sz = d.nx * d.ny;
-    const bool s1_thread = live && gi >= 1 && gi <= kT2G - 2 && ri >= 1 && ri <= kT2R - 2;
-    const bool out_thread = gi >= 2 && gi <= kT2G - 3 && ri >= 2 && ri <= kT2R - 3 && gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny;
-    const bool fx_lo = !g.periodic[0] && gx == 0, fx_hi = !g.periodic[0] && gx + 4 == d.nx;
-    const bool fy_lo = !g.periodic[1] && gy == 0, fy_hi = !g.periodic[1] && gy == d.ny - 1;
-    const auto plane = [&](int q) { return g.periodic[2] ? (q < 0 ? q + d.nz : (q >= d.nz ? q - d.nz : q)) : (static_cast<unsigned>(q) < static_cast<unsigned>(d.nz) ? q : -1); };
-    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const auto load = [&](const float* f, int q) {
-        const int pq = plane(q);
-        return (live && pq >= 0) ? ld4(f + col + sz * pq) : zero;
-    };
-    // one update of this thread's float4 from the ring slot `ring` (x/y
-    // neighbours) and its own z neighbours, with the face ghosts
-    const auto sweep = [&](const float (*ring)[kT2W], float4 cur, float4 below, float4 above, float4 r, int q) {
-        float a = ring[ri][4 * gi - 1], b = ring[ri][4 * gi + 4];
-        float4 c = *reinterpret_cast<const float4*>(&ring[ri - 1][4 * gi]);
-        float4 e = *reinterpret_cast<const float4*>(&ring[ri + 1][4 * gi]);
-        if (fx_lo) a = tb::ghost(g, XM, cur.x);
-        if (fx_hi) b = tb::ghost(g, XP, cur.w);
-        if (fy_lo) c = ghost4(g, YM, cur);
-        if (fy_hi) e = ghost4(g, YP, cur);
-        if (!g.periodic[2] && q == 0) below = ghost4(g, ZM, cur);
-        if (!g.periodic[2] && q == d.nz - 1) above = ghost4(g, ZP, cur);
-        float4 o;
-        o.x = vec_update<KIND>(a + cur.y + c.x + e.x + below.x + above.x, r.x, coef, divisor, recip);
-        o.y = vec_update<KIND>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, coef, divisor, recip);
-        o.z = vec_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, divisor, recip);
-        o.w = vec_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, divisor, recip);
-        return o;
-    };
-    // registers at the start of plane q = zb - 1: input q-1, q, q+1 and q+2 (in flight), rhs q and q+1
-    float4 in_m = load(src, zb - 2), in_c = load(src, zb - 1), in_p = load(src, zb), in_n = load(src, zb + 1);
-    float4 rhs_c = load(rhs, zb - 1), rhs_n = load(rhs, zb), rhs_m = zero;
-    float4 s1_mm = zero, s1_m = zero;
-    for (int q = zb - 1; q <= ze; ++q) {
-        *reinterpret_cast<float4*>(&s_in[q & 1][ri][4 * gi]) = in_c;
-        const float4 in_nn = (q + 3 <= ze + 1) ? load(src, q + 3) : zero;
-        const float4 rhs_nn = (q + 2 <= ze) ? load(rhs, q + 2) : zero;
-        __syncthreads();  // input plane q staged; the first sweep of plane q - 1 is visible
-        float4 s1 = zero;
-        if (s1_thread && plane(q) >= 0) s1 = sweep(s_in[q & 1], in_c, in_m, in_p, rhs_c, plane(q));
-        *reinterpret_cast<float4*>(&s_s1[q & 1][ri][4 * gi]) = s1;
-        const int qo = q - 1;
-        if (out_thread && qo >= zb && qo < ze) *reinterpret_cast<float4*>(dst + col + sz * qo) = sweep(s_s1[qo & 1], s1_m, s1_mm, s1, rhs_m, qo);
-        s1_mm = s1_m;
-        s1_m = s1;
-        in_m = in_c;
-        in_c = in_p;
-        in_p = in_n;
-        in_n = in_nn;
-        rhs_m = rhs_c;
-        rhs_c = rhs_n;
-        rhs_n = rhs_nn;
-    }
 }
 
 // FP64 sums of the pressure residual e = h^2 div - (sum6(p) - 6 p) and of
@@ -606,30 +502,6 @@ __global__ void k_scale_field(T* __restrict__ q, float factor, size_t n) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(to_f(q[i]) * factor);
 }
 
-struct TbShape2 {
-    dim3 grid;
-    int z_chunk;
-};
-
-// Launch shape of k_jacobi_tb2: one wave of CTAs, z chunks of at least 8 planes.
-template <typename Kernel>
-TbShape2 tb2_shape(const Dims& d, Kernel kernel) {
-    static int per_sm = [&] {
-        int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kT2Threads, 0) != cudaSuccess || n < 1) n = 2;
-        return n;
-    }();
-    int sms = 148;
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int bx = (d.nx + kT2OX - 1) / kT2OX, by = (d.ny + kT2OY - 1) / kT2OY;
-    long long chunks = static_cast<long long>(sms) * per_sm / (static_cast<long long>(bx) * by);
-    if (chunks < 1) chunks = 1;
-    int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
-    if (z_chunk < 8) z_chunk = d.nz < 8 ? d.nz : 8;
-    return {dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), static_cast<unsigned>((d.nz + z_chunk - 1) / z_chunk)), z_chunk};
-}
-
 GhostRule ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb);
 
 // Vectorised sweep kernels per element type (4 cells per thread for both).
@@ -681,17 +553,7 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
         const VecShape vs = vec ? vec_shape(d, jacobi_vec) : VecShape{};
         const dim3 jblock(32, 8, 1);
         const dim3 grid(static_cast<unsigned>((d.nx + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
-        // With blocking requested, sweeps go two per pass (k_jacobi_tb2, FP32)
-        // where the grid suits the vectorised kernels, an odd sweep first as
-        // a single sweep. (On B200 two single sweeps are faster: the fused
-        // pass is instruction-bound.)
-        constexpr bool kFp32 = sizeof(T) == sizeof(float);
-        const int pairs = (kFp32 && vec && a.blocked) ? a.iterations / 2 : 0;
-        const int singles = a.iterations - 2 * pairs;
-        const int units = pairs + singles;
-        TbShape2 tb{};
-        if constexpr (kFp32)
-            if (pairs > 0) tb = tb2_shape(d, k_jacobi_tb2<KIND>);
+        const int units = a.iterations;
         // Choose the first source so that the last launch lands in x.
         const T* src = ax;
         if (a.init == INIT_FROM_B) src = ab;
@@ -709,9 +571,7 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             const int left = units - u;  // launches still to run, this one included
             T* dst = (left & 1) ? ax : ascr;
             if (dst == src) dst = (dst == ax) ? ascr : ax;
-            if (u >= singles) {
-                if constexpr (kFp32) k_jacobi_tb2<KIND><<<tb.grid, kT2Threads, 0, s>>>(dst, src, ab, a.coef, tb.z_chunk, d, g);
-            } else if (vec) {
+            if (vec) {
                 jacobi_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, ab, a.coef, vs.z_chunk, d, g);
             } else {
                 k_jacobi<KIND, T><<<grid, jblock, 0, s>>>(dst, src, ab, a.coef, d, a.flow, a.scalar);
@@ -734,6 +594,107 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
     return e;
 }
 
+
+// ------------------------------------------------------ z-wavefront path --
+// K stages per pass (sf_stencil_wave.cuh): Jacobi sweeps, or red-black
+// half-iterations (two stages per iteration), for FP32 fields whose rows are
+// 128 or 256 cells.
+constexpr int kWaveRows = 16;  // rows per CTA (one warp each), halo rows included
+
+// Stages per pass when the caller leaves it open: 4 for rows of 128 cells;
+// 3 for rows of 256 (at 4, a 256-cell row's register history no longer fits
+// the 128 registers a 512-thread CTA can give each thread).
+int wave_default_stages(int v) { return v == 1 ? 4 : 3; }
+
+// Rows of 128 V cells: V, or 0 when the grid does not suit the kernel.
+int wave_width(const StencilArgs& a) {
+    if (a.bf16 || a.scratch == nullptr || !vec_ok(a)) return 0;
+    if (a.dims.nx != 128 && a.dims.nx != 256) return 0;
+    if (a.scheme == SCHEME_RBGS) {
+        // an odd periodic size breaks the red-black colouring across the wrap
+        const int kind = a.kind;
+        const int per[3] = {kind == KIND_SCALAR ? a.scalar.periodic[0] : a.flow.periodic[0], kind == KIND_SCALAR ? a.scalar.periodic[1] : a.flow.periodic[1], kind == KIND_SCALAR ? a.scalar.periodic[2] : a.flow.periodic[2]};
+        const int n[3] = {a.dims.nx, a.dims.ny, a.dims.nz};
+        for (int k = 0; k < 3; ++k)
+            if (per[k] && (n[k] & 1)) return 0;
+    }
+    return a.dims.nx / 128;
+}
+
+template <int KIND, bool RB, int K, int V>
+cudaError_t launch_wave_pass(const wave::WaveArgs& w, int sms, cudaStream_t s) {
+    constexpr size_t smem = wave::WaveLayout<K, V, kWaveRows>::bytes;
+    static_assert(smem <= 232448, "shared memory per CTA");
+    auto kern = wave::k_wave<KIND, RB, K, V, kWaveRows>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (attr != cudaSuccess) return attr;
+    constexpr int ty = kWaveRows - 2 * K;
+    const int tiles = (w.d.ny + ty - 1) / ty;
+    // one wave of CTAs (one per SM): z chunks per tile column
+    int chunks = sms / tiles;
+    if (chunks < 1) chunks = 1;
+    wave::WaveArgs a = w;
+    a.z_chunk = (w.d.nz + chunks - 1) / chunks;
+    const dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>((w.d.nz + a.z_chunk - 1) / a.z_chunk));
+    kern<<<grid, 32 * kWaveRows, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int KIND, bool RB, int V>
+cudaError_t run_wave(const StencilArgs& a, cudaStream_t s) {
+    const Dims& d = a.dims;
+    const size_t bytes = static_cast<size_t>(d.nx) * d.ny * d.nz * sizeof(float);
+    cudaError_t e = cudaSuccess;
+    const int stages = RB ? 2 * a.iterations : a.iterations;
+    int per = wave_default_stages(V);
+    if (a.per_pass >= 2) per = RB ? 2 * a.per_pass : a.per_pass;
+    if (per > 4) per = 4;
+    if (RB) per = per < 2 ? 2 : (per & ~1);  // whole iterations per pass
+    if (stages == 0) {
+        if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
+        else if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(a.x, a.b, bytes, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess || a.out_scale == 1.0f) return e;
+        k_scale_field<<<148u * 32u, 256, 0, s>>>(a.x, a.out_scale, static_cast<size_t>(d.nx) * d.ny * d.nz);
+        if (a.launches) *a.launches += 1;
+        return cudaGetLastError();
+    }
+    wave::WaveArgs w{};
+    w.rhs = a.b;
+    w.coef = a.coef;
+    w.d = d;
+    w.g = ghost_rule(KIND, a.flow, a.scalar);
+    w.parity0 = 0;
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int passes = (stages + per - 1) / per;
+    const float* src = a.init == INIT_ZERO ? nullptr : (a.init == INIT_FROM_B ? a.b : a.x);
+    for (int i = 0; i < passes; ++i) {
+        float* dst = ((passes - 1 - i) % 2 == 0) ? a.x : a.scratch;
+        if (src == dst) {  // warm start from x with an odd pass count: move it aside
+            if ((e = cudaMemcpyAsync(a.scratch, a.x, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+            src = a.scratch;
+        }
+        w.src = src;
+        w.dst = dst;
+        w.k_run = (i == passes - 1) ? stages - per * (passes - 1) : per;
+        w.out_scale = (i == passes - 1) ? a.out_scale : 1.0f;
+        // kernels with a halo of K = 2 or 4 (red-black) and 3 or 4 (Jacobi)
+        // stages; every pass of the solve uses the one sized for `per`
+        if constexpr (RB) e = per == 2 ? launch_wave_pass<KIND, RB, 2, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
+        else e = per <= 3 ? launch_wave_pass<KIND, RB, 3, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
+        if (e != cudaSuccess) return e;
+        if (a.launches) *a.launches += 1;
+        src = dst;
+    }
+    return cudaSuccess;
+}
+
+template <int KIND>
+cudaError_t run_wave_kind(const StencilArgs& a, int v, cudaStream_t s) {
+    const bool rb = a.scheme == SCHEME_RBGS;
+    if (v == 1) return rb ? run_wave<KIND, true, 1>(a, s) : run_wave<KIND, false, 1>(a, s);
+    return rb ? run_wave<KIND, true, 2>(a, s) : run_wave<KIND, false, 2>(a, s);
+}
 
 // ------------------------------------------------ temporally blocked path --
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -982,7 +943,22 @@ bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2
 }
 
 cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
-    if (a.blocked && !a.bf16 && tb_supported(a)) {
+    // per_pass: 0 = automatic (z-wavefront passes where the grid suits them),
+    // 1 = one launch per sweep / colour, >= 2 = that many iterations per pass
+    if (a.per_pass != 1) {
+        if (const int v = wave_width(a)) {
+            switch (a.kind) {
+            case KIND_VEL_X: return run_wave_kind<KIND_VEL_X>(a, v, s);
+            case KIND_VEL_Y: return run_wave_kind<KIND_VEL_Y>(a, v, s);
+            case KIND_VEL_Z: return run_wave_kind<KIND_VEL_Z>(a, v, s);
+            case KIND_SCALAR: return run_wave_kind<KIND_SCALAR>(a, v, s);
+            case KIND_PRESSURE: return run_wave_kind<KIND_PRESSURE>(a, v, s);
+            default: return cudaErrorInvalidValue;
+            }
+        }
+    }
+    // the TMA red-black pass for other grids, when several iterations per pass are asked for
+    if (a.blocked && a.per_pass >= 2 && !a.bf16 && tb_supported(a)) {
         switch (a.kind) {
         case KIND_VEL_X: return run_tb<KIND_VEL_X>(a, s, a.error_flag);
         case KIND_VEL_Y: return run_tb<KIND_VEL_Y>(a, s, a.error_flag);

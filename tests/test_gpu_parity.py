@@ -322,30 +322,82 @@ def test_residual_driven_solve_stops_at_cap(sf, lib, cuda):
     assert st.hit_cap == 1 and st.pressure_iterations == 12 and st.rel_residual > 1e-9
 
 
+def _wave_scene(sf, kind):
+    """Grids whose rows suit the z-wavefront passes (nx = 128 or 256), with
+    several tiles and z chunks, partial last tiles and every boundary kind."""
+    sc = sf.scenes
+    if kind == "stam_128x44x37":
+        return _tiled_scene(sf, (128, 44, 37), sc.stam_walls())
+    if kind == "benchmark_256x30x22":
+        return _tiled_scene(sf, (256, 30, 22), sc.benchmark_walls())
+    if kind == "periodic_y_128x24x40":
+        flow = sc.flow_boundary([sf.FLOW_NO_SLIP_WALL, sf.FLOW_FREE_SLIP_WALL, sf.FLOW_PERIODIC, sf.FLOW_PERIODIC, sf.FLOW_OUTFLOW, sf.FLOW_FREE_SLIP_WALL], pressures=[0, 0, 0, 0, 0.25, 0])
+        sbc = sc.scalar_boundary([sf.SCALAR_FIXED_VALUE, sf.SCALAR_ZERO_FLUX, sf.SCALAR_PERIODIC, sf.SCALAR_PERIODIC, sf.SCALAR_ZERO_FLUX, sf.SCALAR_FIXED_VALUE], values=[0.5, 0, 0, 0, 0, 1.5])
+        return _tiled_scene(sf, (128, 24, 40), (flow, sbc))
+    if kind == "periodic_xz_256x12x10":
+        flow = sc.flow_boundary([sf.FLOW_PERIODIC, sf.FLOW_PERIODIC, sf.FLOW_NO_SLIP_WALL, sf.FLOW_OUTFLOW, sf.FLOW_PERIODIC, sf.FLOW_PERIODIC], velocities=[(0, 0, 0)] * 2 + [(0.3, 0, -0.2), (0, 0, 0)] + [(0, 0, 0)] * 2)
+        sbc = sc.scalar_boundary([sf.SCALAR_PERIODIC, sf.SCALAR_PERIODIC, sf.SCALAR_ZERO_FLUX, sf.SCALAR_FIXED_VALUE, sf.SCALAR_PERIODIC, sf.SCALAR_PERIODIC])
+        return _tiled_scene(sf, (256, 12, 10), (flow, sbc))
+    raise KeyError(kind)
+
+
+WAVE_KINDS = ["stam_128x44x37", "benchmark_256x30x22", "periodic_y_128x24x40", "periodic_xz_256x12x10"]
+
+
+def _run_scene(sf, lib, scene, options=None):
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=options)
+    sf.scenes.run(sim, scene)
+    out = C.collect_outputs(sim, sf, C.Case(scene.name, scene.config, scene.scalars, scene.vectors, scene.steps))
+    sim.close()
+    return out
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["stam_200x60x40", "benchmark_192x56x36", "periodic_xz_128x40x36"])
-def test_blocked_jacobi_matches_single_sweeps(kind, sf, lib, cuda):
-    """Two Jacobi sweeps per HBM pass (iterations_per_pass = 2) give the same
-    bits as one sweep per launch, across tile and z-chunk seams and on
-    periodic axes."""
-    if kind.startswith("stam"):
-        scene = _tiled_scene(sf, (200, 60, 40), sf.scenes.stam_walls())
-    elif kind.startswith("benchmark"):
-        scene = _tiled_scene(sf, (192, 56, 36), sf.scenes.benchmark_walls())
-    else:
-        flow = sf.scenes.flow_boundary([sf.FLOW_PERIODIC, sf.FLOW_PERIODIC, sf.FLOW_FREE_SLIP_WALL, sf.FLOW_OUTFLOW, sf.FLOW_PERIODIC, sf.FLOW_PERIODIC])
-        sbc = sf.scenes.scalar_boundary([sf.SCALAR_PERIODIC, sf.SCALAR_PERIODIC, sf.SCALAR_ZERO_FLUX, sf.SCALAR_FIXED_VALUE, sf.SCALAR_PERIODIC, sf.SCALAR_PERIODIC])
-        scene = _tiled_scene(sf, (128, 40, 36), (flow, sbc))
-    outs = []
-    for per_pass in (0, 2):
+@pytest.mark.parametrize("kind", WAVE_KINDS)
+def test_wave_jacobi_matches_single_sweeps(kind, sf, lib, cuda):
+    """K Jacobi sweeps per HBM pass (the z-wavefront kernel; automatic, 2, 3
+    and 4 per pass) give the same bits as one sweep per launch, across tile
+    and z-chunk seams, partial tiles, every face kind and periodic axes."""
+    scene = _wave_scene(sf, kind)
+    outs = {}
+    for per_pass in (1, 0, 2, 3, 4):
         opts = sf.default_options(lib)
         opts.scheme = sf.SCHEME_JACOBI
         opts.iterations_per_pass = per_pass
-        sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=opts)
-        sf.scenes.run(sim, scene)
-        outs.append(C.collect_outputs(sim, sf, C.Case(kind, scene.config, scene.scalars, scene.vectors, scene.steps)))
-        sim.close()
-    assert_bit_equal(outs[1], outs[0])
+        outs[per_pass] = _run_scene(sf, lib, scene, opts)
+    for per_pass in (0, 2, 3, 4):
+        assert_bit_equal(outs[per_pass], outs[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", WAVE_KINDS)
+def test_wave_rbgs_matches_reference_library(kind, sf, lib, ref_lib, cuda):
+    """Red-black iterations in z-wavefront passes (automatic, one and two
+    iterations per pass) are bit-equal to the reference library, and so is
+    one launch per colour."""
+    scene = _wave_scene(sf, kind)
+    ref = _run_scene(sf, ref_lib, scene)
+    for per_pass in (0, 1, 2):
+        opts = sf.default_options(lib)
+        opts.iterations_per_pass = per_pass
+        assert_bit_equal(_run_scene(sf, lib, scene, opts), ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["stam_128x44x37", "periodic_xz_256x12x10"])
+def test_wave_jacobi_matches_oracle(kind, sf, lib, orc, cuda):
+    """The Jacobi scheme (numerator times the rounded reciprocal) against the
+    FP32 oracle's Jacobi, on grids the wavefront kernel takes."""
+    scene = _wave_scene(sf, kind)
+    opts = sf.default_options(lib)
+    opts.scheme = sf.SCHEME_JACOBI
+    ours = _run_scene(sf, lib, scene, opts)
+    case = C.Case(scene.name, scene.config, scene.scalars, scene.vectors, scene.steps)
+    o = orc.Oracle(scene.config, scene.scalars, scene.vectors, precision=32, scheme=orc.JACOBI)
+    sf.scenes.run(o, scene)
+    ref = C.collect_oracle(o, orc, case)
+    err = errors(ours, ref, ORACLE_FLOOR)
+    assert max(err.values()) <= ORACLE_TOL, err
 
 
 def _batch_vs_single(sf, lib, scenes, options=None, **batch_kw):
