@@ -95,6 +95,9 @@ def parse():
     p.add_argument("--cap", type=int, default=100000, help="pressure-iteration cap of the residual-driven solve")
     p.add_argument("--variants", default="learned,plain,previous,rbgs")
     p.add_argument("--trial", type=int, default=CHECK_INTERVAL, help="learned start: sweeps of the trial against the previous pressure")
+    p.add_argument("--weights", default=str(ROOT / "stable-fluids_b200" / "weights" / "warmstart_128.npy"),
+                   help="trained warm-start parameters (stable-fluids_b200/train_warmstart.py); used when the file exists, unless --train-in-bench")
+    p.add_argument("--train-in-bench", action="store_true", help="train the network inside this run instead of loading --weights")
     p.add_argument("--train-size", type=int, default=128)
     p.add_argument("--train-scenes", type=int, default=6)
     p.add_argument("--train-steps", type=int, default=32, help="pairs per training scene")
@@ -271,6 +274,26 @@ def run_variant(sf, scene, variant, args, world, device, net=None):
         out["used_fallback"] = fallback
         out["trial_sweeps"] = args.trial
     return sim, out
+
+
+def load_network(sf, args, device):
+    """The warm-start network with the committed trained parameters
+    (stable-fluids_b200/train_warmstart.py wrote them and their protocol)."""
+    import hashlib
+
+    import numpy as np
+
+    params = np.load(args.weights)
+    net = sf.WarmStartNetwork(seed=0, device=device)
+    net.set_parameters(params)
+    info = {"source": os.path.relpath(args.weights, ROOT), "sha256": hashlib.sha256(np.ascontiguousarray(params, np.float32).tobytes()).hexdigest()[:16]}
+    try:
+        meta = json.loads(pathlib.Path(args.weights).with_suffix(".json").read_text())
+        info.update({"protocol": meta.get("protocol"), "target_rel_residual": meta.get("target_rel_residual"), "best_held_out_error": meta.get("best_held_out_error"),
+                     "sha256_matches_record": meta.get("sha256", "")[:16] == info["sha256"]})
+    except (OSError, ValueError):
+        pass
+    return net, info
 
 
 def train_network(sf, args, device):
@@ -718,7 +741,9 @@ def main():
 
     variants = [v for v in args.variants.split(",") if v]
     headline = "learned" if "learned" in variants else variants[0]  # profiling runs may leave the network out
-    net, train_info = train_network(sf, args, local) if any(v.startswith("learned") for v in variants) else (None, None)
+    net, train_info = None, None
+    if any(v.startswith("learned") for v in variants):
+        net, train_info = load_network(sf, args, local) if (os.path.exists(args.weights) and not args.train_in_bench) else train_network(sf, args, local)
 
     results = {}
     with Clocks(local, not args.no_clocks and rank == 0) as clk:

@@ -202,11 +202,19 @@ struct Cell {
     float tx, ty, tz;
 };
 
+// p / h, correctly rounded. When h is a power of two, 1 / h is exact and
+// p * (1 / h) is the same correctly rounded value without a division.
+__device__ __forceinline__ float div_h(float p, float h) {
+    const unsigned u = __float_as_uint(h);
+    const bool pow2 = (u & 0x007fffffu) == 0u && (u & 0x7f800000u) != 0u;  // normal, zero mantissa
+    return pow2 ? __fmul_rn(p, __frcp_rn(h)) : p / h;
+}
+
 // Grid coordinates of a world position: g = p / h - 0.5, floor, fraction.
 __device__ __forceinline__ Cell locate(float x, float y, float z, float h) {
-    const float gx = x / h - 0.5f;
-    const float gy = y / h - 0.5f;
-    const float gz = z / h - 0.5f;
+    const float gx = div_h(x, h) - 0.5f;
+    const float gy = div_h(y, h) - 0.5f;
+    const float gz = div_h(z, h) - 0.5f;
     Cell c;
     c.x0 = static_cast<int>(floorf(gx));
     c.y0 = static_cast<int>(floorf(gy));
@@ -257,11 +265,25 @@ __device__ __forceinline__ float3 sample_velocity3(const P* __restrict__ v, floa
                        trilerp(s[0].z, s[1].z, s[2].z, s[3].z, s[4].z, s[5].z, s[6].z, s[7].z, c));
 }
 
-// Midpoint RK2 back-trace in world units (backend-cuda.cu:295-300).
+// Midpoint RK2 back-trace in world units (backend-cuda.cu:295-300), from the
+// centre (x, y, z) of cell (cx, cy, cz).
 template <typename P>
-__device__ __forceinline__ float3 trace_rk2(float x, float y, float z, const P* __restrict__ v, float dt, const Dims& d, float h, const FlowBC& b) {
+__device__ __forceinline__ float3 trace_rk2(float x, float y, float z, int cx, int cy, int cz, const P* __restrict__ v, float dt, const Dims& d, float h, const FlowBC& b) {
+    // The first sample is at the cell's own centre. Where its grid position
+    // comes out exactly on the cell (all three fractions zero, as for a
+    // power-of-two h) every interpolation weight of the other corners is
+    // zero and the trilinear value is the cell's own velocity: read it
+    // directly. (It can differ from the interpolated value only in the sign
+    // of a zero, which x - (0.5 dt) v does not see.)
+    float3 v0;
+    const Cell c = locate(x, y, z, h);
+    if (c.tx == 0.0f && c.ty == 0.0f && c.tz == 0.0f && c.x0 == cx && c.y0 == cy && c.z0 == cz) {
+        const float4 q = ldg4(&v[lin(cx, cy, cz, d)]);
+        v0 = make_float3(q.x, q.y, q.z);
+    } else {
+        v0 = sample_velocity3(v, x, y, z, d, h, b);
+    }
     // x - (0.5 dt) v and x - dt v, each product and difference rounded once
-    const float3 v0 = sample_velocity3(v, x, y, z, d, h, b);
     const float half_dt = __fmul_rn(0.5f, dt);
     const float mx = __fmaf_rn(-half_dt, v0.x, x);
     const float my = __fmaf_rn(-half_dt, v0.y, y);

@@ -15,6 +15,7 @@
 #include "sf_batch.cuh"
 #include "sf_device.cuh"
 #include "sf_launch.h"
+#include "sf_stencil_tb.cuh"
 
 namespace sfb {
 
@@ -89,7 +90,7 @@ __device__ __forceinline__ void advect_velocity_block(uint3 blk, const P* __rest
     const float px = __fmul_rn(static_cast<float>(x) + 0.5f, h);
     const float py = __fmul_rn(static_cast<float>(y) + 0.5f, h);
     const float pz = __fmul_rn(static_cast<float>(z) + 0.5f, h);
-    const float3 t = trace_rk2(px, py, pz, v, dt, d, h, b);
+    const float3 t = trace_rk2(px, py, pz, x, y, z, v, dt, d, h, b);
     const float3 s = sample_velocity3(v, t.x, t.y, t.z, d, h, b);
     const size_t i = lin(x, y, z, d);
     ox[i] = from_f<T>(s.x);
@@ -109,7 +110,7 @@ __device__ __forceinline__ float sourced_scalar(const T* __restrict__ q, const f
         if (!scalar_resolve(x, y, z, d, b, value)) return value;
     }
     const size_t i = lin(x, y, z, d);
-    return ldg_f(&q[i]) + dt * __ldg(&src[i]);
+    return __fmaf_rn(dt, __ldg(&src[i]), ldg_f(&q[i]));  // rho + dt S, one rounding (backend-cuda.cu:326)
 }
 
 // Source injection fused into the advection gather (backend-cuda.cu:321-328
@@ -122,14 +123,25 @@ __device__ __forceinline__ void scalar_source_advect_block(uint3 blk, const P* _
     const float px = __fmul_rn(static_cast<float>(x) + 0.5f, h);
     const float py = __fmul_rn(static_cast<float>(y) + 0.5f, h);
     const float pz = __fmul_rn(static_cast<float>(z) + 0.5f, h);
-    float3 t = trace_rk2(px, py, pz, v, dt, d, h, fb);
+    float3 t = trace_rk2(px, py, pz, x, y, z, v, dt, d, h, fb);
     if (sb.periodic[0]) t.x = wrap_world(t.x, static_cast<float>(d.nx) * h);
     if (sb.periodic[1]) t.y = wrap_world(t.y, static_cast<float>(d.ny) * h);
     if (sb.periodic[2]) t.z = wrap_world(t.z, static_cast<float>(d.nz) * h);
     const Cell c = locate(t.x, t.y, t.z, h);
     float s[8];
+    if (c.x0 >= 0 && c.y0 >= 0 && c.z0 >= 0 && c.x0 + 1 < d.nx && c.y0 + 1 < d.ny && c.z0 + 1 < d.nz) {
+        // the whole 2x2x2 block is inside: no ghost rule applies
+        const size_t i = lin(c.x0, c.y0, c.z0, d);
+        const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, sb);
+        for (int k = 0; k < 8; ++k) {
+            const size_t j = i + static_cast<size_t>(k & 1) + ((k >> 1) & 1 ? sy : 0) + (k >> 2 ? sz : 0);
+            s[k] = __fmaf_rn(dt, __ldg(&src[j]), ldg_f(&q[j]));
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, sb);
+    }
     out[lin(x, y, z, d)] = from_f<T>(trilerp(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], c));
 }
 
@@ -138,7 +150,7 @@ __global__ void __launch_bounds__(256) k_scalar_source_advect(const P* __restric
 
 template <typename T>
 __global__ void k_scalar_source(T* __restrict__ q, const float* __restrict__ src, float dt, size_t n) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(to_f(q[i]) + dt * src[i]);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(__fmaf_rn(dt, src[i], to_f(q[i])));
 }
 
 // backend-cuda.cu:377-384
@@ -351,6 +363,61 @@ __device__ __forceinline__ void post_diagnostics_block(uint3 blk, float* __restr
 template <typename T>
 __global__ void __launch_bounds__(256) k_post_diagnostics(float* __restrict__ div, float* __restrict__ mag, const T* __restrict__ vx, const T* __restrict__ vy, const T* __restrict__ vz, Dims d, float h, FlowBC b) { post_diagnostics_block<T>(blockIdx, div, mag, vx, vy, vz, d, h, b); }
 
+// ------------------------------------- divergence / |u| on the z-march --
+// The same values as divergence_block / post_diagnostics_block for FP32
+// fields with nx % 4 == 0: a thread owns one float4 of a row and marches a z
+// chunk, keeping the z component's planes below / at / above in registers;
+// face ghosts come from the velocity components' GhostRules (copy for
+// outflow and tangential free slip, reflection about the wall velocity
+// otherwise -- load_velocity's rule for a face neighbour), periodic axes are
+// read wrapped. The rounding is written out: central differences, then
+// (dz * c) + ((dx * c) + (dy * c)) with the last two sums fused, and
+// |u| = sqrt(w w + (u u + v v)) with the same fusing -- the contraction the
+// reference's expressions take (backend-cuda.cu:391-395, 429-433).
+constexpr int kDivRows = 4;
+
+struct VelocityGhosts {
+    GhostRule g[3];  // components x, y, z
+};
+
+__device__ __forceinline__ float4 ld4f(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ghost4f(const GhostRule& g, int face, float4 s) {
+    return make_float4(tb::ghost(g, face, s.x), tb::ghost(g, face, s.y), tb::ghost(g, face, s.z), tb::ghost(g, face, s.w));
+}
+__device__ __forceinline__ float div_sum(float dx, float dy, float dz, float c) { return __fmaf_rn(dz, c, __fmaf_rn(dx, c, __fmul_rn(dy, c))); }
+__device__ __forceinline__ float magnitude(float u, float v, float w) { return __fsqrt_rn(__fmaf_rn(w, w, __fmaf_rn(u, u, __fmul_rn(v, v)))); }
+
+template <bool MAG>
+__global__ void __launch_bounds__(32 * kDivRows) k_divergence_vec4(float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, int z_chunk, Dims d, float inv_2h, VelocityGhosts gh) {
+    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kDivRows + threadIdx.y);
+    if (x0 >= d.nx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const int sy = d.nx, sz = d.nx * d.ny;
+    const GhostRule &gx = gh.g[0], &gy = gh.g[1], &gz = gh.g[2];
+    const bool px = gx.periodic[0] != 0, py = gy.periodic[1] != 0, pz = gz.periodic[2] != 0;
+    int i = x0 + sy * (y + d.ny * zb);
+    float4 zc = ld4f(vz + i);
+    float4 zlo = zb > 0 ? ld4f(vz + i - sz) : (pz ? ld4f(vz + i + (d.nz - 1) * sz) : ghost4f(gz, ZM, zc));
+    for (int z = zb; z < ze; ++z, i += sz) {
+        const float4 zhi = z + 1 < d.nz ? ld4f(vz + i + sz) : (pz ? ld4f(vz + i - (d.nz - 1) * sz) : ghost4f(gz, ZP, zc));
+        const float4 xc = ld4f(vx + i);
+        const float xl = x0 > 0 ? vx[i - 1] : (px ? vx[i + d.nx - 1] : tb::ghost(gx, XM, xc.x));
+        const float xr = x0 + 4 < d.nx ? vx[i + 4] : (px ? vx[i + 4 - d.nx] : tb::ghost(gx, XP, xc.w));
+        const float4 yc = ld4f(vy + i);
+        const float4 ylo = y > 0 ? ld4f(vy + i - sy) : (py ? ld4f(vy + i + (d.ny - 1) * sy) : ghost4f(gy, YM, yc));
+        const float4 yhi = y + 1 < d.ny ? ld4f(vy + i + sy) : (py ? ld4f(vy + i - (d.ny - 1) * sy) : ghost4f(gy, YP, yc));
+        float4 o;
+        o.x = div_sum(xc.y - xl, yhi.x - ylo.x, zhi.x - zlo.x, inv_2h);
+        o.y = div_sum(xc.z - xc.x, yhi.y - ylo.y, zhi.y - zlo.y, inv_2h);
+        o.z = div_sum(xc.w - xc.y, yhi.z - ylo.z, zhi.z - zlo.z, inv_2h);
+        o.w = div_sum(xr - xc.z, yhi.w - ylo.w, zhi.w - zlo.w, inv_2h);
+        *reinterpret_cast<float4*>(div + i) = o;
+        if constexpr (MAG) *reinterpret_cast<float4*>(mag + i) = make_float4(magnitude(xc.x, yc.x, zc.x), magnitude(xc.y, yc.y, zc.y), magnitude(xc.z, yc.z, zc.z), magnitude(xc.w, yc.w, zc.w));
+        zlo = zc;
+        zc = zhi;
+    }
+}
+
 // ------------------------------------------------------- work-table batch --
 // One launch per stage over every simulation of a batch (sf_batch.h); each
 // work item runs the single-simulation block body above.
@@ -530,12 +597,41 @@ cudaError_t launch_scale(void* data, float factor, size_t n, int bf16, cudaStrea
     return cudaGetLastError();
 }
 
+GhostRule make_ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb);
+
+// The z-marching divergence for FP32 fields whose rows are whole float4s:
+// false (nothing launched) when the grid or the pointers do not suit it.
+bool launch_divergence_vec4(float* div, float* mag, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, cudaStream_t s) {
+    const auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    const size_t cells = static_cast<size_t>(d.nx) * d.ny * d.nz;
+    if (d.nx % 4 != 0 || cells >= (1ull << 31) || !al(div) || !al(vx) || !al(vy) || !al(vz) || (mag != nullptr && !al(mag))) return false;
+    VelocityGhosts gh{};
+    for (int c = 0; c < 3; ++c) gh.g[c] = make_ghost_rule(KIND_VEL_X + c, b, ScalarBC{});
+    static int per_sm = [] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_divergence_vec4<true>, 32 * kDivRows, 0) != cudaSuccess || n < 1) n = 8;
+        return n;
+    }();
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int bx = (d.nx / 4 + 31) / 32, by = (d.ny + kDivRows - 1) / kDivRows;
+    long long chunks = static_cast<long long>(sms) * per_sm / (static_cast<long long>(bx) * by);  // one wave
+    if (chunks < 1) chunks = 1;
+    int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
+    if (z_chunk < 4) z_chunk = d.nz < 4 ? d.nz : 4;
+    const dim3 grid(static_cast<unsigned>(bx), static_cast<unsigned>(by), static_cast<unsigned>((d.nz + z_chunk - 1) / z_chunk));
+    const float inv_2h = 0.5f / h;
+    if (mag) k_divergence_vec4<true><<<grid, dim3(32, kDivRows), 0, s>>>(div, mag, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), z_chunk, d, inv_2h, gh);
+    else k_divergence_vec4<false><<<grid, dim3(32, kDivRows), 0, s>>>(div, nullptr, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), z_chunk, d, inv_2h, gh);
+    return true;
+}
+
 cudaError_t launch_divergence(float* div, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s) {
+    if (!bf16 && launch_divergence_vec4(div, nullptr, vx, vy, vz, d, h, b, s)) return cudaGetLastError();
     SFB_STORAGE(bf16, (k_divergence<float><<<cell_grid(d), cell_block(), 0, s>>>(div, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), d, h, b)),
                 (k_divergence<bf16_t><<<cell_grid(d), cell_block(), 0, s>>>(div, static_cast<const bf16_t*>(vx), static_cast<const bf16_t*>(vy), static_cast<const bf16_t*>(vz), d, h, b)));
     return cudaGetLastError();
 }
-
 cudaError_t launch_project(void* vx, void* vy, void* vz, void* packed, const float* p, const float* div, Dims d, float h, float h2, const FlowBC& b, DeviceStats* stats, int bf16, cudaStream_t s) {
     SFB_STORAGE(bf16, (k_project<float, float4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<float*>(vx), static_cast<float*>(vy), static_cast<float*>(vz), static_cast<float4*>(packed), p, div, d, h, h2, b, stats)),
                 (k_project<bf16_t, Bf16x4><<<cell_grid(d), cell_block(), 0, s>>>(static_cast<bf16_t*>(vx), static_cast<bf16_t*>(vy), static_cast<bf16_t*>(vz), static_cast<Bf16x4*>(packed), p, div, d, h, h2, b, stats)));
@@ -569,6 +665,7 @@ cudaError_t launch_warm_start_select(DeviceStats* learned, const DeviceStats* pl
 }
 
 cudaError_t launch_post_diagnostics(float* div, float* mag, const void* vx, const void* vy, const void* vz, Dims d, float h, const FlowBC& b, int bf16, cudaStream_t s) {
+    if (!bf16 && launch_divergence_vec4(div, mag, vx, vy, vz, d, h, b, s)) return cudaGetLastError();
     SFB_STORAGE(bf16, (k_post_diagnostics<float><<<cell_grid(d), cell_block(), 0, s>>>(div, mag, static_cast<const float*>(vx), static_cast<const float*>(vy), static_cast<const float*>(vz), d, h, b)),
                 (k_post_diagnostics<bf16_t><<<cell_grid(d), cell_block(), 0, s>>>(div, mag, static_cast<const bf16_t*>(vx), static_cast<const bf16_t*>(vy), static_cast<const bf16_t*>(vz), d, h, b)));
     return cudaGetLastError();
