@@ -170,8 +170,11 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_network_train_step(void*
  * runs warm_start_trial_iterations sweeps on it and on the previous
  * pressure, and continues from the one with the smaller residual
  * (used_fallback = 1 when that is the previous pressure); the sweeps of the
- * trial count towards the step's iterations. The network must outlive the
- * attachment and must not be used on another stream while the context steps. */
+ * trial count towards the step's iterations. Several contexts may share one
+ * network: each attached context predicts with activation buffers of its own
+ * (allocated here, freed when it detaches or is destroyed) and only reads the
+ * shared weights. The network must outlive the attachment, and must not be
+ * trained while an attached context steps. */
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* context, void* network);
 
 /* ---- Batched stepping (no counterpart in the reference) ----
@@ -187,9 +190,8 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_attach_network(void* con
  *    diffusion > 0, viscosity > 0, at most 4 force fields, nx % 4 == 0.
  *  - GRAPHS: the contexts' own step graphs as children of one CUDA graph; the
  *    simulations' kernels run concurrently. Any contexts except ones with a
- *    residual-driven solve (conditional graph nodes) and except two contexts
- *    attached to the same warm-start network (they would use its buffers at
- *    the same time).
+ *    residual-driven solve (conditional graph nodes); contexts attached to
+ *    one warm-start network share it (each has its own activation buffers).
  *
  * Both give the same bits as stepping each context alone. WORK_TABLE packs
  * the simulations into L2-sized groups and runs the groups on `chains`

@@ -329,9 +329,9 @@ struct Stages {
             const float h2c = (2.0f * h()) * (2.0f * h());
             ok(launch_restrict2(c.divergence, c.coarse_b, c.dims, c.stream));
             ok(launch_restrict2(c.pressure, c.coarse_p, c.dims, c.stream));
-            if (ok(net::predict(c.network, c.coarse_b, h2c, c.coarse_p, c.coarse_out, c.coarse_dims(), c.stream, &predicted), 0)) launches += predicted;
+            if (ok(net::predict(c.network, c.coarse_b, h2c, c.coarse_p, c.coarse_out, c.coarse_dims(), c.stream, &predicted, &c), 0)) launches += predicted;
             ok(launch_prolong_add(c.coarse_out, c.coarse_p, c.pressure, c.dims, c.stream));
-        } else if (ok(net::predict(c.network, c.divergence, h() * h(), c.pressure, c.pressure, c.dims, c.stream, &predicted), 0)) {
+        } else if (ok(net::predict(c.network, c.divergence, h() * h(), c.pressure, c.pressure, c.dims, c.stream, &predicted, &c), 0)) {
             launches += predicted;
         }
         if (trial > 0) {
@@ -648,6 +648,7 @@ StableFluidsResult stable_fluids_destroy_context_cuda(void* context) {
     if (context == nullptr) return STABLE_FLUIDS_RESULT_OK;
     auto* c = static_cast<Context*>(context);
     if (c->stream) cudaStreamSynchronize(c->stream);  // :685
+    if (c->network != nullptr) sfb::net::release(c->network, c);  // its inference buffers in the attached network
     delete c;
     return STABLE_FLUIDS_RESULT_OK;
 }
@@ -882,7 +883,7 @@ StableFluidsResult stable_fluids_b200_attach_network(void* context, void* networ
     auto* n = static_cast<sfb::net::Net*>(network);
     if (cudaStreamSynchronize(c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     // the network's buffers for this grid are allocated before the capture
-    if (n != nullptr && sfb::net::prepare(n, c.coarse_b != nullptr ? c.coarse_dims() : c.dims) != cudaSuccess) {
+    if (n != nullptr && sfb::net::prepare(n, c.coarse_b != nullptr ? c.coarse_dims() : c.dims, &c) != cudaSuccess) {
         cudaGetLastError();
         return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     }
@@ -893,6 +894,8 @@ StableFluidsResult stable_fluids_b200_attach_network(void* context, void* networ
         sfb::build_graph(c);  // put the previous step graph back
         return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     }
+    // the new step graph no longer uses the previous network's buffers for this context
+    if (previous != nullptr && previous != n) sfb::net::release(previous, &c);
     return STABLE_FLUIDS_RESULT_OK;
 }
 
@@ -1323,11 +1326,9 @@ cudaError_t build_work_table(Batch& b, bool autotune, const char* cache_path, in
 }
 
 cudaError_t build_child_graphs(Batch& b) {
-    // The children run concurrently: two contexts using one warm-start
-    // network would share its activation buffers at the same time.
-    for (size_t i = 0; i < b.contexts.size(); ++i)
-        for (size_t j = i + 1; j < b.contexts.size(); ++j)
-            if (b.contexts[i]->network != nullptr && b.contexts[i]->network == b.contexts[j]->network) return cudaErrorInvalidValue;
+    // The children run concurrently; contexts attached to one warm-start
+    // network each predict with activation buffers of their own and share
+    // its weights, which no step writes.
     cudaError_t e = cudaGraphCreate(&b.graph, 0);
     if (e != cudaSuccess) return e;
     for (Context* c : b.contexts) {

@@ -21,8 +21,10 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <random>
+#include <set>
 #include <vector>
 
 #include "sf_types.h"
@@ -52,6 +54,7 @@ constexpr int kCinReal[NLAYERS] = {2, 16, 16, 32, 32, 64, 96, 32, 48, 16, 16};
 constexpr int kCout[NLAYERS] = {16, 16, 32, 32, 64, 64, 32, 32, 16, 16, 16};
 
 struct Buffers {
+    const void* owner = nullptr;  // the context predicting with it (inference only), or null
     Dims d0{}, d1{}, d2{};
     size_t n0 = 0, n1 = 0, n2 = 0;
     void* mem = nullptr;
@@ -85,8 +88,12 @@ struct Net {
     __nv_bfloat16* w16t = nullptr;  // BF16 transposed, tap-flipped weights [tap][cin][cout] (data gradient)
     unsigned* error = nullptr;      // set by a convolution whose bounded wait gave up
     int adam_t = 0;
-    // One buffer set per grid size, kept until the network is destroyed so
-    // that step graphs holding their addresses stay valid.
+    // Buffer sets by grid size and owner, kept until the network is
+    // destroyed (or the owner releases them) so that step graphs holding
+    // their addresses stay valid: the network's own set per size (training
+    // and direct predictions, with the gradient buffers), and one
+    // inference-only set per attached context, so that contexts sharing the
+    // network can step at the same time.
     std::vector<std::unique_ptr<Buffers>> sets;
     Buffers* buf = nullptr;
 
@@ -242,14 +249,15 @@ Net* create_net(uint32_t seed) {
     return n.release();
 }
 
-cudaError_t ensure_buffers(Net* n, Dims d) {
+cudaError_t ensure_buffers(Net* n, Dims d, const void* owner = nullptr) {
     if (d.nx % 4 || d.ny % 4 || d.nz % 4 || d.nx < 4 || d.ny < 4 || d.nz < 4) return cudaErrorInvalidValue;
     for (auto& set : n->sets)
-        if (set->d0.nx == d.nx && set->d0.ny == d.ny && set->d0.nz == d.nz) {
+        if (set->owner == owner && set->d0.nx == d.nx && set->d0.ny == d.ny && set->d0.nz == d.nz) {
             n->buf = set.get();
             return cudaSuccess;
         }
     auto b = std::make_unique<Buffers>();
+    b->owner = owner;
     b->d0 = d;
     b->d1 = Dims{d.nx / 2, d.ny / 2, d.nz / 2, 0};
     b->d2 = Dims{d.nx / 4, d.ny / 4, d.nz / 4, 0};
@@ -277,6 +285,8 @@ cudaError_t ensure_buffers(Net* n, Dims d) {
     bf(&b->cat0, b->n0, 48);
     bf(&b->d0a, b->n0, 16);
     bf(&b->d0b, b->n0, 16);
+    const bool training = owner == nullptr;
+    if (training) {
     bf(&b->g16, b->n0, 16);
     bf(&b->gd0b, b->n0, 16);
     bf(&b->gd0a, b->n0, 16);
@@ -292,8 +302,9 @@ cudaError_t ensure_buffers(Net* n, Dims d) {
     bf(&b->gp0, b->n1, 16);
     bf(&b->ge0b, b->n0, 16);
     bf(&b->ge0a, b->n0, 16);
-    items.push_back({reinterpret_cast<void**>(&b->out), b->n0 * sizeof(float)});
     items.push_back({reinterpret_cast<void**>(&b->target), b->n0 * sizeof(float)});
+    }
+    items.push_back({reinterpret_cast<void**>(&b->out), b->n0 * sizeof(float)});
     items.push_back({reinterpret_cast<void**>(&b->sums), 2 * sizeof(double)});
     items.push_back({reinterpret_cast<void**>(&b->scale), sizeof(float)});
     size_t total = 0;
@@ -437,10 +448,35 @@ cudaError_t loss_and_gradients(Net* n, const float* b, float b_factor, const flo
 
 }  // namespace
 
-cudaError_t prepare(Net* n, Dims d) { return ensure_buffers(n, d); }
+cudaError_t prepare(Net* n, Dims d, const void* owner) { return ensure_buffers(n, d, owner); }
 
-cudaError_t predict(Net* n, const float* b, float b_factor, const float* p_prev, float* p0, Dims d, cudaStream_t s, int* launches) {
-    cudaError_t e = ensure_buffers(n, d);
+// Networks created and not yet destroyed: a context destroyed after the
+// network it was attached to must not touch it.
+std::mutex g_live_mu;
+std::set<const Net*> g_live;
+
+void register_live(const Net* n, bool live) {
+    std::lock_guard<std::mutex> lock(g_live_mu);
+    if (live) g_live.insert(n);
+    else g_live.erase(n);
+}
+
+void release(Net* n, const void* owner) {
+    if (n == nullptr || owner == nullptr) return;
+    std::lock_guard<std::mutex> lock(g_live_mu);
+    if (g_live.count(n) == 0) return;
+    for (auto it = n->sets.begin(); it != n->sets.end();) {
+        if ((*it)->owner == owner) {
+            if (n->buf == it->get()) n->buf = nullptr;
+            it = n->sets.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+cudaError_t predict(Net* n, const float* b, float b_factor, const float* p_prev, float* p0, Dims d, cudaStream_t s, int* launches, const void* owner) {
+    cudaError_t e = ensure_buffers(n, d, owner);
     if (e != cudaSuccess) return e;
     if ((e = forward(n, b, b_factor, p_prev, s)) != cudaSuccess) return e;
     k_unpack_output<<<blocks_for(n->buf->n0), 256, 0, s>>>(n->buf->out, p_prev, n->buf->scale, p0, n->buf->n0);
@@ -485,12 +521,14 @@ StableFluidsResult stable_fluids_b200_network_create(uint32_t seed, void** out_n
         cudaGetLastError();
         return STABLE_FLUIDS_RESULT_OUT_OF_MEMORY;
     }
+    sfb::net::register_live(n, true);
     *out_network = n;
     return STABLE_FLUIDS_RESULT_OK;
 }
 
 StableFluidsResult stable_fluids_b200_network_destroy(void* network) {
     if (network != nullptr) cudaDeviceSynchronize();
+    sfb::net::register_live(static_cast<Net*>(network), false);
     delete static_cast<Net*>(network);
     return STABLE_FLUIDS_RESULT_OK;
 }
@@ -511,7 +549,7 @@ StableFluidsResult stable_fluids_b200_network_set_parameters(void* network, cons
 StableFluidsResult stable_fluids_b200_network_predict(void* network, const float* divergence, const float* previous_pressure, int32_t nx, int32_t ny, int32_t nz, float cell_size, float* out_pressure, void* stream) {
     if (network == nullptr || divergence == nullptr || out_pressure == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     const sfb::Dims d{nx, ny, nz, 0};
-    return status(sfb::net::predict(static_cast<Net*>(network), divergence, cell_size * cell_size, previous_pressure, out_pressure, d, static_cast<cudaStream_t>(stream), nullptr));
+    return status(sfb::net::predict(static_cast<Net*>(network), divergence, cell_size * cell_size, previous_pressure, out_pressure, d, static_cast<cudaStream_t>(stream), nullptr, nullptr));
 }
 
 StableFluidsResult stable_fluids_b200_network_gradients(void* network, const float* divergence, const float* previous_pressure, const float* target_pressure, int32_t nx, int32_t ny, int32_t nz, float cell_size, double* out_loss, float* out_host_gradients, void* stream) {

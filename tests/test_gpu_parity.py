@@ -537,25 +537,37 @@ def test_bf16_storage_against_fp64_oracle(scheme, sf, lib, orc, cuda):
 
 
 @pytest.mark.gpu
-def test_batch_refuses_contexts_sharing_a_network(sf, lib, cuda):
-    """Two learned-start contexts attached to one warm-start network would use
-    its activation buffers concurrently inside a batch graph: refused; with a
-    network each they batch."""
-    scene = sf.scenes.plume("shared-net", (16, 16, 16), sources=[(8, 5, 8, 3.0, 10.0, 5.0)], diffuse_iterations=2, pressure_iterations=24)
+def test_batch_shares_one_network(sf, lib, cuda):
+    """Learned-start contexts of different sizes attached to one warm-start
+    network step together in a GRAPHS batch (each predicts with its own
+    activation buffers) and give the same bits as stepping each alone with
+    that network; destroying a context after the network is safe."""
+    scenes = [sf.scenes.plume(f"shared-net-{n}", (n, n, n), sources=[(n / 2, 5, n / 2, 3.0, 10.0, 5.0)], diffuse_iterations=2, pressure_iterations=24, steps=3) for n in (16, 16, 24)]
     opts = sf.default_options(lib)
     opts.scheme = sf.SCHEME_JACOBI
     opts.warm_start = sf.WARM_START_LEARNED
-    sims = [sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib, options=opts) for _ in range(2)]
-    with sf.WarmStartNetwork(seed=0, lib=lib) as net, sf.WarmStartNetwork(seed=1, lib=lib) as other:
-        for sim in sims:
-            net.attach(sim)
-        with pytest.raises(sf.StableFluidsError):
-            sf.Batch(sims)
-        other.attach(sims[1])
-        with sf.Batch(sims) as batch:
-            batch.step(2)
-        for sim in sims:
-            sf.WarmStartNetwork.detach(sim)
-    for sim in sims:
-        assert np.isfinite(sim.fetch(sf.VIEW_FLOW_PRESSURE)).all()
+    opts.compute_residual = 1
+    net = sf.WarmStartNetwork(seed=0, lib=lib)
+    single = []
+    for sc in scenes:
+        sim = sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib, options=opts)
+        net.attach(sim)
+        sf.scenes.run(sim, sc)
+        single.append((C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), sim.stats().rel_residual))
+        sim.close()
+    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib, options=opts) for sc in scenes]
+    for sim, sc in zip(sims, scenes):
+        net.attach(sim)
+        sf.scenes.apply_inputs(sim, sc, 0)
+    with sf.Batch(sims, mode=sf.BATCH_GRAPHS) as batch:
+        for k in range(scenes[0].steps):
+            if k == 1:
+                for sim, sc in zip(sims, scenes):
+                    sf.scenes.apply_inputs(sim, sc, 1)
+            batch.step(1)
+    for sim, sc, (ref, ref_res) in zip(sims, scenes, single):
+        assert_bit_equal(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), ref)
+        assert sim.stats().rel_residual == ref_res
+    net.close()
+    for sim in sims:  # after the network: nothing of it is touched
         sim.close()
