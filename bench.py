@@ -107,7 +107,7 @@ def parse():
     p.add_argument("--learning-rate", type=float, default=3e-4)
     p.add_argument("--e2e-steps", type=int, default=None, help="end-to-end timing through the C ABI: the first N of the device-timed steps (default: all K; 0: skip)")
     p.add_argument("--fixed-steps", type=int, default=20)
-    p.add_argument("--batch-steps", type=int, default=20, help="steps of the batched 64-simulation workload (0: skip)")
+    p.add_argument("--batch-steps", type=int, default=100, help="steps of the batched 64-simulation workload (0: skip)")
     p.add_argument("--bf16-size", type=int, default=384)
     p.add_argument("--bf16-steps", type=int, default=5, help="timed steps of the FP32-vs-BF16-storage comparison (0: skip)")
     p.add_argument("--scene-steps", type=int, default=10, help="steps of the viewer-scene force generator comparison (0: skip)")
@@ -434,7 +434,38 @@ def fixed_iterations(sf, lib, scene, steps, warmup, device, world):
     return {"steps_per_s": world * steps / t, "ms_per_step": 1000.0 * t / steps, "steps": steps, "pressure_iterations": scene.config.pressure_iterations, "scheme": "rbgs"}
 
 
-def batched(sf, lib, steps, warmup, count=64, mode=None):
+def l2_copy_bandwidth(device, mib=24, repeats=50):
+    """Bandwidth of a device copy whose source and destination (2 x `mib`
+    MiB) stay in L2: bytes read + written per second, CUDA events. The
+    denominator of the batched workload's L2 roofline."""
+    import torch
+
+    n = mib * 1024 * 1024 // 4
+    a = torch.rand(n, device=device)
+    b = torch.empty_like(a)
+    for _ in range(5):
+        b.copy_(a)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(repeats):
+        b.copy_(a)
+    end.record()
+    torch.cuda.synchronize()
+    return 2 * 4 * n * repeats / (start.elapsed_time(end) / 1000.0) / 1e9
+
+
+def batch_step_bytes(config):
+    """Algorithmic bytes of one step of a red-black simulation (the bench's
+    batched workload) per cell: 6 B per cell and colour launch (x of the
+    colour read and written, the other colour and b read once), force + pack
+    40, advection 28, scalar source + advection 28, divergence 16, projection
+    44, diagnostics 20, copies for the diffusion starts 4 x 8."""
+    sweeps = 2 * (4 * config.diffuse_iterations + config.pressure_iterations)
+    return 6 * sweeps + 40 + 28 + 28 + 16 + 44 + 20 + 32
+
+
+def batched(sf, lib, steps, warmup, count=64, mode=None, options=None, net=None, device=0):
     """Batched workload: `count` uneven plumes (sizes over {32..128}^3,
     config-0 coefficients, 20 diffusion / 40 red-black pressure iterations).
     mode: "work_table" (one persistent launch per stage over all
@@ -447,8 +478,10 @@ def batched(sf, lib, steps, warmup, count=64, mode=None):
     import torch
 
     scenes = sf.scenes.batch_scenes(count=count)
-    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib) for sc in scenes]
+    sims = [sf.Simulation(sc.config, sc.scalars, sc.vectors, lib=lib, options=options) for sc in scenes]
     for sim, sc in zip(sims, scenes):
+        if net is not None:
+            net.attach(sim)
         sf.scenes.apply_inputs(sim, sc, 0)
     cells = sum(sim.cells for sim in sims)
     batch, extra = None, {}
@@ -479,12 +512,22 @@ def batched(sf, lib, steps, warmup, count=64, mode=None):
         torch.cuda.synchronize()
         t = time.perf_counter() - t0
         timing = "host clock around the steps with a device synchronize on both sides (work spans many streams)"
+    residual = None
+    if options is not None and options.compute_residual:
+        r = sorted(sim.stats().rel_residual for sim in sims)
+        residual = {"min": r[0], "median": statistics.median(r), "max": r[-1]}
     if batch is not None:
         batch.close()
     for sim in sims:
         sim.close()
+    if residual is not None:
+        extra["rel_residual_per_sim"] = residual
+    if options is None or options.scheme == sf.SCHEME_RBGS:
+        extra["algorithmic_bytes_per_s"] = sum(sim.cells * batch_step_bytes(sc.config) for sim, sc in zip(sims, scenes)) * steps / t
     sizes = sorted({sc.config.nx for sc in scenes})
     label = {"work_table": "one persistent launch per stage over a work table of L2-sized groups of simulations, groups on 4 concurrent streams (autotuned z chunks)", "graphs": "one graph of the simulations' step graphs per batch step", None: "each context stepped on its own stream"}[mode]
+    if net is not None:
+        label += "; Jacobi from one shared learned warm start (trial of 16 sweeps against the previous pressure), config-0 iteration count"
     return {"cell_updates_per_s": cells * steps / t, "steps_per_s": steps / t, "sims": count, "cells": cells, "sizes": sizes, "steps": steps, "timing": timing, "mode": label, **extra}
 
 
@@ -788,8 +831,21 @@ def main():
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
     batch = None
     if args.batch_steps > 0:
-        batch = batched(sf, None, args.batch_steps, args.warmup, mode="work_table")
-        batch["graphs_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="graphs").items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "layout_create_s")}
+        rbgs = sf.default_options()
+        rbgs.compute_residual = 1
+        batch = batched(sf, None, args.batch_steps, args.warmup, mode="work_table", options=rbgs)
+        l2 = l2_copy_bandwidth(torch.device("cuda", local))
+        batch["roofline_l2"] = {"achieved_gbs": batch["algorithmic_bytes_per_s"] / 1e9, "peak_gbs": l2, "frac": batch["algorithmic_bytes_per_s"] / 1e9 / l2,
+                                "peak_source": "measured here: device copy of 2 x 24 MiB resident in L2"}
+        batch["graphs_layout"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="graphs", options=rbgs).items() if k in ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "layout_create_s", "rel_residual_per_sim")}
+        if net is not None:
+            learned_opts = solver_options(sf, "learned", 0.0, args.cap, args.trial)
+            learned_opts.compute_residual = 1
+            previous_opts = solver_options(sf, "previous", 0.0, args.cap, args.trial)
+            previous_opts.compute_residual = 1
+            keys = ("steps_per_s", "cell_updates_per_s", "kernels_per_step", "mode", "rel_residual_per_sim")
+            batch["shared_network"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="graphs", options=learned_opts, net=net).items() if k in keys}
+            batch["previous_start_same_iterations"] = {k: v for k, v in batched(sf, None, args.batch_steps, args.warmup, mode="graphs", options=previous_opts).items() if k in keys}
     mixed = bf16_storage(sf, args.bf16_size, args.bf16_steps, args.warmup, local) if args.bf16_steps > 0 else None
     viewer = scene_generator(sf, n, args.scene_steps, local) if args.scene_steps > 0 else None
     render = volume_render(sf, n, local, frames=args.render_frames) if args.render_frames > 0 else None
@@ -825,7 +881,10 @@ def main():
                        "e2e_steps_per_s": e2e["value"] if e2e else None, "jacobi_sweep_us": roofline["sweep_us"], "roofline_frac": roofline["frac"],
                        "network_ms": roofline_network["launch_ms"] if roofline_network else None,
                        "fixed_iterations_steps_per_s": fixed["steps_per_s"] if fixed else None,
-                       "batched_gcups": {"work_table": batch["cell_updates_per_s"] / 1e9, "graphs": batch["graphs_layout"]["cell_updates_per_s"] / 1e9} if batch else None,
+                       "batched_gcups": {"work_table": batch["cell_updates_per_s"] / 1e9, "graphs": batch["graphs_layout"]["cell_updates_per_s"] / 1e9,
+                                         "shared_network": batch["shared_network"]["cell_updates_per_s"] / 1e9 if "shared_network" in batch else None} if batch else None,
+                       "batched_l2_frac": batch["roofline_l2"]["frac"] if batch else None,
+                       "batched_rel_residual_median": {k: b["rel_residual_per_sim"]["median"] for k, b in (("work_table", batch), ("shared_network", batch.get("shared_network")), ("previous", batch.get("previous_start_same_iterations"))) if b} if batch else None,
                        "bf16": {k: mixed[k] for k in ("fp32_steps_per_s", "bf16_steps_per_s", "rel_l2_bf16_vs_fp32")} if mixed else None}
     if net is not None:
         net.close()

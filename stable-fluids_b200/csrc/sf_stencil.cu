@@ -602,8 +602,10 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
 constexpr int kWaveRows = 16;  // rows per CTA (one warp each), halo rows included
 
 // Stages per pass when the caller leaves it open: 4 for rows of 128 cells;
-// 3 for rows of 256 (at 4, a 256-cell row's register history no longer fits
-// the 128 registers a 512-thread CTA can give each thread).
+// 3 (at most) for rows of 256, whose shared-memory rings (4 input planes,
+// two per intermediate stage, K + 3 right-hand-side planes of 16 KB) fill
+// the 227 KB a CTA may use at K = 3, and whose register history no longer
+// fits the 128 registers a 512-thread CTA gives each thread at K = 4.
 int wave_default_stages(int v) { return v == 1 ? 4 : 3; }
 
 // Rows of 128 V cells: V, or 0 when the grid does not suit the kernel.
@@ -649,6 +651,7 @@ cudaError_t run_wave(const StencilArgs& a, cudaStream_t s) {
     int per = wave_default_stages(V);
     if (a.per_pass >= 2) per = RB ? 2 * a.per_pass : a.per_pass;
     if (per > 4) per = 4;
+    if (V == 2 && per > 3) per = 3;  // 256-cell rows: 3 stages fill the shared memory
     if (RB) per = per < 2 ? 2 : (per & ~1);  // whole iterations per pass
     if (stages == 0) {
         if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
@@ -680,7 +683,8 @@ cudaError_t run_wave(const StencilArgs& a, cudaStream_t s) {
         w.out_scale = (i == passes - 1) ? a.out_scale : 1.0f;
         // kernels with a halo of K = 2 or 4 (red-black) and 3 or 4 (Jacobi)
         // stages; every pass of the solve uses the one sized for `per`
-        if constexpr (RB) e = per == 2 ? launch_wave_pass<KIND, RB, 2, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
+        if constexpr (V == 2) e = RB ? launch_wave_pass<KIND, RB, 2, V>(w, sms, s) : launch_wave_pass<KIND, RB, 3, V>(w, sms, s);
+        else if constexpr (RB) e = per == 2 ? launch_wave_pass<KIND, RB, 2, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
         else e = per <= 3 ? launch_wave_pass<KIND, RB, 3, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
         if (e != cudaSuccess) return e;
         if (a.launches) *a.launches += 1;

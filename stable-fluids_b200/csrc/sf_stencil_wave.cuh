@@ -12,14 +12,15 @@
 //     stage), written one time step earlier by the neighbouring warps;
 //   - z neighbours: the lane's own registers -- stage s-1's planes q-1 and q
 //     carried from earlier time steps, and plane q+1 produced by stage s-1
-//     in this time step (stage 1 reads planes q-1 and q of the input from
-//     its three-plane shared ring, and plane q+1 is the input plane t just
-//     loaded).
+//     in this time step (stage 1 reads planes q and q+1 of the input from
+//     the input ring and keeps plane q-1 in registers).
 // Stage 0 is the input: plane t of the iterate and of the right-hand side,
-// loaded from HBM once per pass and kept in shared memory (the right-hand
-// side in a ring of K+1 planes, since stage s reads it at time q + s).
-// Every shared-memory value read in a time step was written in an earlier
-// one, so one barrier per time step orders everything.
+// read from HBM once per pass by asynchronous copies (cp.async, 16 bytes per
+// lane, cached in L2 only) straight into shared memory two time steps ahead
+// of use: a ring of 4 input planes (t-1, t, and t+1, t+2 in flight) and one
+// of K+3 right-hand-side planes (stage s reads plane q at time q + s). Every
+// shared-memory value read in a time step was written -- or its copy waited
+// for -- in an earlier one, so one barrier per time step orders everything.
 //
 // Each stage shrinks the rows whose values are exact by one at each side of
 // the tile, and the planes by one at each end of the chunk: the tile carries
@@ -64,19 +65,23 @@ struct WaveArgs {
     GhostRule g;
 };
 
-// Shared memory of one CTA: the input ring of 3 planes (stage 0: planes
-// t-2, t-1, t), K-1 two-slot rings (stage s's output, s = 1..K-1), then the
-// right-hand-side ring of K + 1 planes; a plane holds the CTA's R rows of nx
-// floats.
+// Shared memory of one CTA: the input ring of 4 planes, K-1 two-slot rings
+// (stage s's output, s = 1..K-1), then the right-hand-side ring of K + 3
+// planes; a plane holds the CTA's R rows of nx floats.
 template <int K, int V, int R>
 struct WaveLayout {
     static constexpr int NX = 128 * V;
     static constexpr int PLANE = R * NX;
-    static constexpr int IN_PLANES = 3;
+    static constexpr int IN_PLANES = 4;
     static constexpr int RING_PLANES = IN_PLANES + 2 * (K - 1);
-    static constexpr int RHS_PLANES = K + 1;
+    static constexpr int RHS_PLANES = K + 3;
     static constexpr size_t bytes = static_cast<size_t>(RING_PLANES + RHS_PLANES) * PLANE * sizeof(float);
 };
+
+// 16-byte asynchronous copy global -> shared, L2 only; zero-fills when !valid.
+__device__ __forceinline__ void cp_async16(float4* dst, const float* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(tb::smem_addr(dst)), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
 
 __device__ __forceinline__ float4 ghost4v(const GhostRule& g, int face, float4 s) {
     return make_float4(tb::ghost(g, face, s.x), tb::ghost(g, face, s.y), tb::ghost(g, face, s.z), tb::ghost(g, face, s.w));
@@ -102,9 +107,10 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
     constexpr int ROW4 = L::NX / 4;  // float4 per row
     static_assert(R > 2 * K, "tile rows must exceed the halo");
     extern __shared__ __align__(16) float4 sm4[];
-    float4* const in_ring = sm4;                                // [3][R][ROW4]
+    float4* const in_ring = sm4;                                // [4][R][ROW4]
     float4* const rings = sm4 + L::IN_PLANES * PLANE / 4;       // [K-1][2][R][ROW4]: stage s's output at s-1
-    float4* const rhs_ring = sm4 + L::RING_PLANES * PLANE / 4;  // [K+1][R][ROW4]
+    float4* const rhs_ring = sm4 + L::RING_PLANES * PLANE / 4;  // [K+3][R][ROW4]
+    constexpr int RS = L::RHS_PLANES;
 
     const Dims d = a.d;
     const GhostRule& g = a.g;
@@ -135,42 +141,45 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
     // plane index of unwrapped z, or -1 outside a non-periodic axis
     const auto plane_of = [&](int z) { return pz ? wrap_index(z, d.nz) : (static_cast<unsigned>(z) < static_cast<unsigned>(d.nz) ? z : -1); };
 
-    // index s (2..K): stage s-1's planes q and q-1 for stage s
+    // index s (2..K): stage s-1's planes q and q-1 for stage s; below[1]:
+    // input plane q-1 of stage 1
     float4 cur[K + 1][V], below[K + 1][V];
 #pragma unroll
     for (int s = 0; s <= K; ++s)
 #pragma unroll
         for (int j = 0; j < V; ++j) cur[s][j] = below[s][j] = make_float4(0.f, 0.f, 0.f, 0.f);
 
-    float4 xin[V], rin[V];
-    const auto fetch = [&](int t) {
-        const int pl = (t <= z1 - 1 + K) ? plane_of(t) : -1;
-#pragma unroll
-        for (int j = 0; j < V; ++j) {
-            xin[j] = rin[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (live && pl >= 0) {
-                const size_t i = static_cast<size_t>(pl) * sz + row_off + 128 * j + 4 * lane;
-                if (a.src != nullptr) xin[j] = __ldg(reinterpret_cast<const float4*>(a.src + i));
-                rin[j] = __ldg(reinterpret_cast<const float4*>(a.rhs + i));
-            }
-        }
-    };
-    fetch(t_begin);
-
-    for (int t = t_begin; t <= t_end; ++t) {
-        // stage 0: plane t into the input ring and the right-hand-side ring
-        float4 above[V];
-        {
-            float4* r0 = in_ring + (wrap_index(t, 3) * R + row) * ROW4;
-            float4* rr = rhs_ring + (wrap_index(t, K + 1) * R + row) * ROW4;
+    // copies of input plane t (x and rhs) into their ring slots, one commit
+    // group per time step (empty past the chunk's last plane)
+    const auto issue = [&](int t) {
+        const int pl = (t <= t_end) ? plane_of(t) : -1;
+        if (pl >= 0) {
+            float4* xs = in_ring + (wrap_index(t, 4) * R + row) * ROW4;
+            float4* rs = rhs_ring + (wrap_index(t, RS) * R + row) * ROW4;
+            const size_t i0 = static_cast<size_t>(pl) * sz + row_off + 4 * lane;
 #pragma unroll
             for (int j = 0; j < V; ++j) {
-                above[j] = xin[j];
-                r0[32 * j + lane] = xin[j];
-                rr[32 * j + lane] = rin[j];
+                const size_t i = i0 + 128 * j;
+                cp_async16(xs + 32 * j + lane, live && a.src != nullptr ? a.src + i : a.rhs, live && a.src != nullptr);
+                cp_async16(rs + 32 * j + lane, live ? a.rhs + i : a.rhs, live);
             }
         }
-        if (t < t_end) fetch(t + 1);
+        tb::cp_async_commit();
+    };
+    issue(t_begin);
+    issue(t_begin + 1);
+    tb::cp_async_wait<1>();
+    __syncthreads();
+
+    for (int t = t_begin; t <= t_end; ++t) {
+        issue(t + 2);  // its slots held planes t - 2 (input) and t - K - 1 (rhs), last read at t - 1
+        // stage 1's newest plane: the input plane t
+        float4 above[V];
+        {
+            const float4* r0 = in_ring + (wrap_index(t, 4) * R + row) * ROW4;
+#pragma unroll
+            for (int j = 0; j < V; ++j) above[j] = r0[32 * j + lane];
+        }
 
 #pragma unroll
         for (int s = 1; s <= K; ++s) {
@@ -179,16 +188,17 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
             const int pq = plane_of(q);
             const bool active = pq >= 0 && q >= z0 - K + s && q <= z1 - 1 + K - s && live && row >= s && row < R - s;  // warp-uniform
             const bool to_ring = s < k_run, to_dst = s == k_run && out_row && q >= z0 && q < z1;
-            const float4* ring_in = s == 1 ? in_ring + wrap_index(q, 3) * R * ROW4 : rings + (((s - 2) * 2 + (q & 1)) * R) * ROW4;
-            const float4* rhs_in = rhs_ring + (wrap_index(q, K + 1) * R + row) * ROW4;
+            const float4* ring_in = s == 1 ? in_ring + wrap_index(q, 4) * R * ROW4 : rings + (((s - 2) * 2 + (q & 1)) * R) * ROW4;
+            const float4* rhs_in = rhs_ring + (wrap_index(q, RS) * R + row) * ROW4;
             float4* ring_out = rings + (((s - 1) * 2 + (q & 1)) * R + row) * ROW4;
             const bool even = RB ? (((gy + pq + ((a.parity0 + s - 1) & 1)) & 1) == 0) : true;
             float lw[V], rx[V];
             float4 cs[V];  // stage s-1's plane q, this lane's cells
+#pragma unroll
+            for (int j = 0; j < V; ++j) cs[j] = s == 1 ? ring_in[row * ROW4 + 32 * j + lane] : cur[s][j];
             if (active) {
 #pragma unroll
                 for (int j = 0; j < V; ++j) {
-                    cs[j] = s == 1 ? ring_in[row * ROW4 + 32 * j + lane] : cur[s][j];
                     lw[j] = __shfl_sync(0xffffffffu, cs[j].w, (lane + 31) & 31);
                     rx[j] = __shfl_sync(0xffffffffu, cs[j].x, (lane + 1) & 31);
                 }
@@ -201,7 +211,7 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
                     const float4 c = cs[j];
                     const float4 ym = face_ylo ? ghost4v(g, YM, c) : ring_in[(row - 1) * ROW4 + 32 * j + lane];
                     const float4 yp = face_yhi ? ghost4v(g, YP, c) : ring_in[(row + 1) * ROW4 + 32 * j + lane];
-                    const float4 zb = (!pz && pq == 0) ? ghost4v(g, ZM, c) : (s == 1 ? in_ring[(wrap_index(q - 1, 3) * R + row) * ROW4 + 32 * j + lane] : below[s][j]);
+                    const float4 zb = (!pz && pq == 0) ? ghost4v(g, ZM, c) : below[s][j];
                     const float4 za = (!pz && pq == d.nz - 1) ? ghost4v(g, ZP, c) : above[j];
                     const float4 r = rhs_in[32 * j + lane];
                     float left = lane == 0 ? lw[(j + V - 1) % V] : lw[j];
@@ -226,15 +236,19 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
                         *reinterpret_cast<float4*>(a.dst + static_cast<size_t>(pq) * sz + row_off + 128 * j + 4 * lane) = w;
                     }
                 }
-                if (s > 1) {
+                if (s == 1) {
+                    below[1][j] = cs[j];
+                } else {
                     below[s][j] = cur[s][j];
                     cur[s][j] = above[j];
                 }
                 above[j] = o;  // stage s+1's newest plane
             }
         }
+        tb::cp_async_wait<1>();  // this thread's copies of plane t + 1 have landed
         __syncthreads();
     }
+    tb::cp_async_wait<0>();
 }
 
 }  // namespace wave
