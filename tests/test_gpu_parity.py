@@ -567,7 +567,7 @@ def test_batch_shares_one_network(sf, lib, cuda):
             batch.step(1)
     for sim, sc, (ref, ref_res) in zip(sims, scenes, single):
         assert_bit_equal(C.collect_outputs(sim, sf, C.Case(sc.name, sc.config, sc.scalars, sc.vectors, sc.steps)), ref)
-        assert sim.stats().rel_residual == ref_res
+        assert sim.stats().rel_residual == pytest.approx(ref_res, rel=1e-9)  # FP64 sums by atomics: order varies
     net.close()
     for sim in sims:  # after the network: nothing of it is touched
         sim.close()
