@@ -192,6 +192,8 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
             const float4* rhs_in = rhs_ring + (wrap_index(q, RS) * R + row) * ROW4;
             float4* ring_out = rings + (((s - 1) * 2 + (q & 1)) * R + row) * ROW4;
             const bool even = RB ? (((gy + pq + ((a.parity0 + s - 1) & 1)) & 1) == 0) : true;
+            const bool zlo = !pz && pq == 0, zhi = !pz && pq == d.nz - 1;
+            const bool edge = face_ylo || face_yhi || zlo || zhi;
             float lw[V], rx[V];
             float4 cs[V];  // stage s-1's plane q, this lane's cells
 #pragma unroll
@@ -209,15 +211,25 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
                 float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (active) {
                     const float4 c = cs[j];
-                    const float4 ym = face_ylo ? ghost4v(g, YM, c) : ring_in[(row - 1) * ROW4 + 32 * j + lane];
-                    const float4 yp = face_yhi ? ghost4v(g, YP, c) : ring_in[(row + 1) * ROW4 + 32 * j + lane];
-                    const float4 zb = (!pz && pq == 0) ? ghost4v(g, ZM, c) : below[s][j];
-                    const float4 za = (!pz && pq == d.nz - 1) ? ghost4v(g, ZP, c) : above[j];
+                    float4 ym, yp, zb, za;
+                    if (!edge) {  // interior rows and planes: no ghost (warp-uniform)
+                        ym = ring_in[(row - 1) * ROW4 + 32 * j + lane];
+                        yp = ring_in[(row + 1) * ROW4 + 32 * j + lane];
+                        zb = below[s][j];
+                        za = above[j];
+                    } else {
+                        ym = face_ylo ? ghost4v(g, YM, c) : ring_in[(row - 1) * ROW4 + 32 * j + lane];
+                        yp = face_yhi ? ghost4v(g, YP, c) : ring_in[(row + 1) * ROW4 + 32 * j + lane];
+                        zb = zlo ? ghost4v(g, ZM, c) : below[s][j];
+                        za = zhi ? ghost4v(g, ZP, c) : above[j];
+                    }
                     const float4 r = rhs_in[32 * j + lane];
                     float left = lane == 0 ? lw[(j + V - 1) % V] : lw[j];
                     float right = lane == 31 ? rx[(j + 1) % V] : rx[j];
-                    if (!px && lane == 0 && j == 0) left = tb::ghost(g, XM, c.x);
-                    if (!px && lane == 31 && j == V - 1) right = tb::ghost(g, XP, c.w);
+                    if (!px) {  // x faces: the row's first and last cell (lanes 0 and 31)
+                        if (j == 0 && lane == 0) left = tb::ghost(g, XM, c.x);
+                        if (j == V - 1 && lane == 31) right = tb::ghost(g, XP, c.w);
+                    }
                     const float n0 = left + c.y + ym.x + yp.x + zb.x + za.x;
                     const float n1 = c.x + c.z + ym.y + yp.y + zb.y + za.y;
                     const float n2 = c.y + c.w + ym.z + yp.z + zb.z + za.z;
