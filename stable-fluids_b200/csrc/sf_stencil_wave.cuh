@@ -138,8 +138,14 @@ __global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
     const double recip = tb::recip64(divisor);
     const float inv = jacobi_inverse(KIND, a.coef);
 
-    // plane index of unwrapped z, or -1 outside a non-periodic axis
-    const auto plane_of = [&](int z) { return pz ? wrap_index(z, d.nz) : (static_cast<unsigned>(z) < static_cast<unsigned>(d.nz) ? z : -1); };
+    // plane index of unwrapped z (z0 - 2K <= z <= z1 - 1 + K: a few
+    // additions wrap it), or -1 outside a non-periodic axis
+    const auto plane_of = [&](int z) {
+        if (!pz) return static_cast<unsigned>(z) < static_cast<unsigned>(d.nz) ? z : -1;
+        while (z < 0) z += d.nz;
+        while (z >= d.nz) z -= d.nz;
+        return z;
+    };
 
     // index s (2..K): stage s-1's planes q and q-1 for stage s; below[1]:
     // input plane q-1 of stage 1
