@@ -601,17 +601,19 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
 // 128 or 256 cells.
 constexpr int kWaveRows = 16;  // rows per CTA (one warp each), halo rows included
 
-// Stages per pass when the caller leaves it open: 4 for rows of 128 cells;
-// 3 (at most) for rows of 256, whose shared-memory rings (4 input planes,
+// Stages per pass: 4 for rows of 128 cells; for rows of 256, 3 (Jacobi) or
+// 2 (one red-black iteration): their shared-memory rings (4 input planes,
 // two per intermediate stage, K + 3 right-hand-side planes of 16 KB) fill
-// the 227 KB a CTA may use at K = 3, and whose register history no longer
-// fits the 128 registers a 512-thread CTA gives each thread at K = 4.
-int wave_default_stages(int v) { return v == 1 ? 4 : 3; }
+// the 227 KB a CTA may use, and their register history the 128 registers a
+// 512-thread CTA gives each thread.
+template <int V, bool RB>
+constexpr int wave_stages() { return V == 1 ? 4 : (RB ? 2 : 3); }
 
 // Rows of 128 V cells: V, or 0 when the grid does not suit the kernel.
 int wave_width(const StencilArgs& a) {
     if (a.bf16 || a.scratch == nullptr || !vec_ok(a)) return 0;
     if (a.dims.nx != 128 && a.dims.nx != 256) return 0;
+    if (a.dims.nz <= 8) return 0;  // the chunk halo wraps a periodic z axis at most once
     if (a.scheme == SCHEME_RBGS) {
         // an odd periodic size breaks the red-black colouring across the wrap
         const int kind = a.kind;
@@ -642,55 +644,63 @@ cudaError_t launch_wave_pass(const wave::WaveArgs& w, int sms, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The solve as whole passes of K stages, the remainder as single sweeps
+// (Jacobi) or single colour launches (red-black) of the same arithmetic.
 template <int KIND, bool RB, int V>
 cudaError_t run_wave(const StencilArgs& a, cudaStream_t s) {
+    constexpr int K = wave_stages<V, RB>();
     const Dims& d = a.dims;
     const size_t bytes = static_cast<size_t>(d.nx) * d.ny * d.nz * sizeof(float);
-    cudaError_t e = cudaSuccess;
     const int stages = RB ? 2 * a.iterations : a.iterations;
-    int per = wave_default_stages(V);
-    if (a.per_pass >= 2) per = RB ? 2 * a.per_pass : a.per_pass;
-    if (per > 4) per = 4;
-    if (V == 2 && per > 3) per = 3;  // 256-cell rows: 3 stages fill the shared memory
-    if (RB) per = per < 2 ? 2 : (per & ~1);  // whole iterations per pass
-    if (stages == 0) {
-        if (a.init == INIT_ZERO) e = cudaMemsetAsync(a.x, 0, bytes, s);
-        else if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(a.x, a.b, bytes, cudaMemcpyDeviceToDevice, s);
-        if (e != cudaSuccess || a.out_scale == 1.0f) return e;
-        k_scale_field<<<148u * 32u, 256, 0, s>>>(a.x, a.out_scale, static_cast<size_t>(d.nx) * d.ny * d.nz);
-        if (a.launches) *a.launches += 1;
-        return cudaGetLastError();
-    }
+    const int passes = stages / K;
+    if (passes == 0) return run_simple<KIND, float>(a, s);
+    const int rest = stages - passes * K;  // Jacobi sweeps / red-black iterations x 2 left over
+    cudaError_t e = cudaSuccess;
+    const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
     wave::WaveArgs w{};
     w.rhs = a.b;
     w.coef = a.coef;
     w.d = d;
-    w.g = ghost_rule(KIND, a.flow, a.scalar);
-    w.parity0 = 0;
+    w.g = g;
     int sms = 148, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int passes = (stages + per - 1) / per;
+    // out-of-place units (Jacobi: the passes and the single sweeps; red-black:
+    // the passes, the colour launches then run in place on x), the last in x
+    const int units = RB ? passes : passes + rest;
     const float* src = a.init == INIT_ZERO ? nullptr : (a.init == INIT_FROM_B ? a.b : a.x);
-    for (int i = 0; i < passes; ++i) {
-        float* dst = ((passes - 1 - i) % 2 == 0) ? a.x : a.scratch;
-        if (src == dst) {  // warm start from x with an odd pass count: move it aside
+    const bool scale_in_pass = rest == 0;
+    const auto vs = vec_shape(d, k_jacobi_vec4<KIND>);
+    for (int u = 0; u < units; ++u) {
+        float* dst = ((units - 1 - u) % 2 == 0) ? a.x : a.scratch;
+        if (src == dst) {  // warm start from x with an odd unit count: move it aside
             if ((e = cudaMemcpyAsync(a.scratch, a.x, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
             src = a.scratch;
         }
-        w.src = src;
-        w.dst = dst;
-        w.k_run = (i == passes - 1) ? stages - per * (passes - 1) : per;
-        w.out_scale = (i == passes - 1) ? a.out_scale : 1.0f;
-        // kernels with a halo of K = 2 or 4 (red-black) and 3 or 4 (Jacobi)
-        // stages; every pass of the solve uses the one sized for `per`
-        if constexpr (V == 2) e = RB ? launch_wave_pass<KIND, RB, 2, V>(w, sms, s) : launch_wave_pass<KIND, RB, 3, V>(w, sms, s);
-        else if constexpr (RB) e = per == 2 ? launch_wave_pass<KIND, RB, 2, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
-        else e = per <= 3 ? launch_wave_pass<KIND, RB, 3, V>(w, sms, s) : launch_wave_pass<KIND, RB, 4, V>(w, sms, s);
-        if (e != cudaSuccess) return e;
+        if (u < passes) {
+            w.src = src;
+            w.dst = dst;
+            w.out_scale = (u == passes - 1 && scale_in_pass) ? a.out_scale : 1.0f;
+            if ((e = launch_wave_pass<KIND, RB, K, V>(w, sms, s)) != cudaSuccess) return e;
+        } else {
+            k_jacobi_vec4<KIND><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
+        }
         if (a.launches) *a.launches += 1;
         src = dst;
     }
-    return cudaSuccess;
+    if (RB && rest > 0) {
+        const auto rs = vec_shape(d, k_rbgs_vec4<KIND>);
+        for (int it = 0; it < rest / 2; ++it)
+            for (int parity = 0; parity < 2; ++parity) k_rbgs_vec4<KIND><<<rs.grid, dim3(32, kVecRows), 0, s>>>(a.x, a.b, a.coef, parity, rs.z_chunk, d, g);
+        if (a.launches) *a.launches += rest;
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (!scale_in_pass && a.out_scale != 1.0f) {
+        const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
+        k_scale_field<<<148u * 32u, 256, 0, s>>>(a.x, a.out_scale, n);
+        if (a.launches) *a.launches += 1;
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 template <int KIND>

@@ -34,7 +34,7 @@
 //   JACOBI : every stage is a Jacobi sweep with this library's Jacobi
 //            arithmetic (jacobi_update); k_jacobi_vec4 computes the same, so
 //            K sweeps here equal K single sweeps bit for bit;
-//   RBGS   : stage s updates the cells of colour (parity0 + s - 1) & 1 and
+//   RBGS   : stage s updates the cells of colour (s - 1) & 1 (red first) and
 //            copies the others, with the reference's exact division
 //            (backend-cuda.cu:354-375, 398-407): 2 stages = one red-black
 //            iteration, bit-equal to the reference's two launches.
@@ -58,8 +58,6 @@ struct WaveArgs {
     float* dst;        // iterate after the pass (never src)
     float coef;        // alpha or h^2
     float out_scale;   // multiplies the pass's result (dissipation; 1 = none)
-    int k_run;         // stages run in this pass (1..K)
-    int parity0;       // red-black: colour of stage 1
     int z_chunk;       // output planes per CTA
     Dims d;
     GhostRule g;
@@ -100,171 +98,196 @@ __device__ __forceinline__ float jacobi_update(float nb, float rhs, float coef, 
     return __fmul_rn(num, inv);
 }
 
+// One time step t of the pipeline (PH = t mod 3 selects which of the three
+// history buffers of each stage holds planes q-1, q and q+1, so the history
+// moves up a plane by renaming, without register copies).
 template <int KIND, bool RB, int K, int V, int R>
-__global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
+struct WaveCta {
     using L = WaveLayout<K, V, R>;
-    constexpr int PLANE = L::PLANE;
-    constexpr int ROW4 = L::NX / 4;  // float4 per row
-    static_assert(R > 2 * K, "tile rows must exceed the halo");
-    extern __shared__ __align__(16) float4 sm4[];
-    float4* const in_ring = sm4;                                // [4][R][ROW4]
-    float4* const rings = sm4 + L::IN_PLANES * PLANE / 4;       // [K-1][2][R][ROW4]: stage s's output at s-1
-    float4* const rhs_ring = sm4 + L::RING_PLANES * PLANE / 4;  // [K+3][R][ROW4]
-    constexpr int RS = L::RHS_PLANES;
+    static constexpr int ROW4 = L::NX / 4;
+    static constexpr int PLANE4 = L::PLANE / 4;
+    static constexpr int RS = L::RHS_PLANES;
+    static constexpr int TY = R - 2 * K;
 
-    const Dims d = a.d;
-    const GhostRule& g = a.g;
-    const int lane = static_cast<int>(threadIdx.x & 31), row = static_cast<int>(threadIdx.x >> 5);
-    constexpr int TY = R - 2 * K;
-    const int gy_u = static_cast<int>(blockIdx.x) * TY - K + row;  // unwrapped global row
-    const bool px = g.periodic[0] != 0, py = g.periodic[1] != 0, pz = g.periodic[2] != 0;
-    int gy = gy_u;
-    bool live = true;
-    if (gy < 0 || gy >= d.ny) {
-        if (py) gy = wrap_index(gy, d.ny);
-        else live = false;
-    }
-    const bool out_row = row >= K && row < R - K && gy_u < d.ny;
-    const bool face_ylo = !py && gy_u == 0, face_yhi = !py && gy_u == d.ny - 1;
-    const int z0 = static_cast<int>(blockIdx.y) * a.z_chunk;
-    if (z0 >= d.nz) return;  // CTA-uniform, before any barrier
-    const int z1 = min(z0 + a.z_chunk, d.nz);
-    const int k_run = a.k_run;
-    const int t_begin = pz ? z0 - K : max(z0 - K, 0);
-    const int t_end = z1 - 1 + k_run;
-    const size_t sz = static_cast<size_t>(d.nx) * d.ny;
-    const size_t row_off = static_cast<size_t>(gy) * d.nx;
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * a.coef;
-    const double recip = tb::recip64(divisor);
-    const float inv = jacobi_inverse(KIND, a.coef);
+    const WaveArgs& a;
+    float4* in_ring;   // [4][R][ROW4]
+    float4* rings;     // [K-1][2][R][ROW4], stage r's output at r-1
+    float4* rhs_ring;  // [RS][R][ROW4]
+    int lane, row, gy, z0, z1, nz;
+    bool live, out_row, face_ylo, face_yhi, px, pz;
+    bool xm_lane, xp_lane;          // this lane holds the row's first / last cell on a non-periodic x axis
+    float4 h[K + 1][3][V];          // stage s's input planes (stage s-1's outputs; s = 1: the input)
+    size_t row_off, sz;
+    float inv;                      // Jacobi: RN(1 / divisor)
+    float divisor;
+    double recip;
 
-    // plane index of unwrapped z (z0 - 2K <= z <= z1 - 1 + K: a few
-    // additions wrap it), or -1 outside a non-periodic axis
-    const auto plane_of = [&](int z) {
-        if (!pz) return static_cast<unsigned>(z) < static_cast<unsigned>(d.nz) ? z : -1;
-        while (z < 0) z += d.nz;
-        while (z >= d.nz) z -= d.nz;
-        return z;
-    };
+    __device__ __forceinline__ int wrap_z(int z) const { return z < 0 ? z + nz : (z >= nz ? z - nz : z); }
 
-    // index s (2..K): stage s-1's planes q and q-1 for stage s; below[1]:
-    // input plane q-1 of stage 1
-    float4 cur[K + 1][V], below[K + 1][V];
+    // the copies of input plane p (x and rhs) into ring slots p & 3 and ps
+    __device__ __forceinline__ void issue(int p, int ps, int t_end) {
+        if (p <= t_end) {
+            const int pl = pz ? wrap_z(p) : p;
+            if (pz || static_cast<unsigned>(pl) < static_cast<unsigned>(nz)) {
+                const size_t i = static_cast<size_t>(pl) * sz + row_off + 4 * lane;
+                float4* xs = in_ring + ((p & 3) * R + row) * ROW4 + lane;
+                float4* rs = rhs_ring + (ps * R + row) * ROW4 + lane;
+                const bool xv = live && a.src != nullptr;
 #pragma unroll
-    for (int s = 0; s <= K; ++s)
-#pragma unroll
-        for (int j = 0; j < V; ++j) cur[s][j] = below[s][j] = make_float4(0.f, 0.f, 0.f, 0.f);
-
-    // copies of input plane t (x and rhs) into their ring slots, one commit
-    // group per time step (empty past the chunk's last plane)
-    const auto issue = [&](int t) {
-        const int pl = (t <= t_end) ? plane_of(t) : -1;
-        if (pl >= 0) {
-            float4* xs = in_ring + (wrap_index(t, 4) * R + row) * ROW4;
-            float4* rs = rhs_ring + (wrap_index(t, RS) * R + row) * ROW4;
-            const size_t i0 = static_cast<size_t>(pl) * sz + row_off + 4 * lane;
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                const size_t i = i0 + 128 * j;
-                cp_async16(xs + 32 * j + lane, live && a.src != nullptr ? a.src + i : a.rhs, live && a.src != nullptr);
-                cp_async16(rs + 32 * j + lane, live ? a.rhs + i : a.rhs, live);
+                for (int j = 0; j < V; ++j) {
+                    cp_async16(xs + 32 * j, xv ? a.src + i + 128 * j : a.rhs, xv);
+                    cp_async16(rs + 32 * j, live ? a.rhs + i + 128 * j : a.rhs, live);
+                }
             }
         }
         tb::cp_async_commit();
-    };
-    issue(t_begin);
-    issue(t_begin + 1);
-    tb::cp_async_wait<1>();
-    __syncthreads();
+    }
 
-    for (int t = t_begin; t <= t_end; ++t) {
-        issue(t + 2);  // its slots held planes t - 2 (input) and t - K - 1 (rhs), last read at t - 1
-        // stage 1's newest plane: the input plane t
-        float4 above[V];
-        {
-            const float4* r0 = in_ring + (wrap_index(t, 4) * R + row) * ROW4;
+    template <int PH>
+    __device__ __forceinline__ void step(int t, int rt, int t_end) {
+        constexpr int B = PH % 3, C = (PH + 1) % 3, N = (PH + 2) % 3;  // planes q-1, q, q+1 of each stage
+        issue(t + 2, rt + 2 >= RS ? rt + 2 - RS : rt + 2, t_end);  // its slots held planes t - 2 and t - K - 1, last read at t - 1
+        {   // stage 1's newest plane: the input plane t
+            const float4* r0 = in_ring + ((t & 3) * R + row) * ROW4 + lane;
 #pragma unroll
-            for (int j = 0; j < V; ++j) above[j] = r0[32 * j + lane];
+            for (int j = 0; j < V; ++j) h[1][N][j] = r0[32 * j];
         }
-
 #pragma unroll
         for (int s = 1; s <= K; ++s) {
-            if (s > k_run) break;
             const int q = t - s;
-            const int pq = plane_of(q);
-            const bool active = pq >= 0 && q >= z0 - K + s && q <= z1 - 1 + K - s && live && row >= s && row < R - s;  // warp-uniform
-            const bool to_ring = s < k_run, to_dst = s == k_run && out_row && q >= z0 && q < z1;
-            const float4* ring_in = s == 1 ? in_ring + wrap_index(q, 4) * R * ROW4 : rings + (((s - 2) * 2 + (q & 1)) * R) * ROW4;
-            const float4* rhs_in = rhs_ring + (wrap_index(q, RS) * R + row) * ROW4;
-            float4* ring_out = rings + (((s - 1) * 2 + (q & 1)) * R + row) * ROW4;
-            const bool even = RB ? (((gy + pq + ((a.parity0 + s - 1) & 1)) & 1) == 0) : true;
-            const bool zlo = !pz && pq == 0, zhi = !pz && pq == d.nz - 1;
-            const bool edge = face_ylo || face_yhi || zlo || zhi;
-            float lw[V], rx[V];
-            float4 cs[V];  // stage s-1's plane q, this lane's cells
-#pragma unroll
-            for (int j = 0; j < V; ++j) cs[j] = s == 1 ? ring_in[row * ROW4 + 32 * j + lane] : cur[s][j];
-            if (active) {
+            const bool in_planes = q >= z0 - K + s && q <= z1 - 1 + K - s && (pz || static_cast<unsigned>(q) < static_cast<unsigned>(nz));
+            float4 o[V];
+            if (in_planes && live && row >= s && row < R - s) {  // warp-uniform
+                const int pq = pz ? wrap_z(q) : q;
+                const float4* ring_in = s == 1 ? in_ring + ((q & 3) * R) * ROW4 + lane : rings + (((s - 2) * 2 + (q & 1)) * R) * ROW4 + lane;
+                const int rslot = rt - s < 0 ? rt - s + RS : rt - s;
+                const float4* rhs_in = rhs_ring + (rslot * R + row) * ROW4 + lane;
+                const bool zlo = !pz && pq == 0, zhi = !pz && pq == nz - 1;
+                const bool edge = face_ylo || face_yhi || zlo || zhi;
+                float lw[V], rx[V];
 #pragma unroll
                 for (int j = 0; j < V; ++j) {
-                    lw[j] = __shfl_sync(0xffffffffu, cs[j].w, (lane + 31) & 31);
-                    rx[j] = __shfl_sync(0xffffffffu, cs[j].x, (lane + 1) & 31);
+                    lw[j] = __shfl_sync(0xffffffffu, h[s][C][j].w, (lane + 31) & 31);
+                    rx[j] = __shfl_sync(0xffffffffu, h[s][C][j].x, (lane + 1) & 31);
                 }
-            }
-            // one float4 segment at a time: update, store, move up one plane
+                const bool even = RB ? (((gy + pq + ((s - 1) & 1)) & 1) == 0) : true;
 #pragma unroll
-            for (int j = 0; j < V; ++j) {
-                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (active) {
-                    const float4 c = cs[j];
-                    float4 ym, yp, zb, za;
-                    if (!edge) {  // interior rows and planes: no ghost (warp-uniform)
-                        ym = ring_in[(row - 1) * ROW4 + 32 * j + lane];
-                        yp = ring_in[(row + 1) * ROW4 + 32 * j + lane];
-                        zb = below[s][j];
-                        za = above[j];
-                    } else {
-                        ym = face_ylo ? ghost4v(g, YM, c) : ring_in[(row - 1) * ROW4 + 32 * j + lane];
-                        yp = face_yhi ? ghost4v(g, YP, c) : ring_in[(row + 1) * ROW4 + 32 * j + lane];
-                        zb = zlo ? ghost4v(g, ZM, c) : below[s][j];
-                        za = zhi ? ghost4v(g, ZP, c) : above[j];
+                for (int j = 0; j < V; ++j) {
+                    const float4 c = h[s][C][j];
+                    float4 ym = ring_in[(row - 1) * ROW4 + 32 * j];
+                    float4 yp = ring_in[(row + 1) * ROW4 + 32 * j];
+                    float4 zb = h[s][B][j], za = h[s][N][j];
+                    if (edge) {  // a face row or plane (warp-uniform, rare)
+                        if (face_ylo) ym = ghost4v(a.g, YM, c);
+                        if (face_yhi) yp = ghost4v(a.g, YP, c);
+                        if (zlo) zb = ghost4v(a.g, ZM, c);
+                        if (zhi) za = ghost4v(a.g, ZP, c);
                     }
-                    const float4 r = rhs_in[32 * j + lane];
+                    const float4 r = rhs_in[32 * j];
                     float left = lane == 0 ? lw[(j + V - 1) % V] : lw[j];
                     float right = lane == 31 ? rx[(j + 1) % V] : rx[j];
-                    if (!px) {  // x faces: the row's first and last cell (lanes 0 and 31)
-                        if (j == 0 && lane == 0) left = tb::ghost(g, XM, c.x);
-                        if (j == V - 1 && lane == 31) right = tb::ghost(g, XP, c.w);
-                    }
+                    if (j == 0) left = xm_lane ? tb::ghost(a.g, XM, c.x) : left;
+                    if (j == V - 1) right = xp_lane ? tb::ghost(a.g, XP, c.w) : right;
                     const float n0 = left + c.y + ym.x + yp.x + zb.x + za.x;
                     const float n1 = c.x + c.z + ym.y + yp.y + zb.y + za.y;
                     const float n2 = c.y + c.w + ym.z + yp.z + zb.z + za.z;
                     const float n3 = c.z + right + ym.w + yp.w + zb.w + za.w;
                     if constexpr (RB) {
-                        if (even) o = make_float4(tb::divide(tb::numerator<KIND>(n0, r.x, a.coef), divisor, recip), c.y, tb::divide(tb::numerator<KIND>(n2, r.z, a.coef), divisor, recip), c.w);
-                        else o = make_float4(c.x, tb::divide(tb::numerator<KIND>(n1, r.y, a.coef), divisor, recip), c.z, tb::divide(tb::numerator<KIND>(n3, r.w, a.coef), divisor, recip));
+                        if (even) o[j] = make_float4(tb::divide(tb::numerator<KIND>(n0, r.x, a.coef), divisor, recip), c.y, tb::divide(tb::numerator<KIND>(n2, r.z, a.coef), divisor, recip), c.w);
+                        else o[j] = make_float4(c.x, tb::divide(tb::numerator<KIND>(n1, r.y, a.coef), divisor, recip), c.z, tb::divide(tb::numerator<KIND>(n3, r.w, a.coef), divisor, recip));
                     } else {
-                        o = make_float4(jacobi_update<KIND>(n0, r.x, a.coef, inv), jacobi_update<KIND>(n1, r.y, a.coef, inv), jacobi_update<KIND>(n2, r.z, a.coef, inv), jacobi_update<KIND>(n3, r.w, a.coef, inv));
-                    }
-                    if (to_ring) {
-                        ring_out[32 * j + lane] = o;
-                    } else if (to_dst) {
-                        float4 w = o;
-                        if (a.out_scale != 1.0f) w = make_float4(__fmul_rn(w.x, a.out_scale), __fmul_rn(w.y, a.out_scale), __fmul_rn(w.z, a.out_scale), __fmul_rn(w.w, a.out_scale));
-                        *reinterpret_cast<float4*>(a.dst + static_cast<size_t>(pq) * sz + row_off + 128 * j + 4 * lane) = w;
+                        o[j] = make_float4(jacobi_update<KIND>(n0, r.x, a.coef, inv), jacobi_update<KIND>(n1, r.y, a.coef, inv), jacobi_update<KIND>(n2, r.z, a.coef, inv), jacobi_update<KIND>(n3, r.w, a.coef, inv));
                     }
                 }
-                if (s == 1) {
-                    below[1][j] = cs[j];
-                } else {
-                    below[s][j] = cur[s][j];
-                    cur[s][j] = above[j];
+                if (s < K) {
+                    float4* ring_out = rings + (((s - 1) * 2 + (q & 1)) * R + row) * ROW4 + lane;
+#pragma unroll
+                    for (int j = 0; j < V; ++j) ring_out[32 * j] = o[j];
+                } else if (out_row && q >= z0 && q < z1) {
+                    float* out = a.dst + static_cast<size_t>(pq) * sz + row_off + 4 * lane;
+                    const float f = a.out_scale;  // 1 leaves every value unchanged
+#pragma unroll
+                    for (int j = 0; j < V; ++j) *reinterpret_cast<float4*>(out + 128 * j) = make_float4(__fmul_rn(o[j].x, f), __fmul_rn(o[j].y, f), __fmul_rn(o[j].z, f), __fmul_rn(o[j].w, f));
                 }
-                above[j] = o;  // stage s+1's newest plane
+            } else {
+#pragma unroll
+                for (int j = 0; j < V; ++j) o[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            if (s < K) {
+#pragma unroll
+                for (int j = 0; j < V; ++j) h[s + 1][N][j] = o[j];  // stage s+1's newest plane
             }
         }
         tb::cp_async_wait<1>();  // this thread's copies of plane t + 1 have landed
         __syncthreads();
+    }
+};
+
+template <int KIND, bool RB, int K, int V, int R>
+__global__ void __launch_bounds__(32 * R, 1) k_wave(WaveArgs a) {
+    using W = WaveCta<KIND, RB, K, V, R>;
+    using L = typename W::L;
+    static_assert(R > 2 * K, "tile rows must exceed the halo");
+    extern __shared__ __align__(16) float4 sm4[];
+    W w{a};
+    w.in_ring = sm4;
+    w.rings = sm4 + L::IN_PLANES * W::PLANE4;
+    w.rhs_ring = sm4 + L::RING_PLANES * W::PLANE4;
+    const Dims d = a.d;
+    w.lane = static_cast<int>(threadIdx.x & 31);
+    w.row = static_cast<int>(threadIdx.x >> 5);
+    w.nz = d.nz;
+    const int gy_u = static_cast<int>(blockIdx.x) * W::TY - K + w.row;  // unwrapped global row
+    w.px = a.g.periodic[0] != 0;
+    const bool py = a.g.periodic[1] != 0;
+    w.pz = a.g.periodic[2] != 0;
+    w.gy = gy_u;
+    w.live = true;
+    if (gy_u < 0 || gy_u >= d.ny) {
+        if (py) w.gy = wrap_index(gy_u, d.ny);
+        else w.live = false;
+    }
+    w.out_row = w.row >= K && w.row < R - K && gy_u < d.ny;
+    w.face_ylo = !py && gy_u == 0;
+    w.face_yhi = !py && gy_u == d.ny - 1;
+    w.xm_lane = !w.px && w.lane == 0;
+    w.xp_lane = !w.px && w.lane == 31;
+    w.z0 = static_cast<int>(blockIdx.y) * a.z_chunk;
+    if (w.z0 >= d.nz) return;  // CTA-uniform, before any barrier
+    w.z1 = min(w.z0 + a.z_chunk, d.nz);
+    w.sz = static_cast<size_t>(d.nx) * d.ny;
+    w.row_off = static_cast<size_t>(w.gy) * d.nx;
+    w.divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * a.coef;
+    w.recip = tb::recip64(w.divisor);
+    w.inv = jacobi_inverse(KIND, a.coef);
+#pragma unroll
+    for (int s = 0; s <= K; ++s)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int j = 0; j < V; ++j) w.h[s][k][j] = make_float4(0.f, 0.f, 0.f, 0.f);
+
+    const int t_begin = w.pz ? w.z0 - K : max(w.z0 - K, 0);
+    const int t_end = w.z1 - 1 + K;
+    // rhs ring slot of plane t_begin (the ring holds plane p at p mod RS)
+    int rt = t_begin % W::RS;
+    if (rt < 0) rt += W::RS;
+    w.issue(t_begin, rt, t_end);
+    w.issue(t_begin + 1, rt + 1 >= W::RS ? rt + 1 - W::RS : rt + 1, t_end);
+    tb::cp_async_wait<1>();
+    __syncthreads();
+    // three time steps per iteration: planes t, t+1, t+2 in phases 0, 1, 2 of
+    // the history buffers (CTA-uniform bounds)
+    const auto next = [](int r) { return r + 1 == W::RS ? 0 : r + 1; };
+    for (int t = t_begin; t <= t_end; t += 3) {
+        w.template step<0>(t, rt, t_end);
+        rt = next(rt);
+        if (t + 1 > t_end) break;
+        w.template step<1>(t + 1, rt, t_end);
+        rt = next(rt);
+        if (t + 2 > t_end) break;
+        w.template step<2>(t + 2, rt, t_end);
+        rt = next(rt);
     }
     tb::cp_async_wait<0>();
 }
