@@ -109,7 +109,7 @@ def parse():
     p.add_argument("--fixed-steps", type=int, default=20)
     p.add_argument("--batch-steps", type=int, default=100, help="steps of the batched 64-simulation workload (0: skip)")
     p.add_argument("--bf16-size", type=int, default=384)
-    p.add_argument("--bf16-steps", type=int, default=5, help="timed steps of the FP32-vs-BF16-storage comparison (0: skip)")
+    p.add_argument("--bf16-steps", type=int, default=50, help="timed steps of the FP32-vs-BF16-storage comparison (config 3: 50; 0: skip)")
     p.add_argument("--scene-steps", type=int, default=10, help="steps of the viewer-scene force generator comparison (0: skip)")
     p.add_argument("--render-frames", type=int, default=5, help="frames of the headless volume rendering measurement (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
