@@ -79,6 +79,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "steps/s at 256³: learned-warm-start vs plain Jacobi at equal ‖∇·u‖ residual"
 CHECK_INTERVAL = 16
 CALIBRATION = ROOT / "bench_calibration.json"
+ITERATIONS_PER_PASS = 0  # set from --iterations-per-pass
 # DRAM bytes (read + write) of one Jacobi pressure pass from an ncu capture,
 # by grid size; filled from profiles/ once captured.
 PASS_TRAFFIC: dict[int, tuple[float, str]] = {}
@@ -116,10 +117,13 @@ def parse():
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--fixed-pressure-iterations", type=int, default=0,
                    help="profiling: run the variants with this fixed sweep count instead of the residual-driven solve (ncu cannot see kernels inside conditional graph nodes)")
+    p.add_argument("--iterations-per-pass", type=int, default=0, help="stencil iterations per HBM pass of the variants' solves (0, 1: one launch per sweep; >= 2: z-wavefront passes)")
     p.add_argument("--calibrate", action="store_true", help="write bench_calibration.json: the red-black iterations each step of the scene needs (this library's rbgs variant), for --impl reference")
     p.add_argument("--calibrate-steps", type=int, default=40)
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
+    global ITERATIONS_PER_PASS
+    ITERATIONS_PER_PASS = a.iterations_per_pass
     return a
 
 
@@ -219,6 +223,7 @@ def solver_options(sf, variant, tol, cap, trial):
     o.residual_check_interval = CHECK_INTERVAL
     o.max_pressure_iterations = cap
     o.warm_start_trial_iterations = trial
+    o.iterations_per_pass = ITERATIONS_PER_PASS
     return o
 
 
