@@ -540,18 +540,28 @@ def bf16_storage(sf, n, steps, warmup, device):
     """Mixed precision at n^3 (the config-1 plume generator, 20 diffusion /
     80 red-black pressure iterations): steps/s with FP32 and with BF16
     storage of velocity and density, and the BF16 run's relative L2
-    difference from the FP32 run per field after warmup + steps steps."""
+    difference from the FP32 run per field after warmup + steps steps --
+    beside the difference a one-ulp change of one force value makes to the
+    FP32 run over the same steps (the flow's own amplification of a
+    rounding-sized difference)."""
     import numpy as np
     import torch
 
     scene = sf.scenes.config1(n=n)
     out = {"grid": [n, n, n], "steps": steps, "warmup": warmup}
     fields = {}
-    for name, storage in (("fp32", sf.STORAGE_FP32), ("bf16", sf.STORAGE_BF16)):
+    for name, storage in (("fp32", sf.STORAGE_FP32), ("bf16", sf.STORAGE_BF16), ("fp32_perturbed", sf.STORAGE_FP32)):
         opts = sf.default_options()
         opts.storage = storage
         sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, options=opts, device=device)
         sf.scenes.apply_inputs(sim, scene, 0)
+        if name == "fp32_perturbed":
+            # the same FP32 run with the force's largest component one ulp larger:
+            # how far the flow itself carries a rounding-sized difference
+            fx, fy, fz = (np.array(f, np.float32, copy=True) for f in scene.force)
+            k = np.unravel_index(np.argmax(np.abs(fy)), fy.shape)
+            fy[k] = np.nextafter(fy[k], np.float32(np.inf))
+            sim.set_vector(sim.vector_handles[0], fx, fy, fz)
         sim.step(warmup)
         torch.cuda.synchronize()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -559,12 +569,15 @@ def bf16_storage(sf, n, steps, warmup, device):
         sim.step(steps)
         end.record(sim.stream)
         torch.cuda.synchronize()
-        out[f"{name}_steps_per_s"] = steps / (start.elapsed_time(end) / 1000.0)
-        out[f"{name}_device_bytes"] = sim.info().device_bytes
+        if name != "fp32_perturbed":
+            out[f"{name}_steps_per_s"] = steps / (start.elapsed_time(end) / 1000.0)
+            out[f"{name}_device_bytes"] = sim.info().device_bytes
         fields[name] = {"density": sim.fetch(sf.VIEW_SCALAR_FIELD_DATA, sim.scalar_handles[0]), "velocity": np.stack(sim.fetch(sf.VIEW_FLOW_VELOCITY)), "pressure": sim.fetch(sf.VIEW_FLOW_PRESSURE)}
         sim.close()
     out["speedup"] = out["bf16_steps_per_s"] / out["fp32_steps_per_s"]
-    out["rel_l2_bf16_vs_fp32"] = {k: float(np.linalg.norm(fields["bf16"][k].astype(np.float64) - fields["fp32"][k]) / max(np.linalg.norm(fields["fp32"][k].astype(np.float64)), 1e-30)) for k in fields["fp32"]}
+    rel = lambda a, b: float(np.linalg.norm(a.astype(np.float64) - b) / max(np.linalg.norm(b.astype(np.float64)), 1e-30))
+    out["rel_l2_bf16_vs_fp32"] = {k: rel(fields["bf16"][k], fields["fp32"][k]) for k in fields["fp32"]}
+    out["rel_l2_fp32_one_ulp_force_vs_fp32"] = {k: rel(fields["fp32_perturbed"][k], fields["fp32"][k]) for k in fields["fp32"]}
     return out
 
 
@@ -816,7 +829,8 @@ def main():
     bytes_per_launch = 12 * cells
     achieved = bytes_per_launch / launch_s / 1e9
     traffic = PASS_TRAFFIC.get(n)
-    roofline = {"bound": "hbm", "kernel": f"k_wave (Jacobi pressure pass, {sweeps_per_launch:g} sweeps per launch)", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
+    kernel_name = "k_jacobi_vec4 (Jacobi pressure sweep)" if sweeps_per_launch == 1 else f"k_wave (Jacobi pressure pass, {sweeps_per_launch:g} sweeps per launch)"
+    roofline = {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic[0] if traffic else None, "traffic_source": traffic[1] if traffic else None, "bytes_per_launch": bytes_per_launch, "launch_us": launch_s * 1e6,
                 "sweeps_per_launch": sweeps_per_launch, "sweep_us": launch_s * 1e6 / sweeps_per_launch,
                 "unit_of_work": f"one pass of {sweeps_per_launch:g} Jacobi sweeps over {n}^3 cells: read p + rhs, write p = 12 B/cell"}
@@ -875,7 +889,7 @@ def main():
     # that it survives in a record that keeps only the end of the line.
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume)", "config": config,
-            "variants": results, "training": train_info, "batched": batch, "viewer_scene_forces": viewer, "volume_render": render, "roofline_network": roofline_network,
+            "variants": results, "training": train_info, "batched": batch, "bf16_storage": mixed, "viewer_scene_forces": viewer, "volume_render": render, "roofline_network": roofline_network,
             "e2e": e2e, "roofline": roofline, "cell_updates_per_s": value * cells, "gpu_launches": learned["gpu_launches"]}
     c = clk.summary() if rank == 0 else None
     if c:
@@ -890,7 +904,7 @@ def main():
                                          "shared_network": batch["shared_network"]["cell_updates_per_s"] / 1e9 if "shared_network" in batch else None} if batch else None,
                        "batched_l2_frac": batch["roofline_l2"]["frac"] if batch else None,
                        "batched_rel_residual_median": {k: b["rel_residual_per_sim"]["median"] for k, b in (("work_table", batch), ("shared_network", batch.get("shared_network")), ("previous", batch.get("previous_start_same_iterations"))) if b} if batch else None,
-                       "bf16": {k: mixed[k] for k in ("fp32_steps_per_s", "bf16_steps_per_s", "rel_l2_bf16_vs_fp32")} if mixed else None}
+                       "bf16": {k: mixed[k] for k in ("fp32_steps_per_s", "bf16_steps_per_s", "rel_l2_bf16_vs_fp32", "rel_l2_fp32_one_ulp_force_vs_fp32")} if mixed else None}
     if net is not None:
         net.close()
     if rank == 0:
