@@ -387,13 +387,14 @@ __device__ __forceinline__ float4 ghost4f(const GhostRule& g, int face, float4 s
 __device__ __forceinline__ float div_sum(float dx, float dy, float dz, float c) { return __fmaf_rn(dz, c, __fmaf_rn(dx, c, __fmul_rn(dy, c))); }
 __device__ __forceinline__ float magnitude(float u, float v, float w) { return __fsqrt_rn(__fmaf_rn(w, w, __fmaf_rn(u, u, __fmul_rn(v, v)))); }
 
+// Block `blk` of the launch (blockIdx for one simulation, the work item's
+// block in a batch).
 template <bool MAG>
-__global__ void __launch_bounds__(32 * kDivRows) k_divergence_vec4(float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, int z_chunk, Dims d, float inv_2h, VelocityGhosts gh) {
-    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kDivRows + threadIdx.y);
+__device__ __forceinline__ void divergence_vec4_block(uint3 blk, float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, int z_chunk, const Dims& d, float inv_2h, const GhostRule& gx, const GhostRule& gy, const GhostRule& gz) {
+    const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kDivRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const int zb = static_cast<int>(blk.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const int sy = d.nx, sz = d.nx * d.ny;
-    const GhostRule &gx = gh.g[0], &gy = gh.g[1], &gz = gh.g[2];
     const bool px = gx.periodic[0] != 0, py = gy.periodic[1] != 0, pz = gz.periodic[2] != 0;
     int i = x0 + sy * (y + d.ny * zb);
     float4 zc = ld4f(vz + i);
@@ -416,6 +417,11 @@ __global__ void __launch_bounds__(32 * kDivRows) k_divergence_vec4(float* __rest
         zlo = zc;
         zc = zhi;
     }
+}
+
+template <bool MAG>
+__global__ void __launch_bounds__(32 * kDivRows) k_divergence_vec4(float* __restrict__ div, float* __restrict__ mag, const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz, int z_chunk, Dims d, float inv_2h, VelocityGhosts gh) {
+    divergence_vec4_block<MAG>(blockIdx, div, mag, vx, vy, vz, z_chunk, d, inv_2h, gh.g[0], gh.g[1], gh.g[2]);
 }
 
 // ------------------------------------------------------- work-table batch --
@@ -464,12 +470,17 @@ __global__ void __launch_bounds__(256) k_batch_scalar_source_advect(BatchTable t
     }
 }
 
-__global__ void __launch_bounds__(256) k_batch_divergence(BatchTable t) {
-    const uint32_t* first = t.first[SHAPE_CELL];
-    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
+// Divergence (MAG: and |u|) of every simulation with the z-marching body
+// (the work table's fields are 256-byte aligned with nx % 4 == 0); each
+// simulation's blocks use its sweep z chunk.
+template <bool MAG>
+__global__ void __launch_bounds__(32 * kDivRows) k_batch_divergence(BatchTable t) {
+    const uint32_t* first = t.first[SHAPE_VEC];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_VEC]; w += gridDim.x) {
         const int si = batch_sim(first, t.nsims, w);
         const BatchSim& m = t.sims[si];
-        divergence_block<float>(cell_block_of(w - first[si], m.d), m.divergence, m.vel[0], m.vel[1], m.vel[2], m.d, m.h, m.flow);
+        const uint3 blk = batch_block(w - first[si], static_cast<uint32_t>((m.d.nx / 4 + 31) / 32), static_cast<uint32_t>((m.d.ny + kDivRows - 1) / kDivRows));
+        divergence_vec4_block<MAG>(blk, m.divergence, m.magnitude, m.vel[0], m.vel[1], m.vel[2], m.z_chunk, m.d, 0.5f / m.h, m.ghost[KIND_VEL_X], m.ghost[KIND_VEL_Y], m.ghost[KIND_VEL_Z]);
     }
 }
 
@@ -479,15 +490,6 @@ __global__ void __launch_bounds__(256) k_batch_project(BatchTable t, int pack) {
         const int si = batch_sim(first, t.nsims, w);
         const BatchSim& m = t.sims[si];
         project_block<float, float4>(cell_block_of(w - first[si], m.d), m.vel[0], m.vel[1], m.vel[2], pack ? reinterpret_cast<float4*>(m.packed) : nullptr, m.pressure, m.divergence, m.d, m.h, m.h * m.h, m.flow, nullptr);
-    }
-}
-
-__global__ void __launch_bounds__(256) k_batch_post_diagnostics(BatchTable t) {
-    const uint32_t* first = t.first[SHAPE_CELL];
-    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_CELL]; w += gridDim.x) {
-        const int si = batch_sim(first, t.nsims, w);
-        const BatchSim& m = t.sims[si];
-        post_diagnostics_block<float>(cell_block_of(w - first[si], m.d), m.divergence, m.magnitude, m.vel[0], m.vel[1], m.vel[2], m.d, m.h, m.flow);
     }
 }
 
@@ -695,7 +697,7 @@ cudaError_t launch_batch_scalar_source_advect(const BatchTable& t, cudaStream_t 
 }
 
 cudaError_t launch_batch_divergence(const BatchTable& t, cudaStream_t s) {
-    k_batch_divergence<<<batch_grid(t.total[SHAPE_CELL], t.sms, 8), cell_block(), 0, s>>>(t);
+    k_batch_divergence<false><<<batch_grid(t.total[SHAPE_VEC], t.sms, 8), dim3(32, kDivRows), 0, s>>>(t);
     return cudaGetLastError();
 }
 
@@ -705,7 +707,7 @@ cudaError_t launch_batch_project(const BatchTable& t, int pack, cudaStream_t s) 
 }
 
 cudaError_t launch_batch_post_diagnostics(const BatchTable& t, cudaStream_t s) {
-    k_batch_post_diagnostics<<<batch_grid(t.total[SHAPE_CELL], t.sms, 8), cell_block(), 0, s>>>(t);
+    k_batch_divergence<true><<<batch_grid(t.total[SHAPE_VEC], t.sms, 8), dim3(32, kDivRows), 0, s>>>(t);
     return cudaGetLastError();
 }
 
