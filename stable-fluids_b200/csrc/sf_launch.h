@@ -66,6 +66,12 @@ cudaError_t launch_residual_sums(const float* p, const float* div, Dims d, float
 // launched) when the grid or the pointers do not suit it (nx % 4, 16-byte
 // alignment).
 bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s);
+// The Jacobi pressure sweeps of one check interval of the residual-driven
+// solve (a.iterations sweeps from x, landing in x), the last of them adding
+// the FP64 residual sums of its input iterate to stats; false (nothing
+// launched) when the solve is not a plain FP32 Jacobi pressure solve on a
+// vectorisable grid.
+bool launch_pressure_interval_fused(const StencilArgs& a, DeviceStats* stats, cudaStream_t s);
 cudaError_t launch_residual_finalize(DeviceStats* stats, Dims d, int singular, int iterations, cudaStream_t s);
 // One check of the residual-driven pressure solve (see k_residual_check).
 cudaError_t launch_residual_check(DeviceStats* stats, Dims d, int singular, int reset, int increment, double tol, int max_iterations, cudaGraphConditionalHandle handle, cudaStream_t s);

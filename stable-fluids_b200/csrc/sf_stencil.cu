@@ -497,6 +497,79 @@ __global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __r
     residual_vec_block(blockIdx, p, div, h2, z_chunk, d, g, stats);
 }
 
+// One Jacobi pressure sweep dst = update(src) that also adds the FP64
+// residual sums of its input iterate src to stats (the sums of
+// residual_vec_block, from the values the sweep loads anyway: no extra
+// traffic). The residual-driven solve runs it as the last sweep of each
+// check interval, so a check sees the residual of the iterate one sweep
+// before the current one; the Jacobi residual's norm never increases from
+// one sweep to the next (I - A/6 is symmetric with its spectrum in (-1, 1]),
+// so that iterate meeting the tolerance means the current one does too.
+__global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4_residual(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
+    const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
+    if (x0 < d.nx && y < d.ny) {
+        const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+        const float inv = wave::jacobi_inverse(KIND_PRESSURE, h2);
+        const VecGhost4 v = vec_ghost4(x0, y, d, g);
+        const int sz = d.nx * d.ny;
+        int i = x0 + d.nx * (y + d.ny * zb);
+        float4 cur = ld4(src + i);
+        float4 below = vec_below4(src, i, zb, d, g, cur);
+        for (int z = zb; z < ze; ++z, i += sz) {
+            const float4 above = vec_above4(src, i, z, d, g, cur);
+            float a = src[i + v.ox_lo], b = src[i + v.ox_hi];
+            float4 c = ld4(src + i + v.oy_lo), e = ld4(src + i + v.oy_hi);
+            const float4 r = ld4(rhs + i);
+            if (v.gx_lo) a = tb::ghost(g, XM, a);
+            if (v.gx_hi) b = tb::ghost(g, XP, b);
+            if (v.gy_lo) c = ghost4(g, YM, c);
+            if (v.gy_hi) e = ghost4(g, YP, e);
+            float4 o;
+            o.x = wave::jacobi_update<KIND_PRESSURE>(a + cur.y + c.x + e.x + below.x + above.x, r.x, h2, inv);
+            o.y = wave::jacobi_update<KIND_PRESSURE>(cur.x + cur.z + c.y + e.y + below.y + above.y, r.y, h2, inv);
+            o.z = wave::jacobi_update<KIND_PRESSURE>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, h2, inv);
+            o.w = wave::jacobi_update<KIND_PRESSURE>(cur.z + b + c.w + e.w + below.w + above.w, r.w, h2, inv);
+            *reinterpret_cast<float4*>(dst + i) = o;
+            const float xm[4] = {a, cur.x, cur.y, cur.z}, xp[4] = {cur.y, cur.z, cur.w, b};
+            const float ym[4] = {c.x, c.y, c.z, c.w}, yp[4] = {e.x, e.y, e.z, e.w};
+            const float zm[4] = {below.x, below.y, below.z, below.w}, zp[4] = {above.x, above.y, above.z, above.w};
+            const float pc[4] = {cur.x, cur.y, cur.z, cur.w}, rc[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double nb = static_cast<double>(xm[k]) + static_cast<double>(xp[k]) + static_cast<double>(ym[k]) + static_cast<double>(yp[k]) + static_cast<double>(zm[k]) + static_cast<double>(zp[k]);
+                const double bb = static_cast<double>(h2) * static_cast<double>(rc[k]);
+                const double ee = bb - (nb - 6.0 * static_cast<double>(pc[k]));
+                se += ee;
+                se2 += ee * ee;
+                sb += bb;
+                sb2 += bb * bb;
+            }
+            below = cur;
+            cur = above;
+        }
+    }
+    __shared__ double part[4][kVecRows];
+    se = vec_warp_sum(se);
+    se2 = vec_warp_sum(se2);
+    sb = vec_warp_sum(sb);
+    sb2 = vec_warp_sum(sb2);
+    if (threadIdx.x == 0) {
+        part[0][threadIdx.y] = se;
+        part[1][threadIdx.y] = se2;
+        part[2][threadIdx.y] = sb;
+        part[3][threadIdx.y] = sb2;
+    }
+    __syncthreads();
+    if (threadIdx.y == 0 && threadIdx.x < 4) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < kVecRows; ++w) t += part[threadIdx.x][w];
+        double* out = threadIdx.x == 0 ? &stats->sum_e : threadIdx.x == 1 ? &stats->sum_e2 : threadIdx.x == 2 ? &stats->sum_b : &stats->sum_b2;
+        atomicAdd(out, t);
+    }
+}
+
 template <typename T = float>
 __global__ void k_scale_field(T* __restrict__ q, float factor, size_t n) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) q[i] = from_f<T>(to_f(q[i]) * factor);
@@ -946,6 +1019,29 @@ cudaError_t batch_sweep(const BatchTable& t, int scheme, int parity, int dst, in
 }
 
 }  // namespace
+
+bool launch_pressure_interval_fused(const StencilArgs& a, DeviceStats* stats, cudaStream_t s) {
+    if (a.kind != KIND_PRESSURE || a.scheme != SCHEME_JACOBI || a.init != INIT_FROM_X || a.bf16 || a.per_pass >= 2 || a.iterations < 1 || a.scratch == nullptr || !vec_ok(a)) return false;
+    const Dims& d = a.dims;
+    const size_t bytes = static_cast<size_t>(d.nx) * d.ny * d.nz * sizeof(float);
+    const GhostRule g = ghost_rule(KIND_PRESSURE, a.flow, a.scalar);
+    const VecShape vs = vec_shape(d, k_jacobi_vec4<KIND_PRESSURE>);
+    const VecShape rs = vec_shape(d, k_jacobi_vec4_residual);
+    const int units = a.iterations;
+    const float* src = a.x;
+    for (int u = 0; u < units; ++u) {
+        float* dst = ((units - 1 - u) % 2 == 0) ? a.x : a.scratch;  // the last sweep lands in x
+        if (src == dst) {  // odd sweep count: move the start aside (an error surfaces in the capture)
+            cudaMemcpyAsync(a.scratch, a.x, bytes, cudaMemcpyDeviceToDevice, s);
+            src = a.scratch;
+        }
+        if (u + 1 < units) k_jacobi_vec4<KIND_PRESSURE><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
+        else k_jacobi_vec4_residual<<<rs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, rs.z_chunk, d, g, stats);
+        src = dst;
+    }
+    if (a.launches) *a.launches += units;
+    return true;  // launch errors stay pending for the caller's capture to report
+}
 
 bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2, const FlowBC& b, DeviceStats* stats, cudaStream_t s) {
     const auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
