@@ -254,14 +254,40 @@ __device__ __forceinline__ void rbgs_vec4_block(uint3 blk, float* x, const float
     }
 }
 
+// Consecutive sweeps are launched as programmatic dependents of the one
+// before (launch_sweep): a dependent's CTAs become resident as the previous
+// grid's CTAs retire and wait here, before their first global read, until
+// that grid has completed and its writes are visible. Without the launch
+// attribute the wait returns at once.
+__device__ __forceinline__ void wait_for_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <int KIND>
 __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
+    wait_for_previous_grid();
     jacobi_vec4_block<KIND>(blockIdx, dst, src, rhs, coef, z_chunk, d, g);
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(32 * kVecRows) k_rbgs_vec4(float* x, const float* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
+    wait_for_previous_grid();
     rbgs_vec4_block<KIND>(blockIdx, x, rhs, coef, parity, z_chunk, d, g);
+}
+
+// Launches a sweep kernel (one that starts with wait_for_previous_grid) as a
+// programmatic dependent of the preceding kernel on the stream.
+template <typename... P, typename... A>
+cudaError_t launch_sweep(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream_t s, A... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...);
 }
 
 
@@ -506,6 +532,7 @@ __global__ void __launch_bounds__(32 * kVecRows) k_residual_vec(const float* __r
 // one sweep to the next (I - A/6 is symmetric with its spectrum in (-1, 1]),
 // so that iterate meeting the tolerance means the current one does too.
 __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4_residual(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float h2, int z_chunk, Dims d, GhostRule g, DeviceStats* stats) {
+    wait_for_previous_grid();
     const int x0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
     double se = 0.0, se2 = 0.0, sb = 0.0, sb2 = 0.0;
     if (x0 < d.nx && y < d.ny) {
@@ -610,7 +637,10 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             const auto kernel = rbgs_vec_kernel<KIND, T>();
             const VecShape vs = vec_shape(d, kernel);
             for (int it = 0; it < a.iterations; ++it)
-                for (int parity = 0; parity < 2; ++parity) kernel<<<vs.grid, dim3(32, kVecRows), 0, s>>>(ax, ab, a.coef, parity, vs.z_chunk, d, g);
+                for (int parity = 0; parity < 2; ++parity) {
+                    if constexpr (sizeof(T) == sizeof(float)) launch_sweep(kernel, vs.grid, dim3(32, kVecRows), s, ax, ab, a.coef, parity, vs.z_chunk, d, g);
+                    else kernel<<<vs.grid, dim3(32, kVecRows), 0, s>>>(ax, ab, a.coef, parity, vs.z_chunk, d, g);
+                }
         } else {
             const dim3 cblock(32, 8, 1);
             const dim3 grid(static_cast<unsigned>(((d.nx + 1) / 2 + 31) / 32), static_cast<unsigned>((d.ny + 7) / 8), static_cast<unsigned>((d.nz + kColourPlanes - 1) / kColourPlanes));
@@ -645,7 +675,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             T* dst = (left & 1) ? ax : ascr;
             if (dst == src) dst = (dst == ax) ? ascr : ax;
             if (vec) {
-                jacobi_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, ab, a.coef, vs.z_chunk, d, g);
+                if constexpr (sizeof(T) == sizeof(float)) launch_sweep(jacobi_vec, vs.grid, dim3(32, kVecRows), s, dst, static_cast<const T*>(src), ab, a.coef, vs.z_chunk, d, g);
+                else jacobi_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, ab, a.coef, vs.z_chunk, d, g);
             } else {
                 k_jacobi<KIND, T><<<grid, jblock, 0, s>>>(dst, src, ab, a.coef, d, a.flow, a.scalar);
             }
@@ -1035,8 +1066,8 @@ bool launch_pressure_interval_fused(const StencilArgs& a, DeviceStats* stats, cu
             cudaMemcpyAsync(a.scratch, a.x, bytes, cudaMemcpyDeviceToDevice, s);
             src = a.scratch;
         }
-        if (u + 1 < units) k_jacobi_vec4<KIND_PRESSURE><<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, vs.z_chunk, d, g);
-        else k_jacobi_vec4_residual<<<rs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, a.b, a.coef, rs.z_chunk, d, g, stats);
+        if (u + 1 < units) launch_sweep(k_jacobi_vec4<KIND_PRESSURE>, vs.grid, dim3(32, kVecRows), s, dst, src, a.b, a.coef, vs.z_chunk, d, g);
+        else launch_sweep(k_jacobi_vec4_residual, rs.grid, dim3(32, kVecRows), s, dst, src, a.b, a.coef, rs.z_chunk, d, g, stats);
         src = dst;
     }
     if (a.launches) *a.launches += units;
