@@ -99,7 +99,7 @@ __device__ __forceinline__ void advect_velocity_block(uint3 blk, const P* __rest
 }
 
 template <typename T, typename P>
-__global__ void __launch_bounds__(256) k_advect_velocity(const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) { advect_velocity_block<T, P>(blockIdx, v, ox, oy, oz, dt, d, h, b); }
+__global__ void __launch_bounds__(256, 5) k_advect_velocity(const P* __restrict__ v, T* __restrict__ ox, T* __restrict__ oy, T* __restrict__ oz, float dt, Dims d, float h, FlowBC b) { advect_velocity_block<T, P>(blockIdx, v, ox, oy, oz, dt, d, h, b); }
 
 // Scalar value after the source injection rho + dt * S at an interior cell,
 // or the fixed face value (the source never reaches a ghost).
