@@ -82,6 +82,7 @@ struct Context {
     float* divergence = nullptr;
     float* magnitude = nullptr;
     float* scratch = nullptr;
+    float* scratch2 = nullptr;  // red-black solves: the split right-hand side
     DeviceStats* stats = nullptr;
     DeviceStats* host_stats = nullptr;  // pinned
     // learned warm start: the network (not owned), the plain candidate and
@@ -281,6 +282,7 @@ struct Stages {
         a.x = x;
         a.b = b;
         a.scratch = c.scratch;
+        a.scratch2 = c.scratch2;
         a.dims = c.dims;
         a.flow = c.flow;
         a.launches = &launches;
@@ -560,6 +562,8 @@ StableFluidsResult create(const StableFluidsContextCreateDesc* desc, const Stabl
         plan.add(reinterpret_cast<void**>(&c->divergence), fb);
         plan.add(reinterpret_cast<void**>(&c->magnitude), fb);
         plan.add(reinterpret_cast<void**>(&c->scratch), fb);
+        // red-black solves split the right-hand side by colour into a second buffer
+        if (options.scheme == STABLE_FLUIDS_B200_SCHEME_RBGS) plan.add(reinterpret_cast<void**>(&c->scratch2), fb);
         plan.add(reinterpret_cast<void**>(&c->stats), sizeof(DeviceStats));
         if (options.warm_start == STABLE_FLUIDS_B200_WARM_START_LEARNED) {
             plan.add(reinterpret_cast<void**>(&c->alt), fb);

@@ -38,6 +38,7 @@ struct StencilArgs {
     float* x;            // the iterate (result lands here); BF16 elements when bf16
     const float* b;      // right-hand side (diffusion: advected field; pressure: divergence); BF16 when bf16
     float* scratch;      // a field-sized buffer for out-of-place sweeps
+    float* scratch2;     // a second field-sized buffer (a red-black solve's split right-hand side); may be null
     Dims dims;
     FlowBC flow;
     ScalarBC scalar;

@@ -291,6 +291,116 @@ cudaError_t launch_sweep(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream
 }
 
 
+// ---- FP32 fields: red-black solves in the split layout ---------------------
+// For an RBGS solve the iterate and the right-hand side are stored split by
+// colour: two arrays (red, black), each [nz][ny][nx / 2], holding in row
+// (y, z) the cells x = 2k + s, k = 0 .. nx/2 - 1, with s = (y + z) & 1 for
+// the red array and 1 - s for the black one (red: x + y + z even). A colour
+// update then reads only the other colour's array and the right-hand side of
+// its own colour, and writes its own array, all dense: 12 B per updated
+// cell, so 12 B per cell per iteration, where a colour launch on the
+// interleaved field moves whole lines (12 B per cell per colour). In the
+// split layout the six neighbours of the cell (x = 2k + s_u, y, z) of colour
+// array u are, in the other array v: k + s_u - 1 and k + s_u of the same row
+// (x - 1, x + 1), and k of rows y - 1, y + 1 and of planes z - 1, z + 1 (the
+// other colour's offset in an adjacent row is s_u, so the cell beside sits
+// at the same k). The update is the colour launch's: the same six values
+// summed in the reference's order (x-, x+, y-, y+, z-, z+), the same
+// numerator and exact division, so every cell gets the same bits. Face
+// ghosts take the cell's own value from u (threads on a face read their own
+// float4); periodic axes wrap k or the row (even sizes only: an odd periodic
+// size breaks the colouring and leaves the solve to the colour launches).
+
+// Splits (or, with SPLIT false, merges and scales) a field: a thread moves
+// eight cells of a row, two float4 of the field and one of each colour
+// array. `red2` / `black2` (split only, may be null) receive a second copy.
+template <bool SPLIT>
+__global__ void __launch_bounds__(256) k_rb_layout(float* __restrict__ field, float* __restrict__ red, float* __restrict__ black, float* __restrict__ red2, float* __restrict__ black2, float scale, Dims d) {
+    const int per_row = d.nx / 8;
+    const size_t n8 = static_cast<size_t>(per_row) * d.ny * d.nz;
+    for (size_t f = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; f < n8; f += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t row = f / per_row;
+        const int y = static_cast<int>(row % d.ny), z = static_cast<int>(row / d.ny);
+        const bool odd = ((y + z) & 1) != 0;  // the row's red cells sit at odd x
+        float4* const fp = reinterpret_cast<float4*>(field + 8 * f);
+        if constexpr (SPLIT) {
+            const float4 v0 = fp[0], v1 = fp[1];
+            const float4 r = odd ? make_float4(v0.y, v0.w, v1.y, v1.w) : make_float4(v0.x, v0.z, v1.x, v1.z);
+            const float4 b = odd ? make_float4(v0.x, v0.z, v1.x, v1.z) : make_float4(v0.y, v0.w, v1.y, v1.w);
+            reinterpret_cast<float4*>(red)[f] = r;
+            reinterpret_cast<float4*>(black)[f] = b;
+            if (red2 != nullptr) {
+                reinterpret_cast<float4*>(red2)[f] = r;
+                reinterpret_cast<float4*>(black2)[f] = b;
+            }
+        } else {
+            float4 r = reinterpret_cast<const float4*>(red)[f], b = reinterpret_cast<const float4*>(black)[f];
+            r = make_float4(__fmul_rn(r.x, scale), __fmul_rn(r.y, scale), __fmul_rn(r.z, scale), __fmul_rn(r.w, scale));
+            b = make_float4(__fmul_rn(b.x, scale), __fmul_rn(b.y, scale), __fmul_rn(b.z, scale), __fmul_rn(b.w, scale));
+            fp[0] = odd ? make_float4(b.x, r.x, b.y, r.y) : make_float4(r.x, b.x, r.y, b.y);
+            fp[1] = odd ? make_float4(b.z, r.z, b.w, r.w) : make_float4(r.z, b.z, r.w, b.w);
+        }
+    }
+}
+
+// One colour of an RBGS iteration in the split layout, in place: u (the
+// colour's array) from v (the other colour's) and w (the right-hand side's
+// array of u's colour); `colour` 0 = red, 1 = black. A thread owns a float4
+// of a half row (k0 .. k0 + 3) and marches a z chunk with v's planes below,
+// at and above in registers; y neighbours and the extra x neighbour come
+// from L1. No thread reads another's cells of u, so the update is in place.
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(float* u, const float* __restrict__ v, const float* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
+    const int hx = d.nx / 2;
+    const int k0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    wait_for_previous_grid();
+    if (k0 >= hx || y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const bool px = g.periodic[0] != 0, py = g.periodic[1] != 0, pz = g.periodic[2] != 0;
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const double recip = tb::recip64(divisor);
+    const int hsz = hx * d.ny;
+    // rows y - 1, y + 1 (offsets in the half plane) and their face ghosts
+    const bool gy_lo = !py && y == 0, gy_hi = !py && y == d.ny - 1;
+    const int oy_lo = y > 0 ? -hx : (py ? (d.ny - 1) * hx : 0), oy_hi = y + 1 < d.ny ? hx : (py ? -(d.ny - 1) * hx : 0);
+    // the extra x neighbour: k0 - 1 (rows whose u cells sit at even x) or
+    // k0 + 4 (odd x), wrapped or replaced by a ghost at a face
+    const bool gx_lo = !px && k0 == 0, gx_hi = !px && k0 + 4 == hx;
+    const int ox_lo = k0 > 0 ? -1 : (px ? hx - 1 : 0), ox_hi = k0 + 4 < hx ? 4 : (px ? 4 - hx : 3);
+    const bool xy_face = gx_lo || gx_hi || gy_lo || gy_hi;
+    int i = k0 + hx * (y + d.ny * zb);
+    float4 cur = ld4(v + i);
+    float4 below = zb > 0 ? ld4(v + i - hsz) : (pz ? ld4(v + i + (d.nz - 1) * hsz) : cur);
+    for (int z = zb; z < ze; ++z, i += hsz) {
+        const bool z_lo = !pz && z == 0, z_hi = !pz && z == d.nz - 1;
+        const float4 above = z + 1 < d.nz ? ld4(v + i + hsz) : (pz ? ld4(v + i - (d.nz - 1) * hsz) : cur);
+        const bool s_odd = ((y + z + colour) & 1) != 0;  // this row's cells of u sit at odd x
+        float ext = v[i + (s_odd ? ox_hi : ox_lo)];
+        float4 c = ld4(v + i + oy_lo), e = ld4(v + i + oy_hi);
+        const float4 r = ld4(w + i);
+        float4 zm = below, zp = above;
+        if (xy_face || z_lo || z_hi) {
+            const float4 self = ld4(u + i);
+            if (s_odd ? gx_hi : gx_lo) ext = tb::ghost(g, s_odd ? XP : XM, s_odd ? self.w : self.x);
+            if (gy_lo) c = ghost4(g, YM, self);
+            if (gy_hi) e = ghost4(g, YP, self);
+            if (z_lo) zm = ghost4(g, ZM, self);
+            if (z_hi) zp = ghost4(g, ZP, self);
+        }
+        const float xm0 = s_odd ? cur.x : ext, xm1 = s_odd ? cur.y : cur.x, xm2 = s_odd ? cur.z : cur.y, xm3 = s_odd ? cur.w : cur.z;
+        const float xp0 = s_odd ? cur.y : cur.x, xp1 = s_odd ? cur.z : cur.y, xp2 = s_odd ? cur.w : cur.z, xp3 = s_odd ? ext : cur.w;
+        float4 o;
+        o.x = vec_update<KIND>(xm0 + xp0 + c.x + e.x + zm.x + zp.x, r.x, coef, divisor, recip);
+        o.y = vec_update<KIND>(xm1 + xp1 + c.y + e.y + zm.y + zp.y, r.y, coef, divisor, recip);
+        o.z = vec_update<KIND>(xm2 + xp2 + c.z + e.z + zm.z + zp.z, r.z, coef, divisor, recip);
+        o.w = vec_update<KIND>(xm3 + xp3 + c.w + e.w + zm.w + zp.w, r.w, coef, divisor, recip);
+        *reinterpret_cast<float4*>(u + i) = o;
+        below = cur;
+        cur = above;
+    }
+}
+
+
 // ---- BF16 fields: 4 cells per thread (one 8-byte vector) ------------------
 // The diffusion fields of a BF16-storage context. Same march, ghosts, sum
 // order and division as the float4 kernels, in FP32 arithmetic on the
@@ -617,6 +727,69 @@ auto rbgs_vec_kernel() {
     else return k_rbgs_bf16<KIND>;
 }
 
+// True when a periodic axis of odd size breaks the red-black colouring
+// across its wrap (the first and last cells of a line share a colour).
+bool odd_periodic(const StencilArgs& a) {
+    const bool sc = a.kind == KIND_SCALAR;
+    const int per[3] = {sc ? a.scalar.periodic[0] : a.flow.periodic[0], sc ? a.scalar.periodic[1] : a.flow.periodic[1], sc ? a.scalar.periodic[2] : a.flow.periodic[2]};
+    const int n[3] = {a.dims.nx, a.dims.ny, a.dims.nz};
+    for (int k = 0; k < 3; ++k)
+        if (per[k] && (n[k] & 1)) return true;
+    return false;
+}
+
+// The split-layout red-black solve applies: FP32 field, rows of a multiple of
+// 8 cells (float4 of each colour array), both scratch buffers, no odd
+// periodic axis; per_pass 1 asks for the colour launches instead.
+bool rb_split_ok(const StencilArgs& a) {
+    if (a.bf16 || a.scratch == nullptr || a.scratch2 == nullptr || a.per_pass == 1 || a.iterations < 1) return false;
+    if (a.dims.nx % 8 != 0 || !vec_ok(a) || (reinterpret_cast<uintptr_t>(a.scratch2) & 15) != 0) return false;
+    return !odd_periodic(a);
+}
+
+template <bool SPLIT>
+cudaError_t launch_rb_layout(float* field, float* red, float* black, float* red2, float* black2, float scale, const Dims& d, cudaStream_t s) {
+    const size_t n8 = static_cast<size_t>(d.nx / 8) * d.ny * d.nz;
+    size_t blocks = (n8 + 255) / 256;
+    if (blocks > 148u * 16u) blocks = 148u * 16u;
+    k_rb_layout<SPLIT><<<static_cast<unsigned>(blocks), 256, 0, s>>>(field, red, black, red2, black2, scale, d);
+    return cudaGetLastError();
+}
+
+// The solve in the split layout: the right-hand side split into scratch2,
+// the iterate into scratch (from x, from b, or zero), the iterations as red
+// and black half launches, then the iterate merged back into x, times
+// out_scale.
+template <int KIND>
+cudaError_t run_rb_split(const StencilArgs& a, cudaStream_t s) {
+    const Dims& d = a.dims;
+    const size_t half = static_cast<size_t>(d.nx) * d.ny * d.nz / 2;
+    float* const xr = a.scratch;
+    float* const xb = a.scratch + half;
+    float* const br = a.scratch2;
+    float* const bb = a.scratch2 + half;
+    cudaError_t e = cudaSuccess;
+    const bool from_b = a.init == INIT_FROM_B;
+    if ((e = launch_rb_layout<true>(const_cast<float*>(a.b), br, bb, from_b ? xr : nullptr, from_b ? xb : nullptr, 1.0f, d, s)) != cudaSuccess) return e;
+    int kernels = 2;  // the right-hand side's split and the final merge
+    if (a.init == INIT_ZERO) {
+        if ((e = cudaMemsetAsync(a.scratch, 0, 2 * half * sizeof(float), s)) != cudaSuccess) return e;
+    } else if (a.init == INIT_FROM_X) {
+        if ((e = launch_rb_layout<true>(a.x, xr, xb, nullptr, nullptr, 1.0f, d, s)) != cudaSuccess) return e;
+        ++kernels;
+    }
+    const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
+    const auto kern = k_rb_half<KIND>;
+    const VecShape vs = vec_shape(d, kern, 8);
+    for (int it = 0; it < a.iterations; ++it) {
+        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xr, static_cast<const float*>(xb), static_cast<const float*>(br), a.coef, 0, vs.z_chunk, d, g)) != cudaSuccess) return e;
+        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xb, static_cast<const float*>(xr), static_cast<const float*>(bb), a.coef, 1, vs.z_chunk, d, g)) != cudaSuccess) return e;
+    }
+    if ((e = launch_rb_layout<false>(a.x, xr, xb, nullptr, nullptr, a.out_scale, d, s)) != cudaSuccess) return e;
+    if (a.launches) *a.launches += 2 * a.iterations + kernels;
+    return cudaSuccess;
+}
+
 // T: element type of x, b and scratch (BF16 only for the diffusion kinds of a
 // BF16-storage context; the pressure is always FP32).
 template <int KIND, typename T>
@@ -629,6 +802,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
     const T* const ab = reinterpret_cast<const T*>(a.b);
     cudaError_t e = cudaSuccess;
     if (a.scheme == SCHEME_RBGS) {
+        if constexpr (sizeof(T) == sizeof(float))
+            if (rb_split_ok(a)) return run_rb_split<KIND>(a, s);
         if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(ax, ab, bytes, cudaMemcpyDeviceToDevice, s);
         else if (a.init == INIT_ZERO) e = cudaMemsetAsync(ax, 0, bytes, s);
         if (e != cudaSuccess) return e;
@@ -718,14 +893,7 @@ int wave_width(const StencilArgs& a) {
     if (a.bf16 || a.scratch == nullptr || !vec_ok(a)) return 0;
     if (a.dims.nx != 128 && a.dims.nx != 256) return 0;
     if (a.dims.nz <= 8) return 0;  // the chunk halo wraps a periodic z axis at most once
-    if (a.scheme == SCHEME_RBGS) {
-        // an odd periodic size breaks the red-black colouring across the wrap
-        const int kind = a.kind;
-        const int per[3] = {kind == KIND_SCALAR ? a.scalar.periodic[0] : a.flow.periodic[0], kind == KIND_SCALAR ? a.scalar.periodic[1] : a.flow.periodic[1], kind == KIND_SCALAR ? a.scalar.periodic[2] : a.flow.periodic[2]};
-        const int n[3] = {a.dims.nx, a.dims.ny, a.dims.nz};
-        for (int k = 0; k < 3; ++k)
-            if (per[k] && (n[k] & 1)) return 0;
-    }
+    if (a.scheme == SCHEME_RBGS && odd_periodic(a)) return 0;  // the colouring breaks across the wrap
     return a.dims.nx / 128;
 }
 

@@ -384,6 +384,40 @@ def test_wave_rbgs_matches_reference_library(kind, sf, lib, ref_lib, cuda):
         assert_bit_equal(_run_scene(sf, lib, scene, opts), ref)
 
 
+def _rb_split_scene(sf, kind):
+    """Grids at the edges of the split-layout red-black solve: colour rows of
+    one float4 and of 64 and 128, a row length it leaves to the colour
+    launches (12), odd y and z sizes, and periodic axes down to two planes."""
+    sc = sf.scenes
+    periodic = (sc.flow_boundary([sf.FLOW_PERIODIC] * 6), sc.scalar_boundary([sf.SCALAR_PERIODIC] * 6))
+    grids = {
+        "narrow_8x9x7": ((8, 9, 7), sc.stam_walls()),
+        "narrow_12x31x6": ((12, 31, 6), sc.benchmark_walls()),
+        "wide_512x11x9": ((512, 11, 9), sc.stam_walls()),
+        "wide_1024x7x6": ((1024, 7, 6), sc.benchmark_walls()),
+        "periodic_16x6x2": ((16, 6, 2), periodic),
+        "periodic_64x10x12": ((64, 10, 12), periodic),
+    }
+    n, walls = grids[kind]
+    return _tiled_scene(sf, n, walls)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["narrow_8x9x7", "narrow_12x31x6", "wide_512x11x9", "wide_1024x7x6", "periodic_16x6x2", "periodic_64x10x12"])
+def test_rbgs_split_matches_colour_launches(kind, sf, lib, ref_lib, cuda):
+    """Red-black solves in the split layout (the default for FP32 fields)
+    give the bits of the colour launches on the interleaved field
+    (iterations_per_pass = 1) and of the reference library."""
+    scene = _rb_split_scene(sf, kind)
+    outs = {}
+    for per_pass in (0, 1):
+        opts = sf.default_options(lib)
+        opts.iterations_per_pass = per_pass
+        outs[per_pass] = _run_scene(sf, lib, scene, opts)
+    assert_bit_equal(outs[0], outs[1])
+    assert_bit_equal(outs[0], _run_scene(sf, ref_lib, scene))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["stam_128x44x37", "periodic_xz_256x12x10"])
 def test_wave_jacobi_matches_oracle(kind, sf, lib, orc, cuda):
