@@ -349,12 +349,15 @@ __global__ void __launch_bounds__(256) k_rb_layout(float* __restrict__ field, fl
 // of a half row (k0 .. k0 + 3) and marches a z chunk with v's planes below,
 // at and above in registers; y neighbours and the extra x neighbour come
 // from L1. No thread reads another's cells of u, so the update is in place.
+// Threads are numbered along the half plane (blockIdx.x, 128 float4 a CTA;
+// blockIdx.z the z chunk), so short rows still fill every lane of a warp.
 template <int KIND>
 __global__ void __launch_bounds__(32 * kVecRows) k_rb_half(float* u, const float* __restrict__ v, const float* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
-    const int hx = d.nx / 2;
-    const int k0 = 4 * static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * kVecRows + threadIdx.y);
+    const int hx = d.nx / 2, q4 = hx / 4;
+    const int j = static_cast<int>(blockIdx.x) * (32 * kVecRows) + static_cast<int>(threadIdx.y * 32 + threadIdx.x);
+    const int y = j / q4, k0 = 4 * (j - y * q4);
     wait_for_previous_grid();
-    if (k0 >= hx || y >= d.ny) return;
+    if (y >= d.ny) return;
     const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const bool px = g.periodic[0] != 0, py = g.periodic[1] != 0, pz = g.periodic[2] != 0;
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
@@ -550,6 +553,26 @@ VecShape vec_shape(const Dims& d, Kernel kernel, int width = 4) {
     if (z_chunk < 4) z_chunk = d.nz < 4 ? d.nz : 4;
     const int bz = (d.nz + z_chunk - 1) / z_chunk;
     return {dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by), static_cast<unsigned>(bz)), z_chunk};
+}
+
+// The grid of a kernel whose threads are numbered along a plane of
+// `per_plane` float4 (128 a CTA) and whose CTAs march z chunks: one wave.
+template <typename Kernel>
+VecShape plane_shape(const Dims& d, Kernel kernel, long long per_plane) {
+    static int per_sm = [&] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 32 * kVecRows, 0) != cudaSuccess || n < 1) n = 4;
+        return n;
+    }();
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long bxy = (per_plane + 32 * kVecRows - 1) / (32 * kVecRows);
+    long long chunks = static_cast<long long>(sms) * per_sm / bxy;
+    if (chunks < 1) chunks = 1;
+    int z_chunk = static_cast<int>((d.nz + chunks - 1) / chunks);
+    if (z_chunk < 4) z_chunk = d.nz < 4 ? d.nz : 4;
+    const int bz = (d.nz + z_chunk - 1) / z_chunk;
+    return {dim3(static_cast<unsigned>(bxy), 1, static_cast<unsigned>(bz)), z_chunk};
 }
 
 bool vec_ok(const StencilArgs& a, int width = 4) {
@@ -780,7 +803,7 @@ cudaError_t run_rb_split(const StencilArgs& a, cudaStream_t s) {
     }
     const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
     const auto kern = k_rb_half<KIND>;
-    const VecShape vs = vec_shape(d, kern, 8);
+    const VecShape vs = plane_shape(d, kern, static_cast<long long>(d.nx / 8) * d.ny);
     for (int it = 0; it < a.iterations; ++it) {
         if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xr, static_cast<const float*>(xb), static_cast<const float*>(br), a.coef, 0, vs.z_chunk, d, g)) != cudaSuccess) return e;
         if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xb, static_cast<const float*>(xr), static_cast<const float*>(bb), a.coef, 1, vs.z_chunk, d, g)) != cudaSuccess) return e;
