@@ -370,21 +370,26 @@ __global__ void __launch_bounds__(32 * kVecRows) k_rb_half(float* u, const float
     // k0 + 4 (odd x), wrapped or replaced by a ghost at a face
     const bool gx_lo = !px && k0 == 0, gx_hi = !px && k0 + 4 == hx;
     const int ox_lo = k0 > 0 ? -1 : (px ? hx - 1 : 0), ox_hi = k0 + 4 < hx ? 4 : (px ? 4 - hx : 3);
-    const bool xy_face = gx_lo || gx_hi || gy_lo || gy_hi;
+    // x faces: one cell of the thread (cell 0 on rows whose cells sit at even
+    // x, cell 3 on odd ones) takes its x ghost, from its own value in u
+    // y faces: the whole row; z faces: the whole plane (a branch interior
+    // threads skip, rather than selects every thread executes)
+    const bool y_face = gy_lo || gy_hi;
+    const int off_up = pz ? -(d.nz - 1) * hsz : 0;  // plane z + 1 from the top plane (itself on a face)
     int i = k0 + hx * (y + d.ny * zb);
     float4 cur = ld4(v + i);
-    float4 below = zb > 0 ? ld4(v + i - hsz) : (pz ? ld4(v + i + (d.nz - 1) * hsz) : cur);
+    float4 below = ld4(v + i + (zb > 0 ? -hsz : (pz ? (d.nz - 1) * hsz : 0)));
     for (int z = zb; z < ze; ++z, i += hsz) {
-        const bool z_lo = !pz && z == 0, z_hi = !pz && z == d.nz - 1;
-        const float4 above = z + 1 < d.nz ? ld4(v + i + hsz) : (pz ? ld4(v + i - (d.nz - 1) * hsz) : cur);
+        const float4 above = ld4(v + i + (z + 1 < d.nz ? hsz : off_up));
         const bool s_odd = ((y + z + colour) & 1) != 0;  // this row's cells of u sit at odd x
         float ext = v[i + (s_odd ? ox_hi : ox_lo)];
         float4 c = ld4(v + i + oy_lo), e = ld4(v + i + oy_hi);
         const float4 r = ld4(w + i);
+        if (s_odd ? gx_hi : gx_lo) ext = tb::ghost(g, s_odd ? XP : XM, u[i + (s_odd ? 3 : 0)]);
         float4 zm = below, zp = above;
-        if (xy_face || z_lo || z_hi) {
+        const bool z_lo = !pz && z == 0, z_hi = !pz && z == d.nz - 1;
+        if (y_face || z_lo || z_hi) [[unlikely]] {
             const float4 self = ld4(u + i);
-            if (s_odd ? gx_hi : gx_lo) ext = tb::ghost(g, s_odd ? XP : XM, s_odd ? self.w : self.x);
             if (gy_lo) c = ghost4(g, YM, self);
             if (gy_hi) e = ghost4(g, YP, self);
             if (z_lo) zm = ghost4(g, ZM, self);
