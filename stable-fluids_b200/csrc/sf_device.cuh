@@ -225,6 +225,19 @@ __device__ __forceinline__ Cell locate(float x, float y, float z, float h) {
     return c;
 }
 
+// The 2x2x2 block of corners at (x0, y0, z0) lies inside the grid. Written
+// as x0 < n - 1, not x0 + 1 < n: the position of a diverged (infinite)
+// velocity saturates x0 to INT_MAX, and x0 + 1 would wrap to a negative.
+__device__ __forceinline__ bool block_inside(const Cell& c, const Dims& d) {
+    return c.x0 >= 0 && c.y0 >= 0 && c.z0 >= 0 && c.x0 < d.nx - 1 && c.y0 < d.ny - 1 && c.z0 < d.nz - 1;
+}
+
+// A corner block's base index for the boundary path, limited to [-2, n]:
+// corners beyond a non-periodic face resolve to the same face value however
+// far out they lie (positions on a periodic axis are wrapped first), and the
+// limit keeps base + 1 from overflowing.
+__device__ __forceinline__ int corner_base(int c, int n) { return c < -2 ? -2 : (c > n ? n : c); }
+
 // Interpolation in x, then y, then z, each as a + (b - a) * t with the
 // product and the sum rounded once (one FMA): the contraction the compiler
 // applies to the reference's expression (backend-cuda.cu:231-237), written
@@ -247,7 +260,7 @@ __device__ __forceinline__ float3 sample_velocity3(const P* __restrict__ v, floa
     if (b.periodic[2]) z = wrap_world(z, static_cast<float>(d.nz) * h);
     const Cell c = locate(x, y, z, h);
     float3 s[8];
-    if (c.x0 >= 0 && c.y0 >= 0 && c.z0 >= 0 && c.x0 + 1 < d.nx && c.y0 + 1 < d.ny && c.z0 + 1 < d.nz) {
+    if (block_inside(c, d)) {
         const size_t i = lin(c.x0, c.y0, c.z0, d);
         const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
         const size_t off[8] = {0, 1, sy, sy + 1, sz, sz + 1, sz + sy, sz + sy + 1};
@@ -257,8 +270,9 @@ __device__ __forceinline__ float3 sample_velocity3(const P* __restrict__ v, floa
             s[k] = make_float3(q.x, q.y, q.z);
         }
     } else {
+        const int bx = corner_base(c.x0, d.nx), by = corner_base(c.y0, d.ny), bz = corner_base(c.z0, d.nz);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) s[k] = load_velocity3(v, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, b);
+        for (int k = 0; k < 8; ++k) s[k] = load_velocity3(v, bx + (k & 1), by + ((k >> 1) & 1), bz + (k >> 2), d, b);
     }
     return make_float3(trilerp(s[0].x, s[1].x, s[2].x, s[3].x, s[4].x, s[5].x, s[6].x, s[7].x, c),
                        trilerp(s[0].y, s[1].y, s[2].y, s[3].y, s[4].y, s[5].y, s[6].y, s[7].y, c),

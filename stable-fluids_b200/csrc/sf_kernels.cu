@@ -129,7 +129,7 @@ __device__ __forceinline__ void scalar_source_advect_block(uint3 blk, const P* _
     if (sb.periodic[2]) t.z = wrap_world(t.z, static_cast<float>(d.nz) * h);
     const Cell c = locate(t.x, t.y, t.z, h);
     float s[8];
-    if (c.x0 >= 0 && c.y0 >= 0 && c.z0 >= 0 && c.x0 + 1 < d.nx && c.y0 + 1 < d.ny && c.z0 + 1 < d.nz) {
+    if (block_inside(c, d)) {
         // the whole 2x2x2 block is inside: no ghost rule applies
         const size_t i = lin(c.x0, c.y0, c.z0, d);
         const size_t sy = static_cast<size_t>(d.nx), sz = static_cast<size_t>(d.nx) * static_cast<size_t>(d.ny);
@@ -139,8 +139,9 @@ __device__ __forceinline__ void scalar_source_advect_block(uint3 blk, const P* _
             s[k] = __fmaf_rn(dt, __ldg(&src[j]), ldg_f(&q[j]));
         }
     } else {
+        const int bx = corner_base(c.x0, d.nx), by = corner_base(c.y0, d.ny), bz = corner_base(c.z0, d.nz);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, c.x0 + (k & 1), c.y0 + ((k >> 1) & 1), c.z0 + (k >> 2), d, sb);
+        for (int k = 0; k < 8; ++k) s[k] = sourced_scalar(q, src, dt, bx + (k & 1), by + ((k >> 1) & 1), bz + (k >> 2), d, sb);
     }
     out[lin(x, y, z, d)] = from_f<T>(trilerp(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], c));
 }

@@ -146,6 +146,27 @@ def test_abi_error_paths(sf, lib, cuda):
     assert lib.stable_fluids_destroy_context_cuda(None) == sf.RESULT_OK
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("walls", ["stam", "benchmark"])
+def test_diverged_velocity_stays_in_bounds(walls, sf, lib, cuda):
+    """A force of +-inf or NaN (a diverged simulation) makes back-traced
+    positions infinite or NaN; the advection gathers must still read inside
+    the fields (the step completes and the views are readable)."""
+    sc = sf.scenes
+    scene = _tiled_scene(sf, (16, 12, 10), sc.stam_walls() if walls == "stam" else sc.benchmark_walls(), steps=2)
+    sim = sf.Simulation(scene.config, scene.scalars, scene.vectors, lib=lib)
+    n = 16 * 12 * 10
+    fx, fy, fz = np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+    fx[5], fy[700], fz[1200] = np.inf, -np.inf, np.nan
+    fx[1500] = 3.0e38
+    sim.set_vector(sim.vector_handles[0], fx, fy, fz)
+    sim.step(2)
+    sim.synchronize()
+    vel = sim.fetch(sf.VIEW_FLOW_VELOCITY)
+    assert all(v.shape == (10, 12, 16) for v in vel)
+    sim.close()
+
+
 def _create_rc(sf, lib, cfg, scalars=(), vectors=()):
     import ctypes
 
