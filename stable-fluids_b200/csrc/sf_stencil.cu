@@ -291,124 +291,6 @@ cudaError_t launch_sweep(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream
 }
 
 
-// ---- FP32 fields: red-black solves in the split layout ---------------------
-// For an RBGS solve the iterate and the right-hand side are stored split by
-// colour: two arrays (red, black), each [nz][ny][nx / 2], holding in row
-// (y, z) the cells x = 2k + s, k = 0 .. nx/2 - 1, with s = (y + z) & 1 for
-// the red array and 1 - s for the black one (red: x + y + z even). A colour
-// update then reads only the other colour's array and the right-hand side of
-// its own colour, and writes its own array, all dense: 12 B per updated
-// cell, so 12 B per cell per iteration, where a colour launch on the
-// interleaved field moves whole lines (12 B per cell per colour). In the
-// split layout the six neighbours of the cell (x = 2k + s_u, y, z) of colour
-// array u are, in the other array v: k + s_u - 1 and k + s_u of the same row
-// (x - 1, x + 1), and k of rows y - 1, y + 1 and of planes z - 1, z + 1 (the
-// other colour's offset in an adjacent row is s_u, so the cell beside sits
-// at the same k). The update is the colour launch's: the same six values
-// summed in the reference's order (x-, x+, y-, y+, z-, z+), the same
-// numerator and exact division, so every cell gets the same bits. Face
-// ghosts take the cell's own value from u (threads on a face read their own
-// float4); periodic axes wrap k or the row (even sizes only: an odd periodic
-// size breaks the colouring and leaves the solve to the colour launches).
-
-// Splits (or, with SPLIT false, merges and scales) a field: a thread moves
-// eight cells of a row, two float4 of the field and one of each colour
-// array. `red2` / `black2` (split only, may be null) receive a second copy.
-template <bool SPLIT>
-__global__ void __launch_bounds__(256) k_rb_layout(float* __restrict__ field, float* __restrict__ red, float* __restrict__ black, float* __restrict__ red2, float* __restrict__ black2, float scale, Dims d) {
-    const int per_row = d.nx / 8;
-    const size_t n8 = static_cast<size_t>(per_row) * d.ny * d.nz;
-    for (size_t f = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; f < n8; f += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const size_t row = f / per_row;
-        const int y = static_cast<int>(row % d.ny), z = static_cast<int>(row / d.ny);
-        const bool odd = ((y + z) & 1) != 0;  // the row's red cells sit at odd x
-        float4* const fp = reinterpret_cast<float4*>(field + 8 * f);
-        if constexpr (SPLIT) {
-            const float4 v0 = fp[0], v1 = fp[1];
-            const float4 r = odd ? make_float4(v0.y, v0.w, v1.y, v1.w) : make_float4(v0.x, v0.z, v1.x, v1.z);
-            const float4 b = odd ? make_float4(v0.x, v0.z, v1.x, v1.z) : make_float4(v0.y, v0.w, v1.y, v1.w);
-            reinterpret_cast<float4*>(red)[f] = r;
-            reinterpret_cast<float4*>(black)[f] = b;
-            if (red2 != nullptr) {
-                reinterpret_cast<float4*>(red2)[f] = r;
-                reinterpret_cast<float4*>(black2)[f] = b;
-            }
-        } else {
-            float4 r = reinterpret_cast<const float4*>(red)[f], b = reinterpret_cast<const float4*>(black)[f];
-            r = make_float4(__fmul_rn(r.x, scale), __fmul_rn(r.y, scale), __fmul_rn(r.z, scale), __fmul_rn(r.w, scale));
-            b = make_float4(__fmul_rn(b.x, scale), __fmul_rn(b.y, scale), __fmul_rn(b.z, scale), __fmul_rn(b.w, scale));
-            fp[0] = odd ? make_float4(b.x, r.x, b.y, r.y) : make_float4(r.x, b.x, r.y, b.y);
-            fp[1] = odd ? make_float4(b.z, r.z, b.w, r.w) : make_float4(r.z, b.z, r.w, b.w);
-        }
-    }
-}
-
-// One colour of an RBGS iteration in the split layout, in place: u (the
-// colour's array) from v (the other colour's) and w (the right-hand side's
-// array of u's colour); `colour` 0 = red, 1 = black. A thread owns a float4
-// of a half row (k0 .. k0 + 3) and marches a z chunk with v's planes below,
-// at and above in registers; y neighbours and the extra x neighbour come
-// from L1. No thread reads another's cells of u, so the update is in place.
-// Threads are numbered along the half plane (blockIdx.x, 128 float4 a CTA;
-// blockIdx.z the z chunk), so short rows still fill every lane of a warp.
-template <int KIND>
-__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(float* u, const float* __restrict__ v, const float* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
-    const int hx = d.nx / 2, q4 = hx / 4;
-    const int j = static_cast<int>(blockIdx.x) * (32 * kVecRows) + static_cast<int>(threadIdx.y * 32 + threadIdx.x);
-    const int y = j / q4, k0 = 4 * (j - y * q4);
-    wait_for_previous_grid();
-    if (y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
-    const bool px = g.periodic[0] != 0, py = g.periodic[1] != 0, pz = g.periodic[2] != 0;
-    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
-    const double recip = tb::recip64(divisor);
-    const int hsz = hx * d.ny;
-    // rows y - 1, y + 1 (offsets in the half plane) and their face ghosts
-    const bool gy_lo = !py && y == 0, gy_hi = !py && y == d.ny - 1;
-    const int oy_lo = y > 0 ? -hx : (py ? (d.ny - 1) * hx : 0), oy_hi = y + 1 < d.ny ? hx : (py ? -(d.ny - 1) * hx : 0);
-    // the extra x neighbour: k0 - 1 (rows whose u cells sit at even x) or
-    // k0 + 4 (odd x), wrapped or replaced by a ghost at a face
-    const bool gx_lo = !px && k0 == 0, gx_hi = !px && k0 + 4 == hx;
-    const int ox_lo = k0 > 0 ? -1 : (px ? hx - 1 : 0), ox_hi = k0 + 4 < hx ? 4 : (px ? 4 - hx : 3);
-    // x faces: one cell of the thread (cell 0 on rows whose cells sit at even
-    // x, cell 3 on odd ones) takes its x ghost, from its own value in u
-    // y faces: the whole row; z faces: the whole plane (a branch interior
-    // threads skip, rather than selects every thread executes)
-    const bool y_face = gy_lo || gy_hi;
-    const int off_up = pz ? -(d.nz - 1) * hsz : 0;  // plane z + 1 from the top plane (itself on a face)
-    int i = k0 + hx * (y + d.ny * zb);
-    float4 cur = ld4(v + i);
-    float4 below = ld4(v + i + (zb > 0 ? -hsz : (pz ? (d.nz - 1) * hsz : 0)));
-    for (int z = zb; z < ze; ++z, i += hsz) {
-        const float4 above = ld4(v + i + (z + 1 < d.nz ? hsz : off_up));
-        const bool s_odd = ((y + z + colour) & 1) != 0;  // this row's cells of u sit at odd x
-        float ext = v[i + (s_odd ? ox_hi : ox_lo)];
-        float4 c = ld4(v + i + oy_lo), e = ld4(v + i + oy_hi);
-        const float4 r = ld4(w + i);
-        if (s_odd ? gx_hi : gx_lo) ext = tb::ghost(g, s_odd ? XP : XM, u[i + (s_odd ? 3 : 0)]);
-        float4 zm = below, zp = above;
-        const bool z_lo = !pz && z == 0, z_hi = !pz && z == d.nz - 1;
-        if (y_face || z_lo || z_hi) [[unlikely]] {
-            const float4 self = ld4(u + i);
-            if (gy_lo) c = ghost4(g, YM, self);
-            if (gy_hi) e = ghost4(g, YP, self);
-            if (z_lo) zm = ghost4(g, ZM, self);
-            if (z_hi) zp = ghost4(g, ZP, self);
-        }
-        const float xm0 = s_odd ? cur.x : ext, xm1 = s_odd ? cur.y : cur.x, xm2 = s_odd ? cur.z : cur.y, xm3 = s_odd ? cur.w : cur.z;
-        const float xp0 = s_odd ? cur.y : cur.x, xp1 = s_odd ? cur.z : cur.y, xp2 = s_odd ? cur.w : cur.z, xp3 = s_odd ? ext : cur.w;
-        float4 o;
-        o.x = vec_update<KIND>(xm0 + xp0 + c.x + e.x + zm.x + zp.x, r.x, coef, divisor, recip);
-        o.y = vec_update<KIND>(xm1 + xp1 + c.y + e.y + zm.y + zp.y, r.y, coef, divisor, recip);
-        o.z = vec_update<KIND>(xm2 + xp2 + c.z + e.z + zm.z + zp.z, r.z, coef, divisor, recip);
-        o.w = vec_update<KIND>(xm3 + xp3 + c.w + e.w + zm.w + zp.w, r.w, coef, divisor, recip);
-        *reinterpret_cast<float4*>(u + i) = o;
-        below = cur;
-        cur = above;
-    }
-}
-
-
 // ---- BF16 fields: 4 cells per thread (one 8-byte vector) ------------------
 // The diffusion fields of a BF16-storage context. Same march, ghosts, sum
 // order and division as the float4 kernels, in FP32 arithmetic on the
@@ -530,6 +412,164 @@ __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_bf16(__nv_bfloat16* __
 template <int KIND, int DEPTH = kBf16Depth>
 __global__ void __launch_bounds__(32 * kVecRows) k_rbgs_bf16(__nv_bfloat16* x, const __nv_bfloat16* __restrict__ rhs, float coef, int parity, int z_chunk, Dims d, GhostRule g) {
     march_bf16<KIND, true, DEPTH>(x, x, rhs, coef, parity, z_chunk, d, g);
+}
+
+// ---- red-black solves in the split layout (FP32 and BF16 fields) ----------
+// For an RBGS solve the iterate and the right-hand side are stored split by
+// colour: two arrays (red, black), each [nz][ny][nx / 2], holding in row
+// (y, z) the cells x = 2k + s, k = 0 .. nx/2 - 1, with s = (y + z) & 1 for
+// the red array and 1 - s for the black one (red: x + y + z even). A colour
+// update then reads only the other colour's array and the right-hand side of
+// its own colour, and writes its own array, all dense: 3 values moved per
+// updated cell, so 3 per cell per iteration, where a colour launch on the
+// interleaved field moves whole lines (3 per cell per colour). In the split
+// layout the six neighbours of the cell (x = 2k + s_u, y, z) of colour array
+// u are, in the other array v: k + s_u - 1 and k + s_u of the same row
+// (x - 1, x + 1), and k of rows y - 1, y + 1 and of planes z - 1, z + 1 (the
+// other colour's offset in an adjacent row is s_u, so the cell beside sits
+// at the same k). The update is the colour launch's: the same six values
+// summed in the reference's order (x-, x+, y-, y+, z-, z+), the same
+// numerator and exact division in FP32 (for BF16 storage: on the unpacked
+// values, rounded once to BF16 on the store), so every cell gets the same
+// bits. Face ghosts take the cell's own value from u (threads on a face read
+// their own four cells); periodic axes wrap k or the row (even sizes only:
+// an odd periodic size breaks the colouring and leaves the solve to the
+// colour launches).
+
+// Four consecutive cells as FP32, and back, for either element type.
+__device__ __forceinline__ float4 ld4v(const float* p) { return ld4(p); }
+__device__ __forceinline__ float4 ld4v(const __nv_bfloat16* p) { return unpack_bf4(ld_bf4(p)); }
+__device__ __forceinline__ float ld1v(const float* p) { return *p; }
+__device__ __forceinline__ float ld1v(const __nv_bfloat16* p) { return ld_bf1(p); }
+__device__ __forceinline__ void st4v(float* p, float4 o) { *reinterpret_cast<float4*>(p) = o; }
+__device__ __forceinline__ void st4v(__nv_bfloat16* p, float4 o) { *reinterpret_cast<uint2*>(p) = make_uint2(pack_bf2(o.x, o.y), pack_bf2(o.z, o.w)); }
+
+// Eight cells of a row split into four of each colour (lo: the even cells,
+// hi: the odd ones), or merged back; FP32 as float4 pairs, BF16 as the
+// 16-bit halves of four words (little endian: the even cell in the low half).
+struct Split8F { float4 even, odd; };
+__device__ __forceinline__ Split8F split8(const float* p) {
+    const float4 v0 = ld4(p), v1 = ld4(p + 4);
+    return {make_float4(v0.x, v0.z, v1.x, v1.z), make_float4(v0.y, v0.w, v1.y, v1.w)};
+}
+__device__ __forceinline__ void merge8(float* p, float4 even, float4 odd) {
+    *reinterpret_cast<float4*>(p) = make_float4(even.x, odd.x, even.y, odd.y);
+    *reinterpret_cast<float4*>(p + 4) = make_float4(even.z, odd.z, even.w, odd.w);
+}
+__device__ __forceinline__ void st4raw(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 ld4raw(const float* p) { return ld4(p); }
+
+struct Split8H { uint2 even, odd; };
+__device__ __forceinline__ Split8H split8(const __nv_bfloat16* p) {
+    const uint4 w = *reinterpret_cast<const uint4*>(p);
+    return {make_uint2(__byte_perm(w.x, w.y, 0x5410), __byte_perm(w.z, w.w, 0x5410)), make_uint2(__byte_perm(w.x, w.y, 0x7632), __byte_perm(w.z, w.w, 0x7632))};
+}
+__device__ __forceinline__ void merge8(__nv_bfloat16* p, uint2 even, uint2 odd) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(__byte_perm(even.x, odd.x, 0x5410), __byte_perm(even.x, odd.x, 0x7632), __byte_perm(even.y, odd.y, 0x5410), __byte_perm(even.y, odd.y, 0x7632));
+}
+__device__ __forceinline__ void st4raw(__nv_bfloat16* p, uint2 v) { *reinterpret_cast<uint2*>(p) = v; }
+__device__ __forceinline__ uint2 ld4raw(const __nv_bfloat16* p) { return ld_bf4(p); }
+__device__ __forceinline__ float4 scale4(float4 v, float f) { return make_float4(__fmul_rn(v.x, f), __fmul_rn(v.y, f), __fmul_rn(v.z, f), __fmul_rn(v.w, f)); }
+__device__ __forceinline__ uint2 scale4(uint2 v, float f) {
+    const float4 u = scale4(unpack_bf4(v), f);  // FP32 product rounded once to BF16, as k_scale_field
+    return make_uint2(pack_bf2(u.x, u.y), pack_bf2(u.z, u.w));
+}
+
+// Splits (or, with SPLIT false, merges and scales) a field: a thread moves
+// eight cells of a row and four of each colour array. `red2` / `black2`
+// (split only, may be null) receive a second copy.
+template <bool SPLIT, typename T>
+__global__ void __launch_bounds__(256) k_rb_layout(T* __restrict__ field, T* __restrict__ red, T* __restrict__ black, T* __restrict__ red2, T* __restrict__ black2, float scale, Dims d) {
+    const int per_row = d.nx / 8;
+    const size_t n8 = static_cast<size_t>(per_row) * d.ny * d.nz;
+    for (size_t f = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; f < n8; f += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t row = f / per_row;
+        const int y = static_cast<int>(row % d.ny), z = static_cast<int>(row / d.ny);
+        const bool odd = ((y + z) & 1) != 0;  // the row's red cells sit at odd x
+        if constexpr (SPLIT) {
+            const auto c = split8(field + 8 * f);
+            st4raw(red + 4 * f, odd ? c.odd : c.even);
+            st4raw(black + 4 * f, odd ? c.even : c.odd);
+            if (red2 != nullptr) {
+                st4raw(red2 + 4 * f, odd ? c.odd : c.even);
+                st4raw(black2 + 4 * f, odd ? c.even : c.odd);
+            }
+        } else {
+            auto r = ld4raw(red + 4 * f), b = ld4raw(black + 4 * f);
+            if (scale != 1.0f) {
+                r = scale4(r, scale);
+                b = scale4(b, scale);
+            }
+            if (odd) merge8(field + 8 * f, b, r);
+            else merge8(field + 8 * f, r, b);
+        }
+    }
+}
+
+// One colour of an RBGS iteration in the split layout, in place: u (the
+// colour's array) from v (the other colour's) and w (the right-hand side's
+// array of u's colour); `colour` 0 = red, 1 = black. A thread owns four
+// cells of a half row (k0 .. k0 + 3) and marches a z chunk with v's planes
+// below, at and above in registers; y neighbours and the extra x neighbour
+// come from L1. No thread reads another's cells of u, so the update is in
+// place. Threads are numbered along the half plane (blockIdx.x, 128 groups
+// of four a CTA; blockIdx.z the z chunk), so short rows still fill every
+// lane of a warp.
+template <int KIND, typename T>
+__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
+    const int hx = d.nx / 2, q4 = hx / 4;
+    const int j = static_cast<int>(blockIdx.x) * (32 * kVecRows) + static_cast<int>(threadIdx.y * 32 + threadIdx.x);
+    const int y = j / q4, k0 = 4 * (j - y * q4);
+    wait_for_previous_grid();
+    if (y >= d.ny) return;
+    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const bool px = g.periodic[0] != 0, py = g.periodic[1] != 0, pz = g.periodic[2] != 0;
+    const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
+    const double recip = tb::recip64(divisor);
+    const int hsz = hx * d.ny;
+    // rows y - 1, y + 1 (offsets in the half plane) and their face ghosts
+    const bool gy_lo = !py && y == 0, gy_hi = !py && y == d.ny - 1;
+    const int oy_lo = y > 0 ? -hx : (py ? (d.ny - 1) * hx : 0), oy_hi = y + 1 < d.ny ? hx : (py ? -(d.ny - 1) * hx : 0);
+    // the extra x neighbour: k0 - 1 (rows whose u cells sit at even x) or
+    // k0 + 4 (odd x), wrapped or replaced by a ghost at a face
+    const bool gx_lo = !px && k0 == 0, gx_hi = !px && k0 + 4 == hx;
+    const int ox_lo = k0 > 0 ? -1 : (px ? hx - 1 : 0), ox_hi = k0 + 4 < hx ? 4 : (px ? 4 - hx : 3);
+    // x faces: one cell of the thread (cell 0 on rows whose cells sit at even
+    // x, cell 3 on odd ones) takes its x ghost, from its own value in u;
+    // y faces (the whole row) and z faces (the whole plane) sit behind a
+    // branch interior threads skip, rather than selects every thread executes
+    const bool y_face = gy_lo || gy_hi;
+    const int off_up = pz ? -(d.nz - 1) * hsz : 0;  // plane z + 1 from the top plane (itself on a face)
+    int i = k0 + hx * (y + d.ny * zb);
+    float4 cur = ld4v(v + i);
+    float4 below = ld4v(v + i + (zb > 0 ? -hsz : (pz ? (d.nz - 1) * hsz : 0)));
+    for (int z = zb; z < ze; ++z, i += hsz) {
+        const float4 above = ld4v(v + i + (z + 1 < d.nz ? hsz : off_up));
+        const bool s_odd = ((y + z + colour) & 1) != 0;  // this row's cells of u sit at odd x
+        float ext = ld1v(v + i + (s_odd ? ox_hi : ox_lo));
+        float4 c = ld4v(v + i + oy_lo), e = ld4v(v + i + oy_hi);
+        const float4 r = ld4v(w + i);
+        if (s_odd ? gx_hi : gx_lo) ext = tb::ghost(g, s_odd ? XP : XM, ld1v(u + i + (s_odd ? 3 : 0)));
+        float4 zm = below, zp = above;
+        const bool z_lo = !pz && z == 0, z_hi = !pz && z == d.nz - 1;
+        if (y_face || z_lo || z_hi) [[unlikely]] {
+            const float4 self = ld4v(u + i);
+            if (gy_lo) c = ghost4(g, YM, self);
+            if (gy_hi) e = ghost4(g, YP, self);
+            if (z_lo) zm = ghost4(g, ZM, self);
+            if (z_hi) zp = ghost4(g, ZP, self);
+        }
+        const float xm0 = s_odd ? cur.x : ext, xm1 = s_odd ? cur.y : cur.x, xm2 = s_odd ? cur.z : cur.y, xm3 = s_odd ? cur.w : cur.z;
+        const float xp0 = s_odd ? cur.y : cur.x, xp1 = s_odd ? cur.z : cur.y, xp2 = s_odd ? cur.w : cur.z, xp3 = s_odd ? ext : cur.w;
+        float4 o;
+        o.x = vec_update<KIND>(xm0 + xp0 + c.x + e.x + zm.x + zp.x, r.x, coef, divisor, recip);
+        o.y = vec_update<KIND>(xm1 + xp1 + c.y + e.y + zm.y + zp.y, r.y, coef, divisor, recip);
+        o.z = vec_update<KIND>(xm2 + xp2 + c.z + e.z + zm.z + zp.z, r.z, coef, divisor, recip);
+        o.w = vec_update<KIND>(xm3 + xp3 + c.w + e.w + zm.w + zp.w, r.w, coef, divisor, recip);
+        st4v(u + i, o);
+        below = cur;
+        cur = above;
+    }
 }
 
 // Launch shape of the vectorised kernels: as many z chunks as fit the
@@ -766,54 +806,55 @@ bool odd_periodic(const StencilArgs& a) {
     return false;
 }
 
-// The split-layout red-black solve applies: FP32 field, rows of a multiple of
-// 8 cells (float4 of each colour array), both scratch buffers, no odd
-// periodic axis; per_pass 1 asks for the colour launches instead.
+// The split-layout red-black solve applies: rows of a multiple of 8 cells
+// (four of each colour a thread), both scratch buffers, no odd periodic
+// axis; per_pass 1 asks for the colour launches instead.
 bool rb_split_ok(const StencilArgs& a) {
-    if (a.bf16 || a.scratch == nullptr || a.scratch2 == nullptr || a.per_pass == 1 || a.iterations < 1) return false;
+    if (a.scratch == nullptr || a.scratch2 == nullptr || a.per_pass == 1 || a.iterations < 1) return false;
     if (a.dims.nx % 8 != 0 || !vec_ok(a) || (reinterpret_cast<uintptr_t>(a.scratch2) & 15) != 0) return false;
     return !odd_periodic(a);
 }
 
-template <bool SPLIT>
-cudaError_t launch_rb_layout(float* field, float* red, float* black, float* red2, float* black2, float scale, const Dims& d, cudaStream_t s) {
+template <bool SPLIT, typename T>
+cudaError_t launch_rb_layout(T* field, T* red, T* black, T* red2, T* black2, float scale, const Dims& d, cudaStream_t s) {
     const size_t n8 = static_cast<size_t>(d.nx / 8) * d.ny * d.nz;
     size_t blocks = (n8 + 255) / 256;
     if (blocks > 148u * 16u) blocks = 148u * 16u;
-    k_rb_layout<SPLIT><<<static_cast<unsigned>(blocks), 256, 0, s>>>(field, red, black, red2, black2, scale, d);
+    k_rb_layout<SPLIT, T><<<static_cast<unsigned>(blocks), 256, 0, s>>>(field, red, black, red2, black2, scale, d);
     return cudaGetLastError();
 }
 
 // The solve in the split layout: the right-hand side split into scratch2,
 // the iterate into scratch (from x, from b, or zero), the iterations as red
 // and black half launches, then the iterate merged back into x, times
-// out_scale.
-template <int KIND>
+// out_scale. T: the element type of x, b and both scratch buffers.
+template <int KIND, typename T>
 cudaError_t run_rb_split(const StencilArgs& a, cudaStream_t s) {
     const Dims& d = a.dims;
     const size_t half = static_cast<size_t>(d.nx) * d.ny * d.nz / 2;
-    float* const xr = a.scratch;
-    float* const xb = a.scratch + half;
-    float* const br = a.scratch2;
-    float* const bb = a.scratch2 + half;
+    T* const x = reinterpret_cast<T*>(a.x);
+    T* const xr = reinterpret_cast<T*>(a.scratch);
+    T* const xb = xr + half;
+    T* const br = reinterpret_cast<T*>(a.scratch2);
+    T* const bb = br + half;
     cudaError_t e = cudaSuccess;
     const bool from_b = a.init == INIT_FROM_B;
-    if ((e = launch_rb_layout<true>(const_cast<float*>(a.b), br, bb, from_b ? xr : nullptr, from_b ? xb : nullptr, 1.0f, d, s)) != cudaSuccess) return e;
+    if ((e = launch_rb_layout<true, T>(reinterpret_cast<T*>(const_cast<float*>(a.b)), br, bb, from_b ? xr : nullptr, from_b ? xb : nullptr, 1.0f, d, s)) != cudaSuccess) return e;
     int kernels = 2;  // the right-hand side's split and the final merge
     if (a.init == INIT_ZERO) {
-        if ((e = cudaMemsetAsync(a.scratch, 0, 2 * half * sizeof(float), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(xr, 0, 2 * half * sizeof(T), s)) != cudaSuccess) return e;
     } else if (a.init == INIT_FROM_X) {
-        if ((e = launch_rb_layout<true>(a.x, xr, xb, nullptr, nullptr, 1.0f, d, s)) != cudaSuccess) return e;
+        if ((e = launch_rb_layout<true, T>(x, xr, xb, nullptr, nullptr, 1.0f, d, s)) != cudaSuccess) return e;
         ++kernels;
     }
     const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
-    const auto kern = k_rb_half<KIND>;
+    const auto kern = k_rb_half<KIND, T>;
     const VecShape vs = plane_shape(d, kern, static_cast<long long>(d.nx / 8) * d.ny);
     for (int it = 0; it < a.iterations; ++it) {
-        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xr, static_cast<const float*>(xb), static_cast<const float*>(br), a.coef, 0, vs.z_chunk, d, g)) != cudaSuccess) return e;
-        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xb, static_cast<const float*>(xr), static_cast<const float*>(bb), a.coef, 1, vs.z_chunk, d, g)) != cudaSuccess) return e;
+        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xr, static_cast<const T*>(xb), static_cast<const T*>(br), a.coef, 0, vs.z_chunk, d, g)) != cudaSuccess) return e;
+        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xb, static_cast<const T*>(xr), static_cast<const T*>(bb), a.coef, 1, vs.z_chunk, d, g)) != cudaSuccess) return e;
     }
-    if ((e = launch_rb_layout<false>(a.x, xr, xb, nullptr, nullptr, a.out_scale, d, s)) != cudaSuccess) return e;
+    if ((e = launch_rb_layout<false, T>(x, xr, xb, nullptr, nullptr, a.out_scale, d, s)) != cudaSuccess) return e;
     if (a.launches) *a.launches += 2 * a.iterations + kernels;
     return cudaSuccess;
 }
@@ -830,8 +871,7 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
     const T* const ab = reinterpret_cast<const T*>(a.b);
     cudaError_t e = cudaSuccess;
     if (a.scheme == SCHEME_RBGS) {
-        if constexpr (sizeof(T) == sizeof(float))
-            if (rb_split_ok(a)) return run_rb_split<KIND>(a, s);
+        if (rb_split_ok(a)) return run_rb_split<KIND, T>(a, s);
         if (a.init == INIT_FROM_B) e = cudaMemcpyAsync(ax, ab, bytes, cudaMemcpyDeviceToDevice, s);
         else if (a.init == INIT_ZERO) e = cudaMemsetAsync(ax, 0, bytes, s);
         if (e != cudaSuccess) return e;

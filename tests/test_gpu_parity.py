@@ -440,6 +440,21 @@ def test_rbgs_split_matches_colour_launches(kind, sf, lib, ref_lib, cuda):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["narrow_8x9x7", "wide_512x11x9", "periodic_64x10x12"])
+def test_rbgs_split_bf16_matches_colour_launches(kind, sf, lib, cuda):
+    """BF16 storage: the split-layout diffusion solves give the bits of the
+    BF16 colour launches (FP32 arithmetic, one rounding to BF16 per update)."""
+    scene = _rb_split_scene(sf, kind)
+    outs = {}
+    for per_pass in (0, 1):
+        opts = sf.default_options(lib)
+        opts.storage = sf.STORAGE_BF16
+        opts.iterations_per_pass = per_pass
+        outs[per_pass] = _run_scene(sf, lib, scene, opts)
+    assert_bit_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["stam_128x44x37", "periodic_xz_256x12x10"])
 def test_wave_jacobi_matches_oracle(kind, sf, lib, orc, cuda):
     """The Jacobi scheme (numerator times the rounded reciprocal) against the
