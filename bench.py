@@ -80,9 +80,11 @@ METRIC = "steps/s at 256³: learned-warm-start vs plain Jacobi at equal ‖∇·
 CHECK_INTERVAL = 16
 CALIBRATION = ROOT / "bench_calibration.json"
 ITERATIONS_PER_PASS = 0  # set from --iterations-per-pass
-# DRAM bytes (read + write) of one Jacobi pressure pass from an ncu capture,
-# by grid size; filled from profiles/ once captured.
-PASS_TRAFFIC: dict[int, tuple[float, str]] = {}
+# DRAM bytes (read + write) of one single-sweep Jacobi pressure launch
+# (k_jacobi_vec4) from an ncu capture, by grid size.
+PASS_TRAFFIC: dict[int, tuple[float, str]] = {
+    256: (138.9e6 + 39.2e6, "profiles/k_jacobi_vec4_pressure_256.md: dram__bytes_read.sum + dram__bytes_write.sum of one launch"),
+}
 
 
 def parse():
@@ -828,7 +830,7 @@ def main():
     cells = n ** 3
     bytes_per_launch = 12 * cells
     achieved = bytes_per_launch / launch_s / 1e9
-    traffic = PASS_TRAFFIC.get(n)
+    traffic = PASS_TRAFFIC.get(n) if sweeps_per_launch == 1 else None
     kernel_name = "k_jacobi_vec4 (Jacobi pressure sweep)" if sweeps_per_launch == 1 else f"k_wave (Jacobi pressure pass, {sweeps_per_launch:g} sweeps per launch)"
     roofline = {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic[0] if traffic else None, "traffic_source": traffic[1] if traffic else None, "bytes_per_launch": bytes_per_launch, "launch_us": launch_s * 1e6,
