@@ -37,7 +37,8 @@ struct BatchSim {
     float* pressure;
     float* divergence;
     float* magnitude;
-    float* scratch;      // field-sized buffer of the Jacobi ping-pong
+    float* scratch;      // field-sized buffer of the Jacobi ping-pong; a red-black solve's split iterate
+    float* scratch2;     // a red-black solve's split right-hand side (null: none)
     float* sdata;        // the scalar field
     float* stemp;        // its advected copy (right-hand side of its diffusion)
     const float* source; // its source
@@ -46,13 +47,16 @@ struct BatchSim {
 };
 
 // Launch shapes: LINEAR = 256 cells per block; CELL = (32, 4, 2) blocks over
-// the grid; VEC = (32, 4) threads x 4 cells per thread over x, z_chunk planes.
-enum BatchShape : int32_t { SHAPE_LINEAR = 0, SHAPE_CELL = 1, SHAPE_VEC = 2 };
+// the grid; VEC = (32, 4) threads x 4 cells per thread over x, z_chunk planes;
+// HALF = 128 groups of 4 cells of a colour-split half plane per block,
+// z_chunk planes; OCT = 256 groups of 8 cells per block.
+enum BatchShape : int32_t { SHAPE_LINEAR = 0, SHAPE_CELL = 1, SHAPE_VEC = 2, SHAPE_HALF = 3, SHAPE_OCT = 4 };
+constexpr int kBatchShapes = 5;
 
 struct BatchTable {
     const BatchSim* sims;      // device array, nsims entries
-    const uint32_t* first[3];  // device arrays per BatchShape, nsims + 1 entries
-    uint32_t total[3];         // work items per BatchShape
+    const uint32_t* first[kBatchShapes];  // device arrays per BatchShape, nsims + 1 entries
+    uint32_t total[kBatchShapes];         // work items per BatchShape
     int32_t nsims;
     int32_t sms;               // multiprocessors of the device
 };
@@ -77,6 +81,15 @@ cudaError_t launch_batch_copy(const BatchTable& t, int kind, int dst, int src, c
 cudaError_t launch_batch_scale_scalar(const BatchTable& t, cudaStream_t s);
 // One RBGS colour (scheme RBGS, in place on X) or one Jacobi sweep dst <- update(src).
 cudaError_t launch_batch_sweep(const BatchTable& t, int kind, int scheme, int parity, int dst, int src, cudaStream_t s);
+// Red-black solves in the colour-split layout (every simulation with a
+// scratch2 buffer, rows of a multiple of 8 cells, even periodic sizes):
+// split `which` (BF_B into scratch2 and, with copy_iterate, also into scratch
+// as the starting iterate; BF_X into scratch), one colour of an iteration,
+// and the merge of scratch into BF_X (times the scalar dissipation factor
+// when `dissipate`).
+cudaError_t launch_batch_rb_split(const BatchTable& t, int kind, int which, int copy_iterate, cudaStream_t s);
+cudaError_t launch_batch_rb_half(const BatchTable& t, int kind, int colour, cudaStream_t s);
+cudaError_t launch_batch_rb_merge(const BatchTable& t, int kind, int dissipate, cudaStream_t s);
 // Per simulation: zero its residual sums (finalize 0) or turn them into
 // rel_res with the iteration count (finalize 1).
 cudaError_t launch_batch_stats(const BatchTable& t, int finalize, int iterations, cudaStream_t s);

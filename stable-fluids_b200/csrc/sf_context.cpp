@@ -942,6 +942,7 @@ struct Batch {
     int chains = 1;                              // groups captured round-robin on this many concurrent streams
     std::vector<cudaStream_t> chain_streams;     // chains - 1 extra capture streams
     std::vector<cudaEvent_t> chain_events;       // fork + one join event per extra stream
+    bool rb_split = false;                       // red-black solves in the colour-split layout
 
     ~Batch() {
         for (auto ev : chain_events) cudaEventDestroy(ev);
@@ -1009,6 +1010,7 @@ BatchSim make_batch_sim(const Context& c, int z_chunk) {
     m.divergence = c.divergence;
     m.magnitude = c.magnitude;
     m.scratch = c.scratch;
+    m.scratch2 = c.scratch2;
     m.sdata = f.data;
     m.stemp = f.temp;
     m.source = f.source;
@@ -1025,16 +1027,16 @@ BatchSim make_batch_sim(const Context& c, int z_chunk) {
 cudaError_t upload_table(Batch& b) {
     const int n = static_cast<int>(b.sims.size());
     const int ng = static_cast<int>(b.groups.size());
-    std::vector<uint32_t> first(3 * static_cast<size_t>(n + ng));
+    std::vector<uint32_t> first(kBatchShapes * static_cast<size_t>(n + ng));
     b.tables.assign(ng, BatchTable{});
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     size_t at = 0;
-    std::vector<size_t> offset(3 * static_cast<size_t>(ng));
+    std::vector<size_t> offset(kBatchShapes * static_cast<size_t>(ng));
     for (int g = 0; g < ng; ++g) {
         const auto [lo, hi] = b.groups[g];
-        for (int shape = 0; shape < 3; ++shape) {
-            offset[3 * g + shape] = at;
+        for (int shape = 0; shape < kBatchShapes; ++shape) {
+            offset[kBatchShapes * g + shape] = at;
             uint32_t acc = 0;
             for (int i = lo; i < hi; ++i) {
                 first[at++] = acc;
@@ -1053,7 +1055,7 @@ cudaError_t upload_table(Batch& b) {
     for (int g = 0; g < ng; ++g) {
         auto& t = b.tables[g];
         t.sims = b.d_sims + b.groups[g].first;
-        for (int shape = 0; shape < 3; ++shape) t.first[shape] = b.d_first + offset[3 * g + shape];
+        for (int shape = 0; shape < kBatchShapes; ++shape) t.first[shape] = b.d_first + offset[kBatchShapes * g + shape];
         t.nsims = b.groups[g].second - b.groups[g].first;
         t.sms = sms;
     }
@@ -1239,8 +1241,24 @@ struct BatchStages {
         else if (e == cudaSuccess) e = x;
     }
 
-    // One solve: the buffer sequence of run_simple (no temporal blocking).
-    void solve(int kind, int init, int iterations) {
+    // One solve: the buffer sequence of run_simple (no temporal blocking);
+    // `dissipate`: multiply the scalar by its dissipation factor afterwards.
+    void solve(int kind, int init, int iterations, bool dissipate = false) {
+        if (r.options.scheme == STABLE_FLUIDS_B200_SCHEME_RBGS && b.rb_split && iterations > 0) {
+            // colour-split layout (run_rb_split); the merge applies the dissipation
+            ok(launch_batch_rb_split(t, kind, BF_B, init == INIT_FROM_B ? 1 : 0, s));
+            if (init == INIT_ZERO) ok(launch_batch_copy(t, kind, BF_SCRATCH, -1, s));
+            else if (init == INIT_FROM_X) ok(launch_batch_rb_split(t, kind, BF_X, 0, s));
+            for (int it = 0; it < iterations; ++it)
+                for (int colour = 0; colour < 2; ++colour) ok(launch_batch_rb_half(t, kind, colour, s));
+            ok(launch_batch_rb_merge(t, kind, dissipate ? 1 : 0, s));
+            return;
+        }
+        solve_plain(kind, init, iterations);
+        if (dissipate) ok(launch_batch_scale_scalar(t, s));
+    }
+
+    void solve_plain(int kind, int init, int iterations) {
         if (r.options.scheme == STABLE_FLUIDS_B200_SCHEME_RBGS) {
             if (init == INIT_FROM_B) ok(launch_batch_copy(t, kind, BF_X, BF_B, s));
             else if (init == INIT_ZERO) ok(launch_batch_copy(t, kind, BF_X, -1, s));
@@ -1283,8 +1301,7 @@ struct BatchStages {
             ok(launch_batch_stats(t, 1, pressure, s));
         }
         ok(launch_batch_scalar_source_advect(t, s));
-        solve(KIND_SCALAR, INIT_FROM_B, diffuse);
-        if (r.scalars[0].desc.dissipation > 0.0f) ok(launch_batch_scale_scalar(t, s));
+        solve(KIND_SCALAR, INIT_FROM_B, diffuse, r.scalars[0].desc.dissipation > 0.0f);
         ok(launch_batch_post_diagnostics(t, s));
         return e;
     }
@@ -1302,6 +1319,15 @@ cudaError_t build_work_table(Batch& b, bool autotune, const char* cache_path, in
         cudaEvent_t ev = nullptr;
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
         b.chain_events.push_back(ev);
+    }
+    // red-black solves in the colour-split layout when every simulation allows it
+    b.rb_split = true;
+    for (const Context* c : b.contexts) {
+        const ScalarBC& sb = c->scalars[0].bc;
+        const int n[3] = {c->dims.nx, c->dims.ny, c->dims.nz};
+        bool ok = c->scratch2 != nullptr && c->dims.nx % 8 == 0;
+        for (int k = 0; k < 3; ++k) ok = ok && !((c->flow.periodic[k] || sb.periodic[k]) && (n[k] & 1));
+        b.rb_split = b.rb_split && ok;
     }
     group_by_l2(b, [&](int i) { return make_batch_sim(*b.contexts[i], std::min(kDefaultZChunk, b.contexts[i]->dims.nz)); });
     e = autotune ? tune_tiles(b, cache_path) : upload_table(b);

@@ -723,9 +723,12 @@ uint32_t batch_blocks(const Dims& d, int shape, int z_chunk) {
         const dim3 g = cell_grid(d);
         return g.x * g.y * g.z;
     }
-    const uint32_t bx = static_cast<uint32_t>((d.nx / 4 + 31) / 32), by = static_cast<uint32_t>((d.ny + 3) / 4);
     const uint32_t zc = static_cast<uint32_t>(z_chunk < 1 ? 1 : z_chunk);
-    return bx * by * ((static_cast<uint32_t>(d.nz) + zc - 1) / zc);
+    const uint32_t chunks = (static_cast<uint32_t>(d.nz) + zc - 1) / zc;
+    if (shape == SHAPE_HALF) return static_cast<uint32_t>((static_cast<size_t>(d.nx / 8) * d.ny + 127) / 128) * chunks;
+    if (shape == SHAPE_OCT) return static_cast<uint32_t>((static_cast<size_t>(d.nx / 8) * d.ny * d.nz + 255) / 256);
+    const uint32_t bx = static_cast<uint32_t>((d.nx / 4 + 31) / 32), by = static_cast<uint32_t>((d.ny + 3) / 4);
+    return bx * by * chunks;
 }
 
 cudaError_t launch_restrict2(const float* fine, float* coarse, Dims fine_dims, cudaStream_t s) {

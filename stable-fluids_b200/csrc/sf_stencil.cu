@@ -475,35 +475,38 @@ __device__ __forceinline__ uint2 scale4(uint2 v, float f) {
     return make_uint2(pack_bf2(u.x, u.y), pack_bf2(u.z, u.w));
 }
 
+template <bool SPLIT, typename T>
+__device__ __forceinline__ void rb_layout_group(size_t f, T* __restrict__ field, T* __restrict__ red, T* __restrict__ black, T* __restrict__ red2, T* __restrict__ black2, float scale, const Dims& d) {
+    const int per_row = d.nx / 8;
+    const size_t row = f / per_row;
+    const int y = static_cast<int>(row % d.ny), z = static_cast<int>(row / d.ny);
+    const bool odd = ((y + z) & 1) != 0;  // the row's red cells sit at odd x
+    if constexpr (SPLIT) {
+        const auto c = split8(field + 8 * f);
+        st4raw(red + 4 * f, odd ? c.odd : c.even);
+        st4raw(black + 4 * f, odd ? c.even : c.odd);
+        if (red2 != nullptr) {
+            st4raw(red2 + 4 * f, odd ? c.odd : c.even);
+            st4raw(black2 + 4 * f, odd ? c.even : c.odd);
+        }
+    } else {
+        auto r = ld4raw(red + 4 * f), b = ld4raw(black + 4 * f);
+        if (scale != 1.0f) {
+            r = scale4(r, scale);
+            b = scale4(b, scale);
+        }
+        if (odd) merge8(field + 8 * f, b, r);
+        else merge8(field + 8 * f, r, b);
+    }
+}
+
 // Splits (or, with SPLIT false, merges and scales) a field: a thread moves
-// eight cells of a row and four of each colour array. `red2` / `black2`
-// (split only, may be null) receive a second copy.
+// eight cells of a row (a group f) and four of each colour array. `red2` /
+// `black2` (split only, may be null) receive a second copy.
 template <bool SPLIT, typename T>
 __global__ void __launch_bounds__(256) k_rb_layout(T* __restrict__ field, T* __restrict__ red, T* __restrict__ black, T* __restrict__ red2, T* __restrict__ black2, float scale, Dims d) {
-    const int per_row = d.nx / 8;
-    const size_t n8 = static_cast<size_t>(per_row) * d.ny * d.nz;
-    for (size_t f = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; f < n8; f += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const size_t row = f / per_row;
-        const int y = static_cast<int>(row % d.ny), z = static_cast<int>(row / d.ny);
-        const bool odd = ((y + z) & 1) != 0;  // the row's red cells sit at odd x
-        if constexpr (SPLIT) {
-            const auto c = split8(field + 8 * f);
-            st4raw(red + 4 * f, odd ? c.odd : c.even);
-            st4raw(black + 4 * f, odd ? c.even : c.odd);
-            if (red2 != nullptr) {
-                st4raw(red2 + 4 * f, odd ? c.odd : c.even);
-                st4raw(black2 + 4 * f, odd ? c.even : c.odd);
-            }
-        } else {
-            auto r = ld4raw(red + 4 * f), b = ld4raw(black + 4 * f);
-            if (scale != 1.0f) {
-                r = scale4(r, scale);
-                b = scale4(b, scale);
-            }
-            if (odd) merge8(field + 8 * f, b, r);
-            else merge8(field + 8 * f, r, b);
-        }
-    }
+    const size_t n8 = static_cast<size_t>(d.nx / 8) * d.ny * d.nz;
+    for (size_t f = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; f < n8; f += static_cast<size_t>(gridDim.x) * blockDim.x) rb_layout_group<SPLIT, T>(f, field, red, black, red2, black2, scale, d);
 }
 
 // One colour of an RBGS iteration in the split layout, in place: u (the
@@ -516,13 +519,12 @@ __global__ void __launch_bounds__(256) k_rb_layout(T* __restrict__ field, T* __r
 // of four a CTA; blockIdx.z the z chunk), so short rows still fill every
 // lane of a warp.
 template <int KIND, typename T>
-__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
+__device__ __forceinline__ void rb_half_block(uint32_t bx, uint32_t bz, T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, const Dims& d, const GhostRule& g) {
     const int hx = d.nx / 2, q4 = hx / 4;
-    const int j = static_cast<int>(blockIdx.x) * (32 * kVecRows) + static_cast<int>(threadIdx.y * 32 + threadIdx.x);
+    const int j = static_cast<int>(bx) * (32 * kVecRows) + static_cast<int>(threadIdx.y * 32 + threadIdx.x);
     const int y = j / q4, k0 = 4 * (j - y * q4);
-    wait_for_previous_grid();
     if (y >= d.ny) return;
-    const int zb = static_cast<int>(blockIdx.z) * z_chunk, ze = min(zb + z_chunk, d.nz);
+    const int zb = static_cast<int>(bz) * z_chunk, ze = min(zb + z_chunk, d.nz);
     const bool px = g.periodic[0] != 0, py = g.periodic[1] != 0, pz = g.periodic[2] != 0;
     const float divisor = KIND == KIND_PRESSURE ? 6.0f : 1.0f + 6.0f * coef;
     const double recip = tb::recip64(divisor);
@@ -570,6 +572,12 @@ __global__ void __launch_bounds__(32 * kVecRows) k_rb_half(T* u, const T* __rest
         below = cur;
         cur = above;
     }
+}
+
+template <int KIND, typename T>
+__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
+    wait_for_previous_grid();
+    rb_half_block<KIND, T>(blockIdx.x, blockIdx.z, u, v, w, coef, colour, z_chunk, d, g);
 }
 
 // Launch shape of the vectorised kernels: as many z chunks as fit the
@@ -1262,6 +1270,45 @@ __global__ void __launch_bounds__(256) k_batch_scale_scalar(BatchTable t) {
     }
 }
 
+// Colour-split red-black solves over the work table (rb_layout_group and
+// rb_half_block per work item; the split buffers are the simulation's scratch
+// and scratch2, red half first).
+__global__ void __launch_bounds__(256) k_batch_rb_layout(BatchTable t, int kind, int which, int copy_iterate, int merge, int dissipate) {
+    const uint32_t* first = t.first[SHAPE_OCT];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_OCT]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const size_t n8 = static_cast<size_t>(m.d.nx / 8) * m.d.ny * m.d.nz, half = 4 * n8;
+        const size_t f = static_cast<size_t>(w - first[si]) * 256u + threadIdx.x;
+        if (f >= n8) continue;
+        if (merge) {
+            rb_layout_group<false, float>(f, batch_field(m, kind, BF_X), m.scratch, m.scratch + half, nullptr, nullptr, dissipate ? m.scale_s : 1.0f, m.d);
+        } else {
+            float* const dst = which == BF_B ? m.scratch2 : m.scratch;
+            float* const dst2 = (which == BF_B && copy_iterate) ? m.scratch : nullptr;
+            rb_layout_group<true, float>(f, batch_field(m, kind, which), dst, dst + half, dst2, dst2 != nullptr ? dst2 + half : nullptr, 1.0f, m.d);
+        }
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(32 * kVecRows) k_batch_rb_half(BatchTable t, int colour) {
+    const uint32_t* first = t.first[SHAPE_HALF];
+    for (uint32_t w = blockIdx.x; w < t.total[SHAPE_HALF]; w += gridDim.x) {
+        const int si = batch_sim(first, t.nsims, w);
+        const BatchSim& m = t.sims[si];
+        const float coef = KIND == KIND_PRESSURE ? m.h * m.h : (KIND == KIND_SCALAR ? m.alpha_s : m.alpha_v);
+        const uint32_t bxy = static_cast<uint32_t>((static_cast<size_t>(m.d.nx / 8) * m.d.ny + 127) / 128);
+        const uint32_t local = w - first[si];
+        const size_t half = static_cast<size_t>(m.d.nx) * m.d.ny * m.d.nz / 2;
+        float* const xr = m.scratch;
+        float* const xb = m.scratch + half;
+        const float* const br = m.scratch2;
+        const float* const bb = m.scratch2 + half;
+        rb_half_block<KIND, float>(local % bxy, local / bxy, colour ? xb : xr, colour ? xr : xb, colour ? bb : br, coef, colour, m.z_chunk, m.d, m.ghost[KIND]);
+    }
+}
+
 template <typename Kernel>
 unsigned batch_grid_vec(uint32_t total, int sms, Kernel kernel) {
     static int per_sm = [&] {
@@ -1370,6 +1417,33 @@ cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
 
 // ------------------------------------------------------ work-table batch --
 GhostRule make_ghost_rule(int kind, const FlowBC& fb, const ScalarBC& sb) { return ghost_rule(kind, fb, sb); }
+
+cudaError_t launch_batch_rb_split(const BatchTable& t, int kind, int which, int copy_iterate, cudaStream_t s) {
+    k_batch_rb_layout<<<batch_grid_linear(t.total[SHAPE_OCT], t.sms), 256, 0, s>>>(t, kind, which, copy_iterate, 0, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_rb_merge(const BatchTable& t, int kind, int dissipate, cudaStream_t s) {
+    k_batch_rb_layout<<<batch_grid_linear(t.total[SHAPE_OCT], t.sms), 256, 0, s>>>(t, kind, BF_X, 0, 1, dissipate);
+    return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t batch_rb_half(const BatchTable& t, int colour, cudaStream_t s) {
+    k_batch_rb_half<KIND><<<batch_grid_vec(t.total[SHAPE_HALF], t.sms, k_batch_rb_half<KIND>), dim3(32, kVecRows), 0, s>>>(t, colour);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_rb_half(const BatchTable& t, int kind, int colour, cudaStream_t s) {
+    switch (kind) {
+    case KIND_VEL_X: return batch_rb_half<KIND_VEL_X>(t, colour, s);
+    case KIND_VEL_Y: return batch_rb_half<KIND_VEL_Y>(t, colour, s);
+    case KIND_VEL_Z: return batch_rb_half<KIND_VEL_Z>(t, colour, s);
+    case KIND_SCALAR: return batch_rb_half<KIND_SCALAR>(t, colour, s);
+    case KIND_PRESSURE: return batch_rb_half<KIND_PRESSURE>(t, colour, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_batch_sweep(const BatchTable& t, int kind, int scheme, int parity, int dst, int src, cudaStream_t s) {
     switch (kind) {
