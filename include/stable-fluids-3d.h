@@ -6,7 +6,10 @@
  * struct field order, field type and exported function signature is the same,
  * so a caller compiled against the upstream header (benchmark.cu, the Vulkan
  * viewer) links against libstable-fluids.so from this project unchanged.
- * tests/test_abi.py checks the layout field by field.
+ * tests/test_abi.py checks the layout field by field. The declarations below
+ * (enums, structs, signatures, the STABLE_FLUIDS_API visibility block) are
+ * therefore the upstream file's, which is distributed under the Mozilla Public
+ * License 2.0; the comments are this project's.
  *
  * Semantics (all functions are asynchronous on the context stream):
  *   - update_* take DEVICE pointers (host pointers are also accepted: the copy
