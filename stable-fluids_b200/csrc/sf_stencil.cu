@@ -183,8 +183,11 @@ __device__ __forceinline__ float4 vec_above4(const float* x, int i, int z, const
 
 
 // One Jacobi sweep dst = update(src), block `blk` of the launch (blockIdx
-// for one simulation, the work item's block in a batch).
-template <int KIND>
+// for one simulation, the work item's block in a batch). DOWN marches the
+// chunk from its top plane down: a sweep that runs opposite to the one
+// before starts on the planes that sweep wrote last, which are still in L2
+// (the values are the same either way: a Jacobi sweep reads only src).
+template <int KIND, bool DOWN = false>
 __device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, const Dims& d, const GhostRule& g) {
     const int x0 = 4 * static_cast<int>(blk.x * 32 + threadIdx.x), y = static_cast<int>(blk.y * kVecRows + threadIdx.y);
     if (x0 >= d.nx || y >= d.ny) return;
@@ -192,12 +195,8 @@ __device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__
     const float inv = wave::jacobi_inverse(KIND, coef);
     const VecGhost4 v = vec_ghost4(x0, y, d, g);
     const int sz = d.nx * d.ny;
-    int i = x0 + d.nx * (y + d.ny * zb);
-    float4 cur = ld4(src + i);
-    float4 below = vec_below4(src, i, zb, d, g, cur);
-#pragma unroll 2
-    for (int z = zb; z < ze; ++z, i += sz) {
-        const float4 above = vec_above4(src, i, z, d, g, cur);
+    // the update of plane z at index i from its planes below / at / above
+    const auto plane = [&](int i, float4 below, float4 cur, float4 above) {
         float a = src[i + v.ox_lo], b = src[i + v.ox_hi];
         float4 c = ld4(src + i + v.oy_lo), e = ld4(src + i + v.oy_hi);
         const float4 r = ld4(rhs + i);
@@ -211,8 +210,29 @@ __device__ __forceinline__ void jacobi_vec4_block(uint3 blk, float* __restrict__
         o.z = wave::jacobi_update<KIND>(cur.y + cur.w + c.z + e.z + below.z + above.z, r.z, coef, inv);
         o.w = wave::jacobi_update<KIND>(cur.z + b + c.w + e.w + below.w + above.w, r.w, coef, inv);
         *reinterpret_cast<float4*>(dst + i) = o;
-        below = cur;
-        cur = above;
+    };
+    if constexpr (!DOWN) {
+        int i = x0 + d.nx * (y + d.ny * zb);
+        float4 cur = ld4(src + i);
+        float4 below = vec_below4(src, i, zb, d, g, cur);
+#pragma unroll 2
+        for (int z = zb; z < ze; ++z, i += sz) {
+            const float4 above = vec_above4(src, i, z, d, g, cur);
+            plane(i, below, cur, above);
+            below = cur;
+            cur = above;
+        }
+    } else {
+        int i = x0 + d.nx * (y + d.ny * (ze - 1));
+        float4 cur = ld4(src + i);
+        float4 above = vec_above4(src, i, ze - 1, d, g, cur);
+#pragma unroll 2
+        for (int z = ze - 1; z >= zb; --z, i -= sz) {
+            const float4 below = vec_below4(src, i, z, d, g, cur);
+            plane(i, below, cur, above);
+            above = cur;
+            cur = below;
+        }
     }
 }
 
@@ -261,10 +281,10 @@ __device__ __forceinline__ void rbgs_vec4_block(uint3 blk, float* x, const float
 // attribute the wait returns at once.
 __device__ __forceinline__ void wait_for_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
-template <int KIND>
+template <int KIND, bool DOWN = false>
 __global__ void __launch_bounds__(32 * kVecRows) k_jacobi_vec4(float* __restrict__ dst, const float* __restrict__ src, const float* __restrict__ rhs, float coef, int z_chunk, Dims d, GhostRule g) {
     wait_for_previous_grid();
-    jacobi_vec4_block<KIND>(blockIdx, dst, src, rhs, coef, z_chunk, d, g);
+    jacobi_vec4_block<KIND, DOWN>(blockIdx, dst, src, rhs, coef, z_chunk, d, g);
 }
 
 template <int KIND>
@@ -519,7 +539,7 @@ __global__ void __launch_bounds__(256) k_rb_layout(T* __restrict__ field, T* __r
 // of four a CTA; blockIdx.z the z chunk), so short rows still fill every
 // lane of a warp.
 template <int KIND, typename T>
-__device__ __forceinline__ void rb_half_block(uint32_t bx, uint32_t bz, T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, const Dims& d, const GhostRule& g) {
+__device__ __forceinline__ void rb_half_block(uint32_t bx, uint32_t bz, T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, const Dims& d, const GhostRule& g, bool down = false) {
     const int hx = d.nx / 2, q4 = hx / 4;
     const int j = static_cast<int>(bx) * (32 * kVecRows) + static_cast<int>(threadIdx.y * 32 + threadIdx.x);
     const int y = j / q4, k0 = 4 * (j - y * q4);
@@ -542,11 +562,8 @@ __device__ __forceinline__ void rb_half_block(uint32_t bx, uint32_t bz, T* u, co
     // branch interior threads skip, rather than selects every thread executes
     const bool y_face = gy_lo || gy_hi;
     const int off_up = pz ? -(d.nz - 1) * hsz : 0;  // plane z + 1 from the top plane (itself on a face)
-    int i = k0 + hx * (y + d.ny * zb);
-    float4 cur = ld4v(v + i);
-    float4 below = ld4v(v + i + (zb > 0 ? -hsz : (pz ? (d.nz - 1) * hsz : 0)));
-    for (int z = zb; z < ze; ++z, i += hsz) {
-        const float4 above = ld4v(v + i + (z + 1 < d.nz ? hsz : off_up));
+    const int off_dn = pz ? (d.nz - 1) * hsz : 0;   // plane z - 1 from the bottom plane
+    const auto update = [&](int z, int i, float4 below, float4 cur, float4 above) {
         const bool s_odd = ((y + z + colour) & 1) != 0;  // this row's cells of u sit at odd x
         float ext = ld1v(v + i + (s_odd ? ox_hi : ox_lo));
         float4 c = ld4v(v + i + oy_lo), e = ld4v(v + i + oy_hi);
@@ -569,15 +586,35 @@ __device__ __forceinline__ void rb_half_block(uint32_t bx, uint32_t bz, T* u, co
         o.z = vec_update<KIND>(xm2 + xp2 + c.z + e.z + zm.z + zp.z, r.z, coef, divisor, recip);
         o.w = vec_update<KIND>(xm3 + xp3 + c.w + e.w + zm.w + zp.w, r.w, coef, divisor, recip);
         st4v(u + i, o);
-        below = cur;
-        cur = above;
+    };
+    // DOWN marches the chunk from its top plane (see jacobi_vec4_block)
+    if (!down) {
+        int i = k0 + hx * (y + d.ny * zb);
+        float4 cur = ld4v(v + i);
+        float4 below = ld4v(v + i + (zb > 0 ? -hsz : off_dn));
+        for (int z = zb; z < ze; ++z, i += hsz) {
+            const float4 above = ld4v(v + i + (z + 1 < d.nz ? hsz : off_up));
+            update(z, i, below, cur, above);
+            below = cur;
+            cur = above;
+        }
+    } else {
+        int i = k0 + hx * (y + d.ny * (ze - 1));
+        float4 cur = ld4v(v + i);
+        float4 above = ld4v(v + i + (ze < d.nz ? hsz : off_up));
+        for (int z = ze - 1; z >= zb; --z, i -= hsz) {
+            const float4 below = ld4v(v + i + (z > 0 ? -hsz : off_dn));
+            update(z, i, below, cur, above);
+            above = cur;
+            cur = below;
+        }
     }
 }
 
 template <int KIND, typename T>
-__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g) {
+__global__ void __launch_bounds__(32 * kVecRows) k_rb_half(T* u, const T* __restrict__ v, const T* __restrict__ w, float coef, int colour, int z_chunk, Dims d, GhostRule g, int down) {
     wait_for_previous_grid();
-    rb_half_block<KIND, T>(blockIdx.x, blockIdx.z, u, v, w, coef, colour, z_chunk, d, g);
+    rb_half_block<KIND, T>(blockIdx.x, blockIdx.z, u, v, w, coef, colour, z_chunk, d, g, down != 0);
 }
 
 // Launch shape of the vectorised kernels: as many z chunks as fit the
@@ -858,9 +895,11 @@ cudaError_t run_rb_split(const StencilArgs& a, cudaStream_t s) {
     const GhostRule g = ghost_rule(KIND, a.flow, a.scalar);
     const auto kern = k_rb_half<KIND, T>;
     const VecShape vs = plane_shape(d, kern, static_cast<long long>(d.nx / 8) * d.ny);
+    // the two colours march their z chunks in opposite directions, so each
+    // launch starts on the planes the one before wrote last (still in L2)
     for (int it = 0; it < a.iterations; ++it) {
-        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xr, static_cast<const T*>(xb), static_cast<const T*>(br), a.coef, 0, vs.z_chunk, d, g)) != cudaSuccess) return e;
-        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xb, static_cast<const T*>(xr), static_cast<const T*>(bb), a.coef, 1, vs.z_chunk, d, g)) != cudaSuccess) return e;
+        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xr, static_cast<const T*>(xb), static_cast<const T*>(br), a.coef, 0, vs.z_chunk, d, g, 0)) != cudaSuccess) return e;
+        if ((e = launch_sweep(kern, vs.grid, dim3(32, kVecRows), s, xb, static_cast<const T*>(xr), static_cast<const T*>(bb), a.coef, 1, vs.z_chunk, d, g, 1)) != cudaSuccess) return e;
     }
     if ((e = launch_rb_layout<false, T>(x, xr, xb, nullptr, nullptr, a.out_scale, d, s)) != cudaSuccess) return e;
     if (a.launches) *a.launches += 2 * a.iterations + kernels;
@@ -926,7 +965,8 @@ cudaError_t run_simple(const StencilArgs& a, cudaStream_t s) {
             T* dst = (left & 1) ? ax : ascr;
             if (dst == src) dst = (dst == ax) ? ascr : ax;
             if (vec) {
-                if constexpr (sizeof(T) == sizeof(float)) launch_sweep(jacobi_vec, vs.grid, dim3(32, kVecRows), s, dst, static_cast<const T*>(src), ab, a.coef, vs.z_chunk, d, g);
+                // consecutive sweeps march their z chunks in opposite directions (the last one upward)
+                if constexpr (sizeof(T) == sizeof(float)) launch_sweep((left - 1) & 1 ? k_jacobi_vec4<KIND, true> : k_jacobi_vec4<KIND>, vs.grid, dim3(32, kVecRows), s, dst, static_cast<const T*>(src), ab, a.coef, vs.z_chunk, d, g);
                 else jacobi_vec<<<vs.grid, dim3(32, kVecRows), 0, s>>>(dst, src, ab, a.coef, vs.z_chunk, d, g);
             } else {
                 k_jacobi<KIND, T><<<grid, jblock, 0, s>>>(dst, src, ab, a.coef, d, a.flow, a.scalar);
@@ -1349,7 +1389,9 @@ bool launch_pressure_interval_fused(const StencilArgs& a, DeviceStats* stats, cu
             cudaMemcpyAsync(a.scratch, a.x, bytes, cudaMemcpyDeviceToDevice, s);
             src = a.scratch;
         }
-        if (u + 1 < units) launch_sweep(k_jacobi_vec4<KIND_PRESSURE>, vs.grid, dim3(32, kVecRows), s, dst, src, a.b, a.coef, vs.z_chunk, d, g);
+        // directions alternate, the last (residual) sweep upward, so each sweep
+        // starts on the planes the one before wrote last (still in L2)
+        if (u + 1 < units) launch_sweep((units - 1 - u) & 1 ? k_jacobi_vec4<KIND_PRESSURE, true> : k_jacobi_vec4<KIND_PRESSURE>, vs.grid, dim3(32, kVecRows), s, dst, src, a.b, a.coef, vs.z_chunk, d, g);
         else launch_sweep(k_jacobi_vec4_residual, rs.grid, dim3(32, kVecRows), s, dst, src, a.b, a.coef, rs.z_chunk, d, g, stats);
         src = dst;
     }
