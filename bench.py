@@ -81,9 +81,10 @@ CHECK_INTERVAL = 16
 CALIBRATION = ROOT / "bench_calibration.json"
 ITERATIONS_PER_PASS = 0  # set from --iterations-per-pass
 # DRAM bytes (read + write) of one single-sweep Jacobi pressure launch
-# (k_jacobi_vec4) from an ncu capture, by grid size.
+# (k_jacobi_vec4, consecutive launches in alternating z directions, caches
+# kept warm between launches) from an ncu capture, by grid size.
 PASS_TRAFFIC: dict[int, tuple[float, str]] = {
-    256: (138.9e6 + 39.2e6, "profiles/k_jacobi_vec4_pressure_256.md: dram__bytes_read.sum + dram__bytes_write.sum of one launch"),
+    256: (84.9e6 + 66.4e6, "profiles/k_jacobi_vec4_pressure_256.md: dram__bytes_read.sum + dram__bytes_write.sum, mean of four consecutive launches with --cache-control none"),
 }
 
 
