@@ -383,10 +383,15 @@ def network_flops(n):
 def e2e_run(sf, scene, args, steps, device, net):
     """The learned variant through the public ABI with host buffers, on a
     fresh context replaying the device-timed run's steps: the same W untimed
-    steps, then the first `steps` of its K timed steps (the same solves), each
-    of which uploads the force field
-    from pinned host memory, step, read the step's statistics and read the
-    density back to pinned host memory."""
+    steps, then the first `steps` of its K timed steps (the same solves). Each
+    step uploads the force field from pinned host memory
+    (stable_fluids_b200_stage_vector_field on an upload stream, so the upload
+    of step k runs while step k - 1 computes), steps, and reads the density
+    back to pinned host memory (stable_fluids_b200_read_view_async on a
+    read-back stream, overlapping step k + 1). The timed region runs from before the first upload to after
+    the last read-back. Returns the time, the bytes moved per step and the
+    pressure iterations of the last step (per-step statistics would need a
+    synchronisation per step)."""
     import numpy as np
     import torch
 
@@ -399,23 +404,25 @@ def e2e_run(sf, scene, args, steps, device, net):
         host_force = [torch.from_numpy(np.ascontiguousarray(f, dtype=np.float32)).pin_memory() for f in scene.force]
         host_rho = torch.empty(n, dtype=torch.float32).pin_memory()
         h = sim.scalar_handles[0]
+        # one copy stream per direction: an upload queued behind the previous
+        # step's read-back would wait for that step to finish
+        up, down = torch.cuda.Stream(device=device), torch.cuda.Stream(device=device)
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
-        its = []
         torch.cuda.synchronize()
         start.record(sim.stream)
+        up.wait_event(start)
+        down.wait_event(start)
         for _ in range(steps):
-            rc = sim.lib.stable_fluids_update_vector_field_cuda(sim.ctx, 1, host_force[0].data_ptr(), host_force[1].data_ptr(), host_force[2].data_ptr())
-            if rc != 0:
-                raise RuntimeError(f"update_vector_field with host pointers failed ({rc})")
+            sim.stage_vector(sim.vector_handles[0], host_force[0], host_force[1], host_force[2], up)
             sim.step(1)
-            its.append(sim.stats().pressure_iterations)
-            rho = sim.view(sf.VIEW_SCALAR_FIELD_DATA, h)
-            with torch.cuda.stream(sim.stream):
-                host_rho.copy_(rho.reshape(-1), non_blocking=True)
+            sim.read_view_async(sf.VIEW_SCALAR_FIELD_DATA, [host_rho], down, handle=h)
+        sim.stream.wait_stream(up)
+        sim.stream.wait_stream(down)
         end.record(sim.stream)
         torch.cuda.synchronize()
         t = start.elapsed_time(end) / 1000.0
+        its = [sim.stats().pressure_iterations]
     finally:
         sim.close()
     return t, 3 * n * 4, n * 4, its
@@ -849,7 +856,7 @@ def main():
     if e2e_steps > 0 and "learned" in results and not args.fixed_pressure_iterations:
         te, h2d, d2h, e2e_its = e2e_run(sf, scene, args, e2e_steps, local, net)
         te = max_over_ranks(te, world)
-        e2e = {"value": world * e2e_steps / te, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps, "pressure_iterations": e2e_its}
+        e2e = {"value": world * e2e_steps / te, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps, "pressure_iterations_last_step": e2e_its, "io": "inputs staged on a copy stream (stable_fluids_b200_stage_vector_field), density read back asynchronously (stable_fluids_b200_read_view_async)"}
     fixed = fixed_iterations(sf, None, scene, args.fixed_steps, args.warmup, local, world) if args.fixed_steps > 0 else None
     batch = None
     if args.batch_steps > 0:

@@ -91,6 +91,32 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_create_context(const Sta
 /* Waits for the context stream and returns the statistics of the last step. */
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_get_step_stats(void* context, StableFluidsB200StepStats* out_stats);
 
+/* Staged update of a vector field, for callers that upload a new field from
+ * the host every step (no counterpart in the reference, whose
+ * stable_fluids_update_vector_field_cuda copies on the context stream and so
+ * holds the next step back until the copy is done). The values (host memory,
+ * pinned for the copy to run asynchronously, or device memory; null
+ * components zero-fill as in update_vector_field) are copied on copy_stream
+ * into staging arrays of the context, so the copy can run while the current
+ * step computes; the next stable_fluids_step_cuda waits for it and moves the
+ * values into the field (a device-to-device copy on the context stream) before
+ * the step. The caller keeps the host arrays unchanged until the copy has run
+ * on copy_stream. The first call allocates the staging arrays (3 fields) and
+ * must not be made during a stream capture. Staging again before a step
+ * replaces the staged values. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_stage_vector_field(void* context, StableFluidsVectorFieldHandle field, const float* values_x, const float* values_y, const float* values_z, void* copy_stream);
+
+/* Asynchronous read-back of a view (no counterpart in the reference): the
+ * view's arrays (one, or three for SOA3 views) are copied on the context
+ * stream into a snapshot buffer of the context, then from it to host_out*
+ * on copy_stream, so the next step can start while the copy to the host
+ * runs. The data is in host_out* once copy_stream has passed this call
+ * (synchronize or record an event on it). The snapshot is reused: the next
+ * read_view_async waits on the context stream until this one's copy to the
+ * host is done. The first calls allocate the snapshot arrays and must not be
+ * made during a stream capture. */
+STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_read_view_async(void* context, const StableFluidsViewRequest* request, float* host_out0, float* host_out1, float* host_out2, void* copy_stream);
+
 /* Stages of the step, for profiling one stage outside the step graph. */
 typedef enum StableFluidsB200Stage {
     STABLE_FLUIDS_B200_STAGE_FORCES             = 0, /* v += dt f, velocity packing */

@@ -128,6 +128,8 @@ B200_SYMBOLS = (
     "stable_fluids_b200_default_options",
     "stable_fluids_b200_create_context",
     "stable_fluids_b200_get_step_stats",
+    "stable_fluids_b200_stage_vector_field",
+    "stable_fluids_b200_read_view_async",
     "stable_fluids_b200_enqueue_stage",
     "stable_fluids_b200_get_step_info",
     "stable_fluids_b200_pressure_residual_noalloc",
@@ -190,6 +192,8 @@ def _bind(lib: ctypes.CDLL, extended: bool) -> ctypes.CDLL:
         lib.stable_fluids_b200_default_options.argtypes = [POINTER(B200Options)]
         lib.stable_fluids_b200_create_context.argtypes = [POINTER(ContextCreateDesc), POINTER(B200Options), POINTER(c_void_p), POINTER(c_uint32), c_uint32, POINTER(c_uint32), c_uint32]
         lib.stable_fluids_b200_get_step_stats.argtypes = [P, POINTER(B200StepStats)]
+        lib.stable_fluids_b200_stage_vector_field.argtypes = [P, c_uint32, P, P, P, P]
+        lib.stable_fluids_b200_read_view_async.argtypes = [P, POINTER(ViewRequest), P, P, P, P]
         lib.stable_fluids_b200_enqueue_stage.argtypes = [P, c_uint32, POINTER(c_int32)]
         lib.stable_fluids_b200_get_step_info.argtypes = [P, POINTER(B200StepInfo)]
         lib.stable_fluids_b200_pressure_residual_noalloc.argtypes = [P, P, c_int32, c_int32, c_int32, c_float, POINTER(FlowBoundary), P, P]

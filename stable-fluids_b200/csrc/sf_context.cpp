@@ -56,6 +56,23 @@ struct ScalarField {
 struct VectorField {
     StableFluidsVectorFieldDesc desc{};
     float* data[3] = {nullptr, nullptr, nullptr};
+    // staged upload (stable_fluids_b200_stage_vector_field): the next values,
+    // copied in on the caller's copy stream and moved into `data` by the next
+    // step; `staged` says a copy is waiting
+    float* stage[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t stage_ready = nullptr;  // the staged copy has landed (copy stream)
+    cudaEvent_t stage_free = nullptr;   // the step has taken it (context stream)
+    bool staged = false;
+};
+
+// Asynchronous read-back (stable_fluids_b200_read_view_async): the view's
+// arrays are copied into `snap` on the context stream, then to the host on
+// the caller's copy stream.
+struct Snapshot {
+    float* snap[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t taken = nullptr;  // the copies into snap are done (context stream)
+    cudaEvent_t sent = nullptr;   // the copies to the host are done (copy stream)
+    bool used = false;
 };
 
 struct Context {
@@ -108,7 +125,19 @@ struct Context {
     int check_kernels = 0;  // kernel nodes in the residual loop's body
     bool blocked = true;   // temporally blocked stencil passes
 
+    Snapshot snapshot;
+
     ~Context() {
+        for (auto& v : vectors) {
+            for (auto* p : v.stage)
+                if (p) cudaFree(p);
+            if (v.stage_ready) cudaEventDestroy(v.stage_ready);
+            if (v.stage_free) cudaEventDestroy(v.stage_free);
+        }
+        for (auto* p : snapshot.snap)
+            if (p) cudaFree(p);
+        if (snapshot.taken) cudaEventDestroy(snapshot.taken);
+        if (snapshot.sent) cudaEventDestroy(snapshot.sent);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (ready) cudaEventDestroy(ready);
@@ -660,6 +689,10 @@ StableFluidsResult stable_fluids_destroy_context_cuda(void* context) {
     if (context == nullptr) return STABLE_FLUIDS_RESULT_OK;
     auto* c = static_cast<Context*>(context);
     if (c->stream) cudaStreamSynchronize(c->stream);  // :685
+    // copies still running on a caller's copy stream into or out of the context
+    for (auto& v : c->vectors)
+        if (v.stage_ready) cudaEventSynchronize(v.stage_ready);
+    if (c->snapshot.used) cudaEventSynchronize(c->snapshot.sent);
     if (c->network != nullptr) sfb::net::release(c->network, c);  // its inference buffers in the attached network
     delete c;
     return STABLE_FLUIDS_RESULT_OK;
@@ -704,7 +737,41 @@ StableFluidsResult stable_fluids_step_cuda(void* context) {
     sfb::Range range("stable.step");
     if (context == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     auto& c = *static_cast<Context*>(context);
+    // staged vector fields: wait for their copies, move them in (device to device)
+    for (auto& v : c.vectors) {
+        if (!v.staged) continue;
+        if (cudaStreamWaitEvent(c.stream, v.stage_ready, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        for (int k = 0; k < 3; ++k)
+            if (cudaMemcpyAsync(v.data[k], v.stage[k], c.field_bytes, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaEventRecord(v.stage_free, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        v.staged = false;
+    }
     return cudaGraphLaunch(c.exec, c.stream) == cudaSuccess ? STABLE_FLUIDS_RESULT_OK : STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+}
+
+StableFluidsResult stable_fluids_b200_stage_vector_field(void* context, StableFluidsVectorFieldHandle field, const float* values_x, const float* values_y, const float* values_z, void* copy_stream) {
+    sfb::Range range("stable.stage_vector_field");
+    if (context == nullptr || copy_stream == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    if (field == 0 || field > c.vectors.size()) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& f = c.vectors[field - 1u];
+    const auto cs = static_cast<cudaStream_t>(copy_stream);
+    if (f.stage[0] == nullptr) {  // first call: the staging arrays and their events
+        for (auto*& p : f.stage)
+            if (cudaMalloc(reinterpret_cast<void**>(&p), c.field_bytes) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaEventCreateWithFlags(&f.stage_ready, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaEventCreateWithFlags(&f.stage_free, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaEventRecord(f.stage_free, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    // a copy staged earlier and not yet taken by a step is replaced; one taken
+    // must have left the staging arrays before they are overwritten
+    if (cudaStreamWaitEvent(cs, f.stage_free, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const float* src[3] = {values_x, values_y, values_z};
+    for (int k = 0; k < 3; ++k)
+        if (sfb::copy_or_zero(f.stage[k], src[k], c.field_bytes, cs) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaEventRecord(f.stage_ready, cs) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    f.staged = true;
+    return STABLE_FLUIDS_RESULT_OK;
 }
 
 StableFluidsResult stable_fluids_get_view_cuda(void* context, const StableFluidsViewRequest* request, StableFluidsView* out_view) {
@@ -763,6 +830,40 @@ StableFluidsResult stable_fluids_get_view_cuda(void* context, const StableFluids
         if (cudaEventRecord(c.ready, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
         if (cudaStreamWaitEvent(static_cast<cudaStream_t>(request->consumer_stream), c.ready, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
     }
+    return STABLE_FLUIDS_RESULT_OK;
+}
+
+StableFluidsResult stable_fluids_b200_read_view_async(void* context, const StableFluidsViewRequest* request, float* host_out0, float* host_out1, float* host_out2, void* copy_stream) {
+    sfb::Range range("stable.read_view_async");
+    if (context == nullptr || request == nullptr || copy_stream == nullptr || host_out0 == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& c = *static_cast<Context*>(context);
+    StableFluidsViewRequest r = *request;
+    r.consumer_stream = nullptr;
+    StableFluidsView v{};
+    if (stable_fluids_get_view_cuda(context, &r, &v) != STABLE_FLUIDS_RESULT_OK) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    const int arrays = v.layout == STABLE_FLUIDS_VIEW_LAYOUT_F32_3D_SOA3 ? 3 : 1;
+    float* const out[3] = {host_out0, host_out1, host_out2};
+    const void* const in[3] = {v.data0, v.data1, v.data2};
+    for (int k = 0; k < arrays; ++k)
+        if (out[k] == nullptr) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    auto& sn = c.snapshot;
+    const auto cs = static_cast<cudaStream_t>(copy_stream);
+    if (sn.taken == nullptr) {
+        if (cudaEventCreateWithFlags(&sn.taken, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+        if (cudaEventCreateWithFlags(&sn.sent, cudaEventDisableTiming) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    }
+    for (int k = 0; k < arrays; ++k)
+        if (sn.snap[k] == nullptr && cudaMalloc(reinterpret_cast<void**>(&sn.snap[k]), c.field_bytes) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    // the previous read-back must have left the snapshot before it is overwritten
+    if (sn.used && cudaStreamWaitEvent(c.stream, sn.sent, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    for (int k = 0; k < arrays; ++k)
+        if (cudaMemcpyAsync(sn.snap[k], in[k], c.field_bytes, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaEventRecord(sn.taken, c.stream) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaStreamWaitEvent(cs, sn.taken, 0) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    for (int k = 0; k < arrays; ++k)
+        if (cudaMemcpyAsync(out[k], sn.snap[k], c.field_bytes, cudaMemcpyDeviceToHost, cs) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    if (cudaEventRecord(sn.sent, cs) != cudaSuccess) return STABLE_FLUIDS_RESULT_BACKEND_FAILURE;
+    sn.used = true;
     return STABLE_FLUIDS_RESULT_OK;
 }
 

@@ -116,6 +116,22 @@ class Simulation:
         px, py, pz = self._device_ptr(x), self._device_ptr(y), self._device_ptr(z)
         self._check(self.lib.stable_fluids_update_vector_field_cuda(self.ctx, handle, px, py, pz), "update_vector_field")
 
+    def stage_vector(self, handle: int, x, y, z, copy_stream):
+        """Staged update (stable_fluids_b200_stage_vector_field): x, y, z are
+        pinned host (or device) torch tensors of the grid's size, or None
+        (zero); copied on `copy_stream` (a torch.cuda.Stream) and applied by
+        the next step. Keep the tensors unchanged until the copy has run."""
+        ptr = [None if t is None else c_void_p(t.data_ptr()) for t in (x, y, z)]
+        self._check(self.lib.stable_fluids_b200_stage_vector_field(self.ctx, handle, ptr[0], ptr[1], ptr[2], c_void_p(copy_stream.cuda_stream)), "stage_vector_field")
+
+    def read_view_async(self, kind: int, outs, copy_stream, handle: int = 0):
+        """Asynchronous read-back (stable_fluids_b200_read_view_async) into
+        pinned host tensors `outs` (one, or three for the vector layouts) on
+        `copy_stream`; the data is there once copy_stream has passed it."""
+        req = ViewRequest(kind=kind, scalar_field=handle if kind in (0, 1) else 0, vector_field=handle if kind == VIEW_VECTOR_FIELD else 0, consumer_stream=None)
+        ptr = [c_void_p(t.data_ptr()) for t in outs] + [None] * (3 - len(outs))
+        self._check(self.lib.stable_fluids_b200_read_view_async(self.ctx, byref(req), ptr[0], ptr[1], ptr[2], c_void_p(copy_stream.cuda_stream)), "read_view_async")
+
     # ------------------------------------------------------------- step --
     def step(self, n: int = 1):
         for _ in range(n):
