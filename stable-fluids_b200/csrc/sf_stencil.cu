@@ -1409,12 +1409,15 @@ bool launch_residual_sums_vec(const float* p, const float* div, Dims d, float h2
 }
 
 cudaError_t launch_stencil(const StencilArgs& a, cudaStream_t s) {
-    // per_pass: 0 (default) or 1 = one launch per sweep / colour; >= 2 =
-    // several sweeps per HBM pass: z-wavefront passes where the rows suit
-    // them, else (red-black) the TMA pass. On B200 one launch per sweep is
-    // the faster form: the single sweep streams its 12 B per cell at ~0.8 of
-    // the copy bandwidth, while a 256-cell-row wavefront pass (16 warps per
-    // SM, one barrier per plane) waits on its own instruction latencies.
+    // per_pass: 0 (default) = one launch per Jacobi sweep, red-black solves
+    // in the colour-split layout where the rows allow (one launch per
+    // colour); 1 = one launch per sweep or per colour on the interleaved
+    // field; >= 2 = several sweeps per HBM pass: z-wavefront passes where the
+    // rows suit them, else (red-black) the TMA pass. On B200 one launch per
+    // sweep is the faster form: consecutive single sweeps in alternating z
+    // directions stream their 12 B per cell at about the copy bandwidth,
+    // while a 256-cell-row wavefront pass (16 warps per SM, one barrier per
+    // plane) waits on its own instruction latencies.
     if (a.per_pass >= 2) {
         if (const int v = wave_width(a)) {
             switch (a.kind) {
