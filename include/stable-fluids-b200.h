@@ -53,7 +53,10 @@ typedef enum StableFluidsB200Storage {
 typedef struct StableFluidsB200Options {
     uint32_t scheme;                  /* StableFluidsB200Scheme */
     uint32_t warm_start;              /* StableFluidsB200WarmStart */
-    int32_t iterations_per_pass;      /* temporal-blocking depth (iterations per HBM pass); 0 = automatic */
+    int32_t iterations_per_pass;      /* 0 = automatic (single sweeps; red-black solves in the
+                                       * colour-split layout where rows are a multiple of 8 cells);
+                                       * 1 = one launch per sweep / colour on the interleaved field;
+                                       * >= 2 = temporally blocked passes of that many iterations */
     float residual_tolerance;         /* > 0: solve pressure until rel_res <= tolerance */
     int32_t max_pressure_iterations;  /* cap of the residual-driven solve */
     int32_t residual_check_interval;  /* iterations between residual checks (>= 1) */
