@@ -19,6 +19,7 @@
 #include <cudaTypedefs.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -31,6 +32,7 @@
 #include "sf_unet.h"
 #include "sf_unet_kernels.cuh"
 #include "sf_unet_tc.cuh"
+#include "sf_unet_wgrad_tc.cuh"
 #include "stable-fluids-b200.h"
 
 namespace sfb::net {
@@ -178,17 +180,48 @@ cudaError_t conv_any(int cin, int cout, int epi, const __nv_bfloat16* in, const 
     return cudaErrorInvalidValue;
 }
 
+// The weight gradient on the tcgen05 tensor cores (sf_unet_wgrad_tc.cuh);
+// STABLE_FLUIDS_B200_WGRAD=mma selects the mma.sync GEMM per tap instead.
+bool wgrad_on_mma_sync() {
+    static const bool v = [] {
+        const char* e = std::getenv("STABLE_FLUIDS_B200_WGRAD");
+        return e != nullptr && std::strcmp(e, "mma") == 0;
+    }();
+    return v;
+}
+
 template <int CIN, int COUT>
-cudaError_t wgrad(const __nv_bfloat16* in, const __nv_bfloat16* dout, float* dw, float* db, Dims d, cudaStream_t s) {
-    const int zper = d.nz >= 64 ? 4 : (d.nz >= 16 ? 2 : 1);
-    const dim3 grid(27, static_cast<unsigned>((d.nz + zper - 1) / zper));
-    k_conv3d_wgrad<CIN, COUT><<<grid, 128, 0, s>>>(in, dout, dw, db, d, zper);
+cudaError_t wgrad(const __nv_bfloat16* in, const __nv_bfloat16* dout, float* dw, float* db, Dims d, cudaStream_t s, unsigned* error) {
+    if (wgrad_on_mma_sync() || static_cast<long long>(d.nx) * d.ny * d.nz >= (1ll << 31)) {  // the tensor-core form indexes voxels in 32 bits
+        const int zper = d.nz >= 64 ? 4 : (d.nz >= 16 ? 2 : 1);
+        const dim3 grid(27, static_cast<unsigned>((d.nz + zper - 1) / zper));
+        k_conv3d_wgrad<CIN, COUT><<<grid, 128, 0, s>>>(in, dout, dw, db, d, zper);
+        return cudaGetLastError();
+    }
+    using C = tc::WgCfg<CIN, COUT>;
+    const auto kern = tc::k_conv3d_wgrad_tc<CIN, COUT>;
+    static const cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
+    if (attr != cudaSuccess) return attr;
+    static const int per_sm = [&] {
+        int k = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kern, tc::kWgThreads, C::BYTES) != cudaSuccess || k < 1) k = 1;
+        return k;
+    }();
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long nvox = static_cast<long long>(d.nx) * d.ny * d.nz;
+    const long long nchunks = (nvox + tc::kWgK - 1) / tc::kWgK;
+    long long per_tap = static_cast<long long>(sms) * per_sm / 27;  // one wave of CTAs over the 27 taps
+    if (per_tap < 1) per_tap = 1;
+    const long long chunks = (nchunks + per_tap - 1) / per_tap;
+    const dim3 grid(27, static_cast<unsigned>((nchunks + chunks - 1) / chunks));
+    kern<<<grid, tc::kWgThreads, C::BYTES, s>>>(in, dout, dw, db, d, static_cast<int>(chunks), error);
     return cudaGetLastError();
 }
 
-cudaError_t wgrad_any(int cin, int cout, const __nv_bfloat16* in, const __nv_bfloat16* dout, float* dw, float* db, Dims d, cudaStream_t s) {
+cudaError_t wgrad_any(int cin, int cout, const __nv_bfloat16* in, const __nv_bfloat16* dout, float* dw, float* db, Dims d, cudaStream_t s, unsigned* error) {
 #define SFB_WG(CI, CO) \
-    if (cin == CI && cout == CO) return wgrad<CI, CO>(in, dout, dw, db, d, s);
+    if (cin == CI && cout == CO) return wgrad<CI, CO>(in, dout, dw, db, d, s, error);
     SFB_WG(16, 16) SFB_WG(16, 32) SFB_WG(32, 32) SFB_WG(32, 64) SFB_WG(64, 64) SFB_WG(96, 32) SFB_WG(48, 16)
 #undef SFB_WG
     return cudaErrorInvalidValue;
@@ -378,48 +411,48 @@ cudaError_t backward(Net* n, cudaStream_t s) {
     cudaError_t e;
     SFB_TRY(cudaMemsetAsync(n->g, 0, n->nparams * sizeof(float), s));
     // out layer (linear)
-    SFB_TRY(wgrad_any(16, 16, B.d0b, B.g16, GW(n, OUT), GB(n, OUT), B.d0, s));
+    SFB_TRY(wgrad_any(16, 16, B.d0b, B.g16, GW(n, OUT), GB(n, OUT), B.d0, s, n->error));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.g16, WT(n, OUT), nullptr, B.gd0b, 16, 0, B.d0, s, n->error));
     // d0b, d0a (input of d0a: cat0 = [up(d1b) | e0b])
     k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.gd0b, B.d0b, B.n0 * 16);
-    SFB_TRY(wgrad_any(16, 16, B.d0a, B.gd0b, GW(n, D0B), GB(n, D0B), B.d0, s));
+    SFB_TRY(wgrad_any(16, 16, B.d0a, B.gd0b, GW(n, D0B), GB(n, D0B), B.d0, s, n->error));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.gd0b, WT(n, D0B), nullptr, B.gd0a, 16, 0, B.d0, s, n->error));
     k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.gd0a, B.d0a, B.n0 * 16);
-    SFB_TRY(wgrad_any(48, 16, B.cat0, B.gd0a, GW(n, D0A), GB(n, D0A), B.d0, s));
+    SFB_TRY(wgrad_any(48, 16, B.cat0, B.gd0a, GW(n, D0A), GB(n, D0A), B.d0, s, n->error));
     SFB_TRY(conv_any(16, 48, tc::LINEAR_BF16, B.gd0a, WT(n, D0A), nullptr, B.gcat0, 48, 0, B.d0, s, n->error));
     k_upsample2_backward<<<row_grid(B.d1.nx, 4, B.d1.ny, B.d1.nz), 256, 0, s>>>(B.gcat0, 48, 0, 32, B.d1, B.gd1b);
     // d1b, d1a (input of d1a: cat1 = [up(bb) | e1b])
     k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.gd1b, B.d1b, B.n1 * 32);
-    SFB_TRY(wgrad_any(32, 32, B.d1a, B.gd1b, GW(n, D1B), GB(n, D1B), B.d1, s));
+    SFB_TRY(wgrad_any(32, 32, B.d1a, B.gd1b, GW(n, D1B), GB(n, D1B), B.d1, s, n->error));
     SFB_TRY(conv_any(32, 32, tc::LINEAR_BF16, B.gd1b, WT(n, D1B), nullptr, B.gd1a, 32, 0, B.d1, s, n->error));
     k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.gd1a, B.d1a, B.n1 * 32);
-    SFB_TRY(wgrad_any(96, 32, B.cat1, B.gd1a, GW(n, D1A), GB(n, D1A), B.d1, s));
+    SFB_TRY(wgrad_any(96, 32, B.cat1, B.gd1a, GW(n, D1A), GB(n, D1A), B.d1, s, n->error));
     SFB_TRY(conv_any(32, 96, tc::LINEAR_BF16, B.gd1a, WT(n, D1A), nullptr, B.gcat1, 96, 0, B.d1, s, n->error));
     k_upsample2_backward<<<row_grid(B.d2.nx, 8, B.d2.ny, B.d2.nz), 256, 0, s>>>(B.gcat1, 96, 0, 64, B.d2, B.gbb);
     // bottleneck
     k_relu_backward<<<blocks_for(B.n2 * 64 / 8), 256, 0, s>>>(B.gbb, B.bb, B.n2 * 64);
-    SFB_TRY(wgrad_any(64, 64, B.ba, B.gbb, GW(n, BB), GB(n, BB), B.d2, s));
+    SFB_TRY(wgrad_any(64, 64, B.ba, B.gbb, GW(n, BB), GB(n, BB), B.d2, s, n->error));
     SFB_TRY(conv_any(64, 64, tc::LINEAR_BF16, B.gbb, WT(n, BB), nullptr, B.gba, 64, 0, B.d2, s, n->error));
     k_relu_backward<<<blocks_for(B.n2 * 64 / 8), 256, 0, s>>>(B.gba, B.ba, B.n2 * 64);
-    SFB_TRY(wgrad_any(32, 64, B.p1, B.gba, GW(n, BA), GB(n, BA), B.d2, s));
+    SFB_TRY(wgrad_any(32, 64, B.p1, B.gba, GW(n, BA), GB(n, BA), B.d2, s, n->error));
     SFB_TRY(conv_any(64, 32, tc::LINEAR_BF16, B.gba, WT(n, BA), nullptr, B.gp1, 32, 0, B.d2, s, n->error));
     // e1b receives the skip (channels 64..95 of cat1) and the pooled path
     k_copy_channels<<<blocks_for(B.n1 * 4), 256, 0, s>>>(B.gcat1, 96, 64, B.ge1b, 32, 0, 32, B.n1, 0);
     k_pool2_backward<<<row_grid(B.d1.nx, 4, B.d1.ny, B.d1.nz), 256, 0, s>>>(B.gp1, 32, B.d2, B.ge1b, 32, 0, 1);
     k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.ge1b, B.e1b, B.n1 * 32);
-    SFB_TRY(wgrad_any(32, 32, B.e1a, B.ge1b, GW(n, E1B), GB(n, E1B), B.d1, s));
+    SFB_TRY(wgrad_any(32, 32, B.e1a, B.ge1b, GW(n, E1B), GB(n, E1B), B.d1, s, n->error));
     SFB_TRY(conv_any(32, 32, tc::LINEAR_BF16, B.ge1b, WT(n, E1B), nullptr, B.ge1a, 32, 0, B.d1, s, n->error));
     k_relu_backward<<<blocks_for(B.n1 * 32 / 8), 256, 0, s>>>(B.ge1a, B.e1a, B.n1 * 32);
-    SFB_TRY(wgrad_any(16, 32, B.p0, B.ge1a, GW(n, E1A), GB(n, E1A), B.d1, s));
+    SFB_TRY(wgrad_any(16, 32, B.p0, B.ge1a, GW(n, E1A), GB(n, E1A), B.d1, s, n->error));
     SFB_TRY(conv_any(32, 16, tc::LINEAR_BF16, B.ge1a, WT(n, E1A), nullptr, B.gp0, 16, 0, B.d1, s, n->error));
     // e0b: skip (channels 32..47 of cat0) + pooled path
     k_copy_channels<<<blocks_for(B.n0 * 2), 256, 0, s>>>(B.gcat0, 48, 32, B.ge0b, 16, 0, 16, B.n0, 0);
     k_pool2_backward<<<row_grid(B.d0.nx, 2, B.d0.ny, B.d0.nz), 256, 0, s>>>(B.gp0, 16, B.d1, B.ge0b, 16, 0, 1);
     k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.ge0b, B.e0b, B.n0 * 16);
-    SFB_TRY(wgrad_any(16, 16, B.e0a, B.ge0b, GW(n, E0B), GB(n, E0B), B.d0, s));
+    SFB_TRY(wgrad_any(16, 16, B.e0a, B.ge0b, GW(n, E0B), GB(n, E0B), B.d0, s, n->error));
     SFB_TRY(conv_any(16, 16, tc::LINEAR_BF16, B.ge0b, WT(n, E0B), nullptr, B.ge0a, 16, 0, B.d0, s, n->error));
     k_relu_backward<<<blocks_for(B.n0 * 16 / 8), 256, 0, s>>>(B.ge0a, B.e0a, B.n0 * 16);
-    SFB_TRY(wgrad_any(16, 16, B.in, B.ge0a, GW(n, E0A), GB(n, E0A), B.d0, s));
+    SFB_TRY(wgrad_any(16, 16, B.in, B.ge0a, GW(n, E0A), GB(n, E0A), B.d0, s, n->error));
     return cudaGetLastError();
 }
 
