@@ -21,9 +21,10 @@
 // memory (the B groups, the next stage, a pad at the end), and those rows of
 // the accumulator are never read. Four stages: the copies of chunks i + 1
 // and i + 2 are in flight while chunk i is multiplied, the latter into the
-// stage chunk i - 2 was multiplied from. At the end warp w reads accumulator lanes 32 w .. 32 w + 31 (the
-// output channels) and adds them to dw with FP32 atomics; the centre tap's
-// CTAs also sum dout into the bias gradient. Every wait on an mbarrier is
+// stage chunk i - 2 was multiplied from. At the end warp w reads
+// accumulator lanes 32 w .. 32 w + 31 (the output channels) and adds them to
+// dw with FP32 atomics; the centre tap's CTAs also sum dout into the bias
+// gradient. Every wait on an mbarrier is
 // bounded (tc::mbar_wait); a CTA that gives up records it in *error.
 #pragma once
 
