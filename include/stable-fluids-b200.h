@@ -106,8 +106,9 @@ STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_get_step_stats(void* con
  * the step. The caller keeps the host arrays unchanged until the copy has run
  * on copy_stream. The first call allocates the staging arrays (3 fields) and
  * must not be made during a stream capture. Staging again before a step
- * replaces the staged values. Only stable_fluids_step_cuda applies staged
- * values (a batch step does not). */
+ * replaces the staged values, and staged values still pending at the next
+ * step overwrite an update_vector_field made in between. Only
+ * stable_fluids_step_cuda applies staged values (a batch step does not). */
 STABLE_FLUIDS_API StableFluidsResult stable_fluids_b200_stage_vector_field(void* context, StableFluidsVectorFieldHandle field, const float* values_x, const float* values_y, const float* values_z, void* copy_stream);
 
 /* Asynchronous read-back of a view (no counterpart in the reference): the
